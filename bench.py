@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Throughput of the PCG-OLE expansion hot path on B200.
+
+A step is one party's full PCG-OLE expansion at N=2^20, c=4, t=16 (w=1,
+ChaCha8 tree PRG): 4096 keyed half-tree DPF instances of domain 2^17
+(2^29 leaves) -> output-layer hash/convert -> gather into the folded
+g_ij -> NTT products with the resident a_i images -> x, z.  It yields N OLE
+correlations for that party, so the metric is N / step time (corr/s).
+
+  value   whole-job corr/s, inputs (keys, noise) already resident in HBM,
+          device-timed with CUDA events on the library's stream; L2 flushed
+          (256 MiB write) between timed steps.
+  e2e     the same through pcgb_expand_host with pinned host buffers: the
+          H2D of the step's keys and noise and the D2H of x and z are inside
+          the timed region.
+  roofline  the dominant kernel (the fused leaf/out-hash/gather kernel) is
+          integer-ALU bound (ChaCha8 ARX); achieved = its algorithmic int ops
+          per launch / its mean duration, peak = the ARX throughput probe run
+          in this process.  roofline_ntt gives the HBM view of the NTT stage.
+  cpu_baseline  the oracle's CPU restatement of the same expansion, timed on
+          a bounded sample on this host's cores (rank 0, N=1 only).
+
+`--impl reference` times the reference's CPU implementation of the path (the
+oracle port; the reference's own CPU DPF needs emp-tool, absent here) on the
+host cores and prints its line with "impl": "reference".
+
+Multi-GPU (torchrun): every rank runs its own expansions (independent
+replicas, no data-path collective); value = total correlations of all ranks
+/ max over ranks of the timed region.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "pcg-square_b200"))
+
+METRIC = "OLE corr/s at N=2^20,c=4,t=16, bit-exact; serve p50/p99 vs plain one-shot"
+N, C_, T_, W_ = 1 << 20, 4, 16, 1
+A_SEED = 7
+L2_BYTES = 126 * 1024 * 1024
+# Published figure for this metric and shape (1x L40S, serial arm,
+# GPU_baseline/final_l40s/e2e_arms.csv:32): 2^20 / 192.11 ms.
+PUBLISHED = 2 ** 20 / 0.19211
+# ChaCha8 quarter-round ops (4 add, 4 xor, 4 rotate) x 4 QR x 8 rounds.
+OPS_PER_BLOCK = 12 * 4 * 8
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-verify", action="store_true")
+    return ap.parse_args()
+
+
+# ---- distributed plumbing ---------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.rank = int(os.environ.get("RANK", 0))
+        self.world = int(os.environ.get("WORLD_SIZE", 1))
+        self.local = int(os.environ.get("LOCAL_RANK", 0))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+            self.torch = torch
+            self.device = torch.device("cuda", self.local) if backend == "nccl" else None
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64, device=self.device)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.barrier()
+            self.pg.destroy_process_group()
+
+
+# ---- clocks -----------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(power) if power else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---- CPU baseline (oracle port, bounded sample) ------------------------------
+def cpu_sample(threads, n_blocks=None, keys=None, polymuls=None):
+    """Times a bounded sample of the oracle's expansion and extrapolates to one
+    full expansion: returns (corr/s, seconds of CPU work, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_lib as O
+    s = O.shape(N, C_, T_)
+    if not hasattr(cpu_sample, "material"):
+        r0, _, cws, cwo = O.deal_keys(s, 1000)
+        cpu_sample.material = (r0, cws, cwo, O.public_a(s, A_SEED))
+    r0, cws, cwo, a = cpu_sample.material
+    B = T_ * T_
+    n_blocks = n_blocks or 1
+    keys = keys or min(B, max(threads, 32))
+    polymuls = polymuls or threads
+    t_dpf, t_ntt = O.bench_sample(s, 0, r0, cws, cwo, a, n_blocks, keys, polymuls, threads)
+    total_keys = C_ * C_ * B
+    n_products = C_ + 2 * C_ * C_   # step 4 of pcg_ole_impl.h:460-483
+    t_full = t_dpf * total_keys / (n_blocks * keys) + t_ntt * n_products / polymuls
+    desc = (f"{n_blocks * keys} of {total_keys} keys (DPF+convert+scatter) and {polymuls} of "
+            f"{n_products} length-2^20 products, {threads} threads, extrapolated to one expansion")
+    return N / t_full, t_dpf + t_ntt, desc
+
+
+def run_reference(args, d):
+    if d.rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_sample(threads, keys=threads)
+    vals, spent = [], 0.0
+    for _ in range(args.steps):
+        v, sec, desc = cpu_sample(threads, keys=threads)
+        vals.append(v)
+        spent += sec
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "corr/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * N / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": value / PUBLISHED, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": "pcg-ole expansion N=2^20 c=4 t=16 w=1 chacha8 (one party)",
+                   "N": N, "c": C_, "t": T_, "host_threads": threads},
+        "cpu_baseline": {"value": value, "unit": "corr/s", "cores": threads, "kind": "port",
+                         "sample": desc},
+        "e2e": {"value": value, "unit": "corr/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- our arm -----------------------------------------------------------------
+def run_ours(args, d):
+    import ctypes as C
+
+    import pcg_b200 as L
+    L.set_device(d.local)
+    a = L.public_a(N, C_, A_SEED)
+    e = L.Expander(N, C_, T_, W_, L.PRG_CHACHA8, public_a=a)
+    K, levels = e.K, e.levels
+    seed = 1000 + d.rank
+    d_r0, d_r1 = L.DeviceBuffer(16 * K), L.DeviceBuffer(16 * K)
+    d_cws, d_cwo = L.DeviceBuffer(16 * K * levels), L.DeviceBuffer(8 * K)
+    e.deal_keys_device(seed, d_r0.ptr, d_r1.ptr, d_cws.ptr, d_cwo.ptr)
+    pos0, val0 = L.noise(N, C_, T_, seed, 0)
+    pos1, val1 = L.noise(N, C_, T_, seed, 1)
+    d_pos, d_val = L.to_device(pos0), L.to_device(val0)
+    d_x, d_z = L.DeviceBuffer(8 * N), L.DeviceBuffer(8 * N)
+    flush = L.DeviceBuffer(2 * L2_BYTES)
+    args_dev = (d_r0.ptr, d_cws.ptr, d_cwo.ptr, d_pos.ptr, d_val.ptr, d_x.ptr, d_z.ptr)
+
+    for _ in range(args.warmup):
+        e.expand_device(0, *args_dev)
+    L.synchronize()
+    gops_peak, _ = L.arx_peak()
+
+    e.set_profiling(args.steps)
+    evs = [(L.Event(), L.Event()) for _ in range(args.steps)]
+    clocks = Clocks(d.local)
+    d.barrier()
+    L.synchronize()
+    clocks.start()
+    launches0 = L.launch_count()
+    for i in range(args.steps):
+        L.lib.pcgb_memset(flush.ptr, i & 0xFF, flush.nbytes, None)  # L2 flush, not timed
+        evs[i][0].record()
+        e.expand_device(0, *args_dev)
+        evs[i][1].record()
+    L.synchronize()
+    launches = L.launch_count() - launches0
+    clk = clocks.stop()
+    step_ms = [s.elapsed_ms(t) for s, t in evs]
+    stages = e.stage_times()
+    total_ms = float(np.sum(step_ms))
+    total_ms_max = d.max(total_ms)
+    d.barrier()
+    value = N * args.steps * d.world / (total_ms_max / 1e3)
+
+    # Bit-exactness spot check (untimed): party 1 on the same keys, then the
+    # OLE relation z0 + z1 = x0 * x1 over the whole ring.
+    verified = None
+    if not args.no_verify:
+        x0, z0 = d_x.download(np.uint64, N), d_z.download(np.uint64, N)
+        d_pos1, d_val1 = L.to_device(pos1), L.to_device(val1)
+        e.expand_device(1, d_r1.ptr, d_cws.ptr, d_cwo.ptr, d_pos1.ptr, d_val1.ptr, d_x.ptr, d_z.ptr)
+        x1, z1 = d_x.download(np.uint64, N), d_z.download(np.uint64, N)
+        prod, _ = L.poly_mul_u64_gpuntt(x0, x1, 1, N)
+        zs = z0 + z1
+        zs = np.where(zs >= np.uint64(L.P), zs - np.uint64(L.P), zs)
+        verified = bool((prod == zs).all())
+
+    # e2e through the public host API with pinned buffers.
+    e2e = None
+    if args.e2e_steps > 0:
+        try:
+            import torch
+            pin = lambda n: torch.empty(n, dtype=torch.int64, pin_memory=True)
+        except Exception:
+            pin = None
+        h_r0 = d_r0.download(np.uint64, 2 * K)
+        h_cws = d_cws.download(np.uint64, 2 * K * levels)
+        h_cwo = d_cwo.download(np.uint64, K)
+        host = [h_r0, h_cws, h_cwo, pos0, val0, np.zeros(N, np.uint64), np.zeros(N, np.uint64)]
+        if pin:
+            keep = []
+            for i, arr in enumerate(host):
+                t = pin(arr.size)
+                v = t.numpy().view(np.uint64)
+                v[:] = arr
+                keep.append(t)
+                host[i] = v
+        ptrs = [h.ctypes.data for h in host]
+        h2d = sum(h.nbytes for h in host[:5])
+        d2h = host[5].nbytes + host[6].nbytes
+        lib = L.lib
+        lib.pcgb_expand_host(e.h, 0, *ptrs)  # warm the staging buffers
+        s, t = L.Event(), L.Event()
+        s.record()
+        for _ in range(args.e2e_steps):
+            rc = lib.pcgb_expand_host(e.h, 0, *ptrs)
+            if rc:
+                raise RuntimeError(lib.pcgb_last_error().decode())
+        t.record()
+        e2e_ms = d.max(s.elapsed_ms(t))
+        e2e = {"value": N * args.e2e_steps * d.world / (e2e_ms / 1e3), "unit": "corr/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "pinned": bool(pin)}
+
+    # Roofline of the dominant kernel (fused leaf gather), ALU bound.
+    leaf_ms = float(np.mean([s[1] for s in stages])) if stages else None
+    D = 1 << e.levels
+    S = 16
+    blocks_per_launch = K * D * (1 + (S - 1) / S)   # out-hash + tree blocks below the frontier
+    ops = blocks_per_launch * OPS_PER_BLOCK
+    achieved = ops / (leaf_ms * 1e-3) / 1e12 if leaf_ms else None
+    peak = gops_peak / 1e3
+    roofline = {"bound": "int_alu", "kernel": "leaf_gather_kernel<1,4,chacha8>",
+                "achieved": achieved, "peak": peak, "unit": "Tops/s",
+                "frac": achieved / peak if achieved else None,
+                "traffic": LEAF_TRAFFIC_BYTES,
+                "peak_source": "ARX probe (pcgb_arx_peak) in this run; MEASURED_PEAKS.json has "
+                               "no integer-ALU figure",
+                "ops_per_launch": ops, "launch_ms": leaf_ms}
+    ntt_ms = float(np.mean([s[3] for s in stages])) if stages else None
+    Q = e.Q
+    ntt_bytes = 8 * N * (4 * Q + 3)
+    roofline_ntt = {"bound": "hbm", "achieved": ntt_bytes / (ntt_ms * 1e-3) / 1e9 if ntt_ms else None,
+                    "peak": hbm_peak(), "unit": "GB/s", "bytes_per_step": ntt_bytes,
+                    "stage_ms": ntt_ms}
+    if roofline_ntt["achieved"]:
+        roofline_ntt["frac"] = roofline_ntt["achieved"] / roofline_ntt["peak"]
+
+    cpu = None
+    if d.world == 1 and d.rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, sec, desc = cpu_sample(threads)
+        cpu = {"value": v, "unit": "corr/s", "cores": threads, "kind": "port",
+               "sample": desc, "sample_seconds": sec}
+
+    if d.rank == 0:
+        stage_means = [float(np.mean([s[i] for s in stages])) for i in range(4)] if stages else None
+        line = {
+            "metric": METRIC, "value": value, "unit": "corr/s", "n_gpus": d.world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": value / PUBLISHED, "dtype": "u64",
+            "data": "synthetic",
+            "config": {"workload": "pcg-ole expansion N=2^20 c=4 t=16 w=1 chacha8 (one party, "
+                                   "keyed DPF from the GPU dealer)",
+                       "N": N, "c": C_, "t": T_, "w": W_, "keys": K, "leaves": K * D,
+                       "parallelism": f"replicas x{d.world}",
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "vs_baseline_ref": "1x L40S serial arm 5.46M corr/s "
+                                          "(GPU_baseline/final_l40s/e2e_arms.csv:32)"},
+            "stage_ms": dict(zip(["tops", "leaf_gather", "x", "ntt"], stage_means))
+            if stage_means else None,
+            "bit_exact_ole_relation": verified,
+            "gpu_launches": int(launches),
+            "clocks": clk, "roofline": roofline, "roofline_ntt": roofline_ntt,
+            "e2e": e2e, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    e.close()
+
+
+# DRAM bytes per launch of the leaf kernel from the ncu capture summarised in
+# profiles/leaf_gather_N2e20_c4_t16.md (None until captured).
+LEAF_TRAFFIC_BYTES = None
+
+
+def hbm_peak():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except Exception:
+        return 6650.0   # fallback figure for this pool
+
+
+def main():
+    args = parse()
+    d = Dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, d)
+        else:
+            run_ours(args, d)
+    finally:
+        d.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,197 @@
+/*
+ * pcg_b200 — C ABI of the B200 (sm_100a) PCG-OLE expansion library.
+ *
+ * Two groups of entry points:
+ *
+ *  1. Drop-ins for the reference's pcg_cuda:: hooks (same argument meaning,
+ *     host buffers in and out, same error cases).  Each names the reference
+ *     declaration it replaces.  include/common/ declares the C++
+ *     pcg_cuda:: wrappers with the reference's exact signatures on top of
+ *     these, so CPU_baseline's PCG_ENABLE_CUDA code links unchanged.
+ *
+ *  2. Native device-resident entry points (keyed DPF, fused expansion,
+ *     batched NTT, serving).  Pointers marked d_ are device pointers;
+ *     `stream` is a cudaStream_t (NULL = the library's own stream on the
+ *     current device).
+ *
+ * Every function returns 0 on success or a negative PCGB_E* code; the
+ * message of the last failure on the calling thread is pcgb_last_error().
+ * Nothing here falls back to the CPU: without a usable CUDA device the
+ * calls fail with PCGB_ENODEV.
+ */
+#ifndef PCG_B200_H_
+#define PCG_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PCGB_OK 0
+#define PCGB_EINVAL (-1)   /* bad argument / unsupported shape */
+#define PCGB_ECUDA (-2)    /* CUDA runtime error */
+#define PCGB_ENODEV (-3)   /* no CUDA device */
+#define PCGB_ENOMEM (-4)   /* allocation failed / over the memory budget */
+#define PCGB_ECALLBACK (-5) /* exchange callback reported failure */
+#define PCGB_ETIMEOUT (-6) /* a bounded wait gave up */
+#define PCGB_ESTATE (-7)   /* object in the wrong state (closed, cancelled) */
+
+#define PCGB_PRG_AES 0
+#define PCGB_PRG_CHACHA8 1
+
+/* 128-bit DPF node: lo = bytes 0..7, hi = bytes 8..15 (the memory order of
+ * emp::block; same layout as pcg_cuda::DpfBlk, GPU_baseline/common/dpf_gpu.h:23-26). */
+typedef struct pcgb_blk {
+    uint64_t lo, hi;
+} pcgb_blk;
+
+/* Per-level correction-word exchange: fill peer[0..count) with the other
+ * party's shares of my[0..count).  Return 0, or nonzero to abort the call
+ * (reported as PCGB_ECALLBACK).  Replaces the std::function DpfExchangeFn
+ * (GPU_baseline/common/dpf_gpu.h:31-32). */
+typedef int (*pcgb_exchange_fn)(const pcgb_blk* my, pcgb_blk* peer, size_t count, void* user);
+
+const char* pcgb_last_error(void);
+int pcgb_version(void); /* major*10000 + minor*100 + patch */
+
+/* ---- device / runtime -------------------------------------------------- */
+/* is_cuda_available / device_name / runtime_version
+ * (GPU_baseline/common/poly_mul_cuda.h:13-16). */
+int pcgb_is_cuda_available(void); /* 1 or 0 */
+int pcgb_device_name(char* buf, size_t len);
+int pcgb_runtime_version(char* buf, size_t len);
+int pcgb_set_device(int dev);
+int pcgb_get_device(int* dev);
+int pcgb_sm_count(int* n);
+int pcgb_malloc(void** d_ptr, size_t bytes);
+int pcgb_free(void* d_ptr);
+int pcgb_memcpy_h2d(void* d_dst, const void* src, size_t bytes, void* stream);
+int pcgb_memcpy_d2h(void* dst, const void* d_src, size_t bytes, void* stream);
+int pcgb_memset(void* d_dst, int value, size_t bytes, void* stream);
+int pcgb_stream_synchronize(void* stream);
+int pcgb_device_synchronize(void);
+void* pcgb_default_stream(void);
+/* Kernel launches issued by the library since load (all devices). */
+unsigned long long pcgb_launch_count(void);
+/* Integer-ALU roofline probe: ChaCha8 quarter rounds on register-resident
+ * states over every SM; *gops = G int-ops/s (12 ops per quarter round). */
+int pcgb_arx_peak(double* gops, float* ms);
+/* CUDA events on the library's streams (device-side timing). */
+int pcgb_event_create(void** ev);
+int pcgb_event_destroy(void* ev);
+int pcgb_event_record(void* ev, void* stream);
+/* Waits for `stop`, then *ms = elapsed time start -> stop. */
+int pcgb_event_elapsed(void* start, void* stop, float* ms);
+
+/* ---- drop-ins: half-tree DPF (GPU_baseline/common/dpf_gpu.h:55-75) ------ */
+/* dpf_gpu_batch_full_eval: B instances, domain 2^n, branching 2^w (w in
+ * [1,4], w | n); roots[B]; dltsft[B][n/w][2^w-1]; round_keys: AES only,
+ * (2^w-1)*176 bytes; party is accepted and unused (ordering lives inside
+ * the exchange); out_leaves[B][2^n]. */
+int pcgb_dpf_batch_full_eval(int B, int n, int w, const pcgb_blk* roots,
+                             const pcgb_blk* dltsft, const uint8_t* round_keys, int party,
+                             pcgb_exchange_fn exchange, void* user, pcgb_blk* out_leaves,
+                             int prg);
+/* dpf_gpu_batch_full_eval_device: leaves stay on the device; *d_leaves
+ * aliases an internal pool, valid until the next pcgb_dpf_batch_* call on
+ * this device (B <= 0 gives NULL). */
+int pcgb_dpf_batch_full_eval_device(int B, int n, int w, const pcgb_blk* roots,
+                                    const pcgb_blk* dltsft, const uint8_t* round_keys, int party,
+                                    pcgb_exchange_fn exchange, void* user, int prg,
+                                    const pcgb_blk** d_leaves);
+
+/* ---- drop-ins: output layer (GPU_baseline/common/leaf_convert_cuda.h:43-52) */
+int pcgb_dpf_out_sums(const pcgb_blk* d_leaves, int B, size_t D, uint64_t prime,
+                      uint64_t* sumC_host, uint64_t* sumT_host);
+int pcgb_dpf_out_scatter_g(const pcgb_blk* d_leaves, int B, size_t D, int t, int party,
+                           uint64_t prime, const uint64_t* CW_host, uint64_t* g_out_host,
+                           int N);
+
+/* ---- drop-ins: negacyclic poly-mul (GPU_baseline/common/poly_mul_cuda.h:14-31,
+ * plus the merge / 4-step names called from CPU_baseline/pcg_ole_2pc/pcg_ole.h:147,157,226-230).
+ * variant selects the supported-size rules of each reference name; all run
+ * the same four-step kernels. */
+#define PCGB_POLYMUL_V1 0     /* poly_mul_u64: N in [2, 32768] */
+#define PCGB_POLYMUL_MERGE 1  /* poly_mul_u64_gpuntt: N in [2, 2^24] */
+#define PCGB_POLYMUL_4STEP 2  /* poly_mul_u64_gpuntt_4step: N in [4096, 2^24] */
+#define PCGB_POLYMUL_SQUARE 3 /* poly_mul_u64_gpuntt_square: N in [256, 2^24] */
+/* 1 if supported, 0 if not (reason filled), <0 on error. */
+int pcgb_poly_mul_supported(int variant, uint64_t prime, int N, char* reason, size_t len);
+int pcgb_poly_mul_u64(int variant, uint64_t* out, const uint64_t* a, const uint64_t* b,
+                      int batch, int N, uint64_t prime, double* device_ms);
+
+/* ---- drop-ins: AES-128 (GPU_baseline/common/aes_gpu.h:13-19) ------------ */
+int pcgb_aes128_expand_key(const uint8_t key[16], uint8_t round_keys[176]);
+int pcgb_aes128_ecb_encrypt(const uint8_t* keys, const uint8_t* in, uint8_t* out, int count);
+/* Tree-PRG sub-key schedules from a master key (half_tree_dpf/tree_prg.h:45-57;
+ * half_tree_dpf/dpf.cpp:605-619): nk*176 bytes. */
+int pcgb_aes_tree_round_keys(const uint8_t master[16], int nk, uint8_t* round_keys);
+
+/* ---- native: keyed DPF ---------------------------------------------------
+ * A keyed instance: root, CW[level][0..2^w-1) (the last child's CW is their
+ * XOR), and for the output layer one field element cw_out.  Both parties
+ * hold the same CWs; roots differ by Delta. */
+/* Full-domain leaves of K keys: d_leaves[K][2^n]. */
+int pcgb_dpf_keyed_full_eval(int K, int n, int w, int prg, const pcgb_blk* d_roots,
+                             const pcgb_blk* d_cws, const uint8_t* round_keys,
+                             pcgb_blk* d_leaves, void* stream);
+
+/* ---- native: batched NTT ----------------------------------------------- */
+/* c[k] = a[k] * b[k] mod (X^N + 1) for k < batch (device, c may alias). */
+int pcgb_poly_mul_device(uint64_t* d_c, const uint64_t* d_a, const uint64_t* d_b, int batch,
+                         int N, void* stream);
+/* Uneven batch: polys of different lengths in one call; d_a[i], d_b[i],
+ * d_c[i] each of length N[i]. */
+int pcgb_poly_mul_device_multi(int count, uint64_t* const* d_c, const uint64_t* const* d_a,
+                               const uint64_t* const* d_b, const int* N, void* stream);
+
+/* ---- native: PCG-OLE expansion -------------------------------------------
+ * An expander owns the resident per-shape state of one (N, c, t, w, prg)
+ * shape: NTT plans, the a_i evaluation images and their pair products, the
+ * gather plan and scratch.  public_a: (c-1)*N coefficients of a_1..a_{c-1}
+ * (a_0 = 1).  master_key: AES tree-PRG master key (AES only, else NULL). */
+typedef struct pcgb_expander pcgb_expander;
+int pcgb_expander_create(pcgb_expander** e, int N, int c, int t, int w, int prg,
+                         const uint64_t* public_a, const uint8_t* master_key);
+int pcgb_expander_destroy(pcgb_expander* e);
+/* Shape-derived sizes: K keys, levels, nk CWs per level. */
+int pcgb_expander_info(const pcgb_expander* e, int* K, int* levels, int* nk, size_t* scratch_bytes);
+/* One party's expansion from device-resident inputs:
+ *   d_roots[K], d_cws[K*levels*nk], d_cw_out[K], d_pos[c*t], d_val[c*t]
+ *   -> d_x[N], d_z[N] (x = sum a_i e_i, z = sum_{i,j} a_i a_j g_ij). */
+int pcgb_expand_device(pcgb_expander* e, int party, const pcgb_blk* d_roots,
+                       const pcgb_blk* d_cws, const uint64_t* d_cw_out, const uint64_t* d_pos,
+                       const uint64_t* d_val, uint64_t* d_x, uint64_t* d_z, void* stream);
+/* Same with host buffers (copies in and out included). */
+int pcgb_expand_host(pcgb_expander* e, int party, const pcgb_blk* roots, const pcgb_blk* cws,
+                     const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val,
+                     uint64_t* x, uint64_t* z);
+/* Only the DPF + output-layer stages: the folded, pair-merged g' buffers
+ * (Q = c(c+1)/2 of N words, pair order (0,0),(0,1)..(0,c-1),(1,1),..),
+ * g'_ij = g_ij + g_ji for i < j.  For parity checks and staged pipelines. */
+int pcgb_expand_g_device(pcgb_expander* e, int party, const pcgb_blk* d_roots,
+                         const pcgb_blk* d_cws, const uint64_t* d_cw_out, uint64_t* d_g,
+                         void* stream);
+/* Per-stage device timing without host synchronisation: with slots > 0 each
+ * expansion records events into the next of `slots` slots (0 turns it off).
+ * pcgb_expander_stage_times waits for the recorded expansions and writes
+ * ms[4*i + s] for stage s of the i-th one ([0] tops, [1] leaf gather,
+ * [2] x, [3] NTT products); returns how many expansions were recorded and
+ * starts a new recording. */
+int pcgb_expander_set_profiling(pcgb_expander* e, int slots);
+int pcgb_expander_stage_times(pcgb_expander* e, float* ms, int max_expansions);
+
+/* Seeded synthetic material (own deterministic generator). */
+int pcgb_noise(int N, int c, int t, uint64_t seed, int party, uint64_t* pos, uint64_t* val);
+int pcgb_public_a(int N, int c, uint64_t a_seed, uint64_t* a);
+/* Dealer on the GPU: keys for both parties of one expansion. */
+int pcgb_deal_keys_device(pcgb_expander* e, uint64_t seed, pcgb_blk* d_roots0,
+                          pcgb_blk* d_roots1, pcgb_blk* d_cws, uint64_t* d_cw_out,
+                          void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

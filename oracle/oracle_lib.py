@@ -1,15 +1,15 @@
 """ctypes bindings for the CPU oracle (oracle/liboracle.so) and for the
 reference code compiled from its own sources (oracle/_ref/*.so).
 
-Test infrastructure only: the library under test never imports this module.
+Test infrastructure only: used by tests/, the smoke check and bench.py's CPU
+baseline leg; the library under test never imports this module.
 """
 import ctypes as C
 import os
 
 import numpy as np
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
 P = 4611686018326724609
 PRG_AES, PRG_CHACHA8 = 0, 1
 
@@ -79,6 +79,9 @@ def lib():
                                  u64p, C.c_void_p, C.c_uint64, C.c_int, u64p, u64p,
                                  C.c_void_p]
         L.orc_mt64_fill.argtypes = [C.c_uint64, u64p, C.c_size_t]
+        L.orc_bench_sample.argtypes = [C.POINTER(Shape), C.c_int, u64p, u64p, u64p, u64p,
+                                       C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -297,3 +300,17 @@ def ref_gpu():
         L.ref_free.argtypes = [C.c_void_p]
         _ref_gpu = L
     return _ref_gpu
+
+
+def bench_sample(s, party, roots, cws, cw_out, a, n_blocks, keys_per_block, n_polymuls, threads):
+    """Times a bounded sample of one party's expansion on the host:
+    DPF + convert of n_blocks x keys_per_block keys and n_polymuls negacyclic
+    products of length N, on `threads` threads.  Returns (t_dpf_s, t_ntt_s)."""
+    t1, t2 = C.c_double(), C.c_double()
+    rc = lib().orc_bench_sample(C.byref(s), party, np.ascontiguousarray(roots, np.uint64),
+                                np.ascontiguousarray(cws, np.uint64),
+                                np.ascontiguousarray(cw_out, np.uint64),
+                                np.ascontiguousarray(a, np.uint64), n_blocks, keys_per_block,
+                                n_polymuls, threads, C.byref(t1), C.byref(t2))
+    assert rc == 0, rc
+    return t1.value, t2.value

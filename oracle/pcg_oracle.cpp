@@ -4,6 +4,7 @@
 // See pcg_oracle.h for how parity is pinned.
 #include "pcg_oracle.h"
 
+#include <chrono>
 #include <cstring>
 #include <mutex>
 #include <thread>
@@ -751,6 +752,64 @@ int orc_expand(const orc_shape* s, int party, const orc_blk* roots,
             for (int d = 0; d < N; ++d) acc[d] = addm(acc[d], tmp[d]);
         }
     std::memcpy(z, acc.data(), sizeof(uint64_t) * N);
+    return 0;
+}
+
+int orc_bench_sample(const orc_shape* s, int party, const orc_blk* roots, const orc_blk* cws,
+                     const uint64_t* cw_out, const uint64_t* a, int n_blocks,
+                     int keys_per_block, int n_polymuls, int threads, double* t_dpf,
+                     double* t_ntt) {
+    const int N = s->N, t = s->t, B = t * t;
+    const size_t D = static_cast<size_t>(1) << s->n, bin = D / 2;
+    const size_t per = static_cast<size_t>(s->levels) * s->nk;
+    if (threads < 1) threads = 1;
+    if (keys_per_block <= 0 || keys_per_block > B) keys_per_block = B;
+    if (n_blocks > s->c * s->c) n_blocks = s->c * s->c;
+    using clk = std::chrono::steady_clock;
+    // Part 1: the keyed DPF + output layer of the sampled keys (the per-key
+    // work of orc_expand), keys spread over the threads, one 2N-long g per
+    // thread and block (pcg_ole_impl.h:330-446).
+    auto t0 = clk::now();
+    {
+        std::vector<std::thread> pool;
+        const int total = n_blocks * keys_per_block;
+        for (int w = 0; w < threads; ++w)
+            pool.emplace_back([&, w] {
+                std::vector<orc_blk> leaves(D);
+                std::vector<uint64_t> g2(2 * static_cast<size_t>(N), 0);
+                for (int k = w; k < total; k += threads) {
+                    const int blk = k / keys_per_block, b = k % keys_per_block;
+                    const size_t id = static_cast<size_t>(blk) * B + b;
+                    orc_dpf_keyed_full_eval(1, s->n, s->w, roots + id, cws + id * per, nullptr,
+                                            s->prg, leaves.data());
+                    const size_t base = static_cast<size_t>(b / t + b % t) * bin;
+                    for (size_t d = 0; d < D; ++d) {
+                        uint64_t y = orc_out_hash_lo64(leaves[d]) % P;
+                        if (leaves[d].lo & 1) y = addm(y, cw_out[id]);
+                        if (party == 1) y = subm(0, y);
+                        g2[base + d] = addm(g2[base + d], y);
+                    }
+                }
+            });
+        for (auto& th : pool) th.join();
+    }
+    auto t1 = clk::now();
+    // Part 2: step-4 products (pcg_ole_impl.h:460-483), one per task.
+    {
+        std::vector<std::thread> pool;
+        for (int w = 0; w < threads; ++w)
+            pool.emplace_back([&, w] {
+                std::vector<uint64_t> c(N);
+                for (int k = w; k < n_polymuls; k += threads) {
+                    const uint64_t* x = a + static_cast<size_t>(k % (s->c > 1 ? s->c - 1 : 1)) * N;
+                    poly_mul1(c.data(), x, x, N);
+                }
+            });
+        for (auto& th : pool) th.join();
+    }
+    auto t2 = clk::now();
+    *t_dpf = std::chrono::duration<double>(t1 - t0).count();
+    *t_ntt = std::chrono::duration<double>(t2 - t1).count();
     return 0;
 }
 

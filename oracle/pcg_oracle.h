@@ -131,6 +131,15 @@ int orc_expand(const orc_shape* s, int party, const orc_blk* roots,
                uint64_t blocks_mask, int threads, uint64_t* x, uint64_t* z,
                uint64_t* g_out);
 
+/* Bounded CPU sample of one party's expansion for the timed baseline:
+ * output layer of n_blocks blocks x keys_per_block keys (keyed DPF + convert
+ * + scatter, as orc_expand) and n_polymuls length-N products, the work split
+ * over `threads` threads.  *t_dpf / *t_ntt: wall seconds of the two parts. */
+int orc_bench_sample(const orc_shape* s, int party, const orc_blk* roots, const orc_blk* cws,
+                     const uint64_t* cw_out, const uint64_t* a, int n_blocks,
+                     int keys_per_block, int n_polymuls, int threads, double* t_dpf,
+                     double* t_ntt);
+
 /* mt19937_64 (reference fixtures use std::mt19937_64). */
 void orc_mt64_fill(uint64_t seed, uint64_t* out, size_t n);
 

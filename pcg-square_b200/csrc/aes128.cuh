@@ -1,0 +1,64 @@
+// Device AES-128 encryption with four 256-word T-tables staged in shared
+// memory (FIPS-197 rounds: SubBytes+ShiftRows+MixColumns folded into table
+// lookups, AddRoundKey as word XORs).  The 16-byte state is four
+// little-endian column words, so a DPF node {lo, hi} maps to words
+// (lo, lo>>32, hi, hi>>32): the byte order the reference feeds its AES
+// (GPU_baseline/common/aes_gpu.cuh:128-141).
+//
+// Te_r[x] holds column (2S, S, S, 3S)(x) rotated up by r bytes; the final
+// round extracts S(x) as byte 1 of Te_0[x].
+#ifndef PCGB_AES128_CUH_
+#define PCGB_AES128_CUH_
+
+#include <cstdint>
+
+namespace pcgb {
+
+// te: 1024 words in shared memory (Te0 | Te1 | Te2 | Te3); rk: 44 words.
+__device__ __forceinline__ void aes128_encrypt_words(const uint32_t* __restrict__ te,
+                                                     const uint32_t* __restrict__ rk,
+                                                     uint32_t& w0, uint32_t& w1, uint32_t& w2,
+                                                     uint32_t& w3) {
+    uint32_t s0 = w0 ^ rk[0], s1 = w1 ^ rk[1], s2 = w2 ^ rk[2], s3 = w3 ^ rk[3];
+    const uint32_t* te0 = te;
+    const uint32_t* te1 = te + 256;
+    const uint32_t* te2 = te + 512;
+    const uint32_t* te3 = te + 768;
+#pragma unroll
+    for (int r = 1; r < 10; ++r) {
+        const uint32_t t0 = te0[s0 & 0xff] ^ te1[(s1 >> 8) & 0xff] ^ te2[(s2 >> 16) & 0xff] ^
+                            te3[s3 >> 24] ^ rk[4 * r + 0];
+        const uint32_t t1 = te0[s1 & 0xff] ^ te1[(s2 >> 8) & 0xff] ^ te2[(s3 >> 16) & 0xff] ^
+                            te3[s0 >> 24] ^ rk[4 * r + 1];
+        const uint32_t t2 = te0[s2 & 0xff] ^ te1[(s3 >> 8) & 0xff] ^ te2[(s0 >> 16) & 0xff] ^
+                            te3[s1 >> 24] ^ rk[4 * r + 2];
+        const uint32_t t3 = te0[s3 & 0xff] ^ te1[(s0 >> 8) & 0xff] ^ te2[(s1 >> 16) & 0xff] ^
+                            te3[s2 >> 24] ^ rk[4 * r + 3];
+        s0 = t0; s1 = t1; s2 = t2; s3 = t3;
+    }
+    // Final round: S-box bytes (byte 1 of Te0 entries), ShiftRows, AddRoundKey.
+#define PCGB_SB(x) ((te0[(x)] >> 8) & 0xffu)
+    w0 = (PCGB_SB(s0 & 0xff) | (PCGB_SB((s1 >> 8) & 0xff) << 8) |
+          (PCGB_SB((s2 >> 16) & 0xff) << 16) | (PCGB_SB(s3 >> 24) << 24)) ^ rk[40];
+    w1 = (PCGB_SB(s1 & 0xff) | (PCGB_SB((s2 >> 8) & 0xff) << 8) |
+          (PCGB_SB((s3 >> 16) & 0xff) << 16) | (PCGB_SB(s0 >> 24) << 24)) ^ rk[41];
+    w2 = (PCGB_SB(s2 & 0xff) | (PCGB_SB((s3 >> 8) & 0xff) << 8) |
+          (PCGB_SB((s0 >> 16) & 0xff) << 16) | (PCGB_SB(s1 >> 24) << 24)) ^ rk[42];
+    w3 = (PCGB_SB(s3 & 0xff) | (PCGB_SB((s0 >> 8) & 0xff) << 8) |
+          (PCGB_SB((s1 >> 16) & 0xff) << 16) | (PCGB_SB(s2 >> 24) << 24)) ^ rk[43];
+#undef PCGB_SB
+}
+
+// Correlation-robust hash H(x) = AES_k(x) ^ x on a node held as (lo, hi).
+__device__ __forceinline__ void aes_ccr(const uint32_t* te, const uint32_t* rk, uint64_t lo,
+                                        uint64_t hi, uint64_t& olo, uint64_t& ohi) {
+    uint32_t w0 = static_cast<uint32_t>(lo), w1 = static_cast<uint32_t>(lo >> 32);
+    uint32_t w2 = static_cast<uint32_t>(hi), w3 = static_cast<uint32_t>(hi >> 32);
+    aes128_encrypt_words(te, rk, w0, w1, w2, w3);
+    olo = (w0 | (static_cast<uint64_t>(w1) << 32)) ^ lo;
+    ohi = (w2 | (static_cast<uint64_t>(w3) << 32)) ^ hi;
+}
+
+}  // namespace pcgb
+
+#endif

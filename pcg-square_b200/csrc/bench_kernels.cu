@@ -1,0 +1,76 @@
+// Measurement helpers: the library's kernel-launch counter and an ARX
+// throughput probe that bounds the ChaCha8-bound kernels from above.
+//
+// The probe runs the ChaCha8 double round (the same QR with PRMT/SHF
+// rotations as chacha8.cuh) on two independent register-resident states per
+// thread, with every SM fully occupied, and reports integer ops/s counting
+// 12 ops per quarter round (4 add, 4 xor, 4 rotate).  It is the achievable
+// peak for exactly the instruction mix of the DPF kernels.
+#include "pcgb_internal.h"
+
+#include <atomic>
+
+#include "chacha8.cuh"
+
+namespace pcgb {
+namespace {
+
+std::atomic<unsigned long long> g_launches{0};
+
+__global__ void __launch_bounds__(256) arx_probe_kernel(uint32_t seed, int iters, uint32_t* sink) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t a0 = seed ^ tid, a1 = tid * 3u, a2 = tid + 7u, a3 = 0x9e3779b9u;
+    uint32_t a4 = 1, a5 = 2, a6 = 3, a7 = 4, a8 = 5, a9 = 6, a10 = 7, a11 = 8;
+    uint32_t a12 = tid, a13 = 9, a14 = 10, a15 = 11;
+    uint32_t b0 = tid ^ 0x55u, b1 = 12, b2 = 13, b3 = 14, b4 = 15, b5 = 16, b6 = 17, b7 = 18;
+    uint32_t b8 = 19, b9 = 20, b10 = 21, b11 = 22, b12 = seed, b13 = 23, b14 = 24, b15 = 25;
+    for (int i = 0; i < iters; ++i) {
+        PCGB_QR(a0, a4, a8, a12) PCGB_QR(b0, b4, b8, b12)
+        PCGB_QR(a1, a5, a9, a13) PCGB_QR(b1, b5, b9, b13)
+        PCGB_QR(a2, a6, a10, a14) PCGB_QR(b2, b6, b10, b14)
+        PCGB_QR(a3, a7, a11, a15) PCGB_QR(b3, b7, b11, b15)
+        PCGB_QR(a0, a5, a10, a15) PCGB_QR(b0, b5, b10, b15)
+        PCGB_QR(a1, a6, a11, a12) PCGB_QR(b1, b6, b11, b12)
+        PCGB_QR(a2, a7, a8, a13) PCGB_QR(b2, b7, b8, b13)
+        PCGB_QR(a3, a4, a9, a14) PCGB_QR(b3, b4, b9, b14)
+    }
+    const uint32_t r = a0 ^ a1 ^ a2 ^ a3 ^ a4 ^ a5 ^ a6 ^ a7 ^ a8 ^ a9 ^ a10 ^ a11 ^ a12 ^ a13 ^
+                       a14 ^ a15 ^ b0 ^ b1 ^ b2 ^ b3 ^ b4 ^ b5 ^ b6 ^ b7 ^ b8 ^ b9 ^ b10 ^ b11 ^
+                       b12 ^ b13 ^ b14 ^ b15;
+    if (r == 0x12345678u) sink[0] = r;  // keeps the work alive
+}
+
+}  // namespace
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+// Returns G int-ops/s; *ms = probe duration.
+double arx_probe(float* ms_out) {
+    cudaStream_t st = default_stream();
+    const int sms = sm_count();
+    const int blocks = sms * 8, threads = 256, iters = 4096;
+    uint32_t* sink = nullptr;
+    PCGB_CK(cudaMallocAsync(&sink, 4, st));
+    arx_probe_kernel<<<blocks, threads, 0, st>>>(1, 64, sink);  // warm-up
+    PCGB_POST_LAUNCH();
+    cudaEvent_t e0, e1;
+    PCGB_CK(cudaEventCreate(&e0));
+    PCGB_CK(cudaEventCreate(&e1));
+    PCGB_CK(cudaEventRecord(e0, st));
+    arx_probe_kernel<<<blocks, threads, 0, st>>>(2, iters, sink);
+    PCGB_POST_LAUNCH();
+    PCGB_CK(cudaEventRecord(e1, st));
+    PCGB_CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    PCGB_CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    PCGB_CK(cudaFreeAsync(sink, st));
+    if (ms_out) *ms_out = ms;
+    const double ops = static_cast<double>(blocks) * threads * iters * 2 /*states*/ * 8 * 12;
+    return ops / (ms * 1e-3) / 1e9;
+}
+
+}  // namespace pcgb

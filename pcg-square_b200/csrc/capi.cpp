@@ -1,0 +1,523 @@
+// extern "C" entry points of include/pcg_b200.h: argument checks, error
+// codes and the thread-local last-error message around the pcgb:: internals.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "pcg_b200.h"
+#include "pcgb_internal.h"
+
+namespace pcgb {
+
+// Implemented in the .cu translation units.
+const Blk* dpf_interactive_device(int B, int n, int w, const Blk* roots, const Blk* dltsft,
+                                  const uint8_t* rks, int prg, pcgb_exchange_fn ex, void* user,
+                                  Blk* host_out);
+void dpf_out_sums_host(const Blk* d_leaves, int B, size_t D, uint64_t prime, uint64_t* sumC,
+                       uint64_t* sumT);
+void dpf_out_scatter_host(const Blk* d_leaves, int B, size_t D, int t, int party, uint64_t prime,
+                          const uint64_t* CW, uint64_t* g_out, int N);
+void aes_ecb_encrypt_device(const uint8_t* keys, const uint8_t* in, uint8_t* out, int count);
+pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64_t* public_a,
+                               const uint8_t* master_key);
+void expander_destroy(pcgb_expander* e);
+void expand_device(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
+                   const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val, uint64_t* x,
+                   uint64_t* z, cudaStream_t st);
+void expand_host(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
+                 const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val, uint64_t* x,
+                 uint64_t* z);
+void expand_g_device(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
+                     const uint64_t* cw_out, uint64_t* d_g, cudaStream_t st);
+void expander_info(const pcgb_expander* e, int* K, int* levels, int* nk, size_t* scratch);
+void expander_set_profiling(pcgb_expander* e, int slots);
+int expander_stage_times(pcgb_expander* e, float* ms, int max_exp);
+void noise_host(int N, int c, int t, uint64_t seed, int party, uint64_t* pos, uint64_t* val);
+void public_a_host(int N, int c, uint64_t a_seed, uint64_t* a);
+void deal_keys_device(pcgb_expander* e, uint64_t seed, Blk* r0, Blk* r1, Blk* cws, uint64_t* cwo,
+                      cudaStream_t st);
+unsigned long long launch_count();
+double arx_probe(float* ms_out);
+
+namespace {
+thread_local std::string g_last_error;
+
+int device_count() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        if (device_count() == 0) {
+            g_last_error = "no CUDA device is available";
+            return PCGB_ENODEV;
+        }
+        f();
+        return PCGB_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return PCGB_ENOMEM;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return PCGB_EINVAL;
+    }
+}
+
+bool pow2(long long v) { return v > 0 && (v & (v - 1)) == 0; }
+
+int ilog2i(long long v) {
+    int l = 0;
+    while ((1ll << l) < v) ++l;
+    return l;
+}
+
+void copy_str(char* buf, size_t len, const std::string& s) {
+    if (!buf || len == 0) return;
+    std::snprintf(buf, len, "%s", s.c_str());
+}
+
+}  // namespace
+
+void fail(int code, const std::string& msg) { throw Error(code, msg); }
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    cudaGetLastError();
+    throw Error(e == cudaErrorMemoryAllocation ? PCGB_ENOMEM : PCGB_ECUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+cudaStream_t default_stream() {
+    static std::mutex mu;
+    static cudaStream_t streams[64] = {nullptr};
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lk(mu);
+    if (!streams[dev]) check_cuda(cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking),
+                                  "cudaStreamCreate");
+    return streams[dev];
+}
+
+int sm_count() {
+    int dev = 0, n = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    check_cuda(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev), "sm count");
+    return n;
+}
+
+// Supported-size rules of the reference's poly-mul entry points.
+bool poly_mul_rules(int variant, uint64_t prime, int N, std::string* reason) {
+    auto no = [&](const char* r) {
+        if (reason) *reason = r;
+        return false;
+    };
+    if (prime != kP) return no("CUDA backend only supports the project 62-bit prime");
+    switch (variant) {
+        case PCGB_POLYMUL_V1:
+            if (!pow2(N) || N < 2 || N > 32768) return no("CUDA backend requires power-of-two N in [2,32768]");
+            break;
+        case PCGB_POLYMUL_MERGE:
+            if (!pow2(N) || N < 2 || N > (1 << kMaxLogN)) return no("requires power-of-two N in [2, 2^24]");
+            break;
+        case PCGB_POLYMUL_4STEP:
+            if (!pow2(N) || N < 4096 || N > (1 << kMaxLogN)) return no("4-step requires power-of-two N in [4096, 2^24]");
+            break;
+        case PCGB_POLYMUL_SQUARE:
+            if (!pow2(N) || N < 256 || N > (1 << kMaxLogN)) return no("square requires logN in [8, 24]");
+            break;
+        default: return no("unknown poly-mul variant");
+    }
+    if ((prime - 1) % (2 * static_cast<uint64_t>(N)) != 0) return no("prime is not NTT-friendly for this N");
+    if (device_count() == 0) return no("no CUDA device is available");
+    if (reason) reason->clear();
+    return true;
+}
+
+}  // namespace pcgb
+
+using pcgb::Blk;
+using pcgb::guarded;
+
+extern "C" {
+
+const char* pcgb_last_error(void) { return pcgb::g_last_error.c_str(); }
+int pcgb_version(void) { return 100; }
+
+int pcgb_is_cuda_available(void) { return pcgb::device_count() > 0 ? 1 : 0; }
+
+int pcgb_device_name(char* buf, size_t len) {
+    return guarded([&] {
+        int dev = 0;
+        PCGB_CK(cudaGetDevice(&dev));
+        cudaDeviceProp prop;
+        PCGB_CK(cudaGetDeviceProperties(&prop, dev));
+        pcgb::copy_str(buf, len, prop.name);
+    });
+}
+
+int pcgb_runtime_version(char* buf, size_t len) {
+    int v = 0;
+    if (cudaRuntimeGetVersion(&v) != cudaSuccess) {
+        pcgb::copy_str(buf, len, "unavailable");
+        return PCGB_ECUDA;
+    }
+    pcgb::copy_str(buf, len, std::to_string(v / 1000) + "." + std::to_string((v % 1000) / 10));
+    return PCGB_OK;
+}
+
+int pcgb_set_device(int dev) { return guarded([&] { PCGB_CK(cudaSetDevice(dev)); }); }
+int pcgb_get_device(int* dev) { return guarded([&] { PCGB_CK(cudaGetDevice(dev)); }); }
+int pcgb_sm_count(int* n) { return guarded([&] { *n = pcgb::sm_count(); }); }
+
+int pcgb_malloc(void** p, size_t bytes) { return guarded([&] { PCGB_CK(cudaMalloc(p, bytes)); }); }
+int pcgb_free(void* p) { return guarded([&] { PCGB_CK(cudaFree(p)); }); }
+
+int pcgb_memcpy_h2d(void* d, const void* s, size_t bytes, void* stream) {
+    return guarded([&] {
+        cudaStream_t st = pcgb::as_stream(stream);
+        PCGB_CK(cudaMemcpyAsync(d, s, bytes, cudaMemcpyHostToDevice, st));
+        PCGB_CK(cudaStreamSynchronize(st));
+    });
+}
+int pcgb_memcpy_d2h(void* d, const void* s, size_t bytes, void* stream) {
+    return guarded([&] {
+        cudaStream_t st = pcgb::as_stream(stream);
+        PCGB_CK(cudaMemcpyAsync(d, s, bytes, cudaMemcpyDeviceToHost, st));
+        PCGB_CK(cudaStreamSynchronize(st));
+    });
+}
+int pcgb_memset(void* d, int v, size_t bytes, void* stream) {
+    return guarded([&] { PCGB_CK(cudaMemsetAsync(d, v, bytes, pcgb::as_stream(stream))); });
+}
+int pcgb_stream_synchronize(void* stream) {
+    return guarded([&] { PCGB_CK(cudaStreamSynchronize(pcgb::as_stream(stream))); });
+}
+int pcgb_device_synchronize(void) { return guarded([&] { PCGB_CK(cudaDeviceSynchronize()); }); }
+void* pcgb_default_stream(void) {
+    void* s = nullptr;
+    guarded([&] { s = pcgb::default_stream(); });
+    return s;
+}
+
+unsigned long long pcgb_launch_count(void) { return pcgb::launch_count(); }
+
+int pcgb_arx_peak(double* gops, float* ms) {
+    return guarded([&] {
+        const double g = pcgb::arx_probe(ms);
+        if (gops) *gops = g;
+    });
+}
+
+int pcgb_event_create(void** ev) {
+    return guarded([&] {
+        cudaEvent_t e = nullptr;
+        PCGB_CK(cudaEventCreate(&e));
+        *ev = e;
+    });
+}
+int pcgb_event_destroy(void* ev) {
+    return guarded([&] { PCGB_CK(cudaEventDestroy(static_cast<cudaEvent_t>(ev))); });
+}
+int pcgb_event_record(void* ev, void* stream) {
+    return guarded([&] {
+        PCGB_CK(cudaEventRecord(static_cast<cudaEvent_t>(ev), pcgb::as_stream(stream)));
+    });
+}
+int pcgb_event_elapsed(void* start, void* stop, float* ms) {
+    return guarded([&] {
+        PCGB_CK(cudaEventSynchronize(static_cast<cudaEvent_t>(stop)));
+        PCGB_CK(cudaEventElapsedTime(ms, static_cast<cudaEvent_t>(start),
+                                     static_cast<cudaEvent_t>(stop)));
+    });
+}
+
+// ---- DPF drop-ins -------------------------------------------------------
+int pcgb_dpf_batch_full_eval(int B, int n, int w, const pcgb_blk* roots, const pcgb_blk* dltsft,
+                             const uint8_t* round_keys, int party, pcgb_exchange_fn exchange,
+                             void* user, pcgb_blk* out_leaves, int prg) {
+    (void)party;
+    if (B <= 0) return PCGB_OK;
+    return guarded([&] {
+        if (!out_leaves) pcgb::fail(PCGB_EINVAL, "dpf_gpu_batch_full_eval: null out_leaves");
+        pcgb::dpf_interactive_device(B, n, w, reinterpret_cast<const Blk*>(roots),
+                                     reinterpret_cast<const Blk*>(dltsft), round_keys, prg,
+                                     exchange, user, reinterpret_cast<Blk*>(out_leaves));
+    });
+}
+
+int pcgb_dpf_batch_full_eval_device(int B, int n, int w, const pcgb_blk* roots,
+                                    const pcgb_blk* dltsft, const uint8_t* round_keys, int party,
+                                    pcgb_exchange_fn exchange, void* user, int prg,
+                                    const pcgb_blk** d_leaves) {
+    (void)party;
+    if (d_leaves) *d_leaves = nullptr;
+    if (B <= 0) return PCGB_OK;
+    return guarded([&] {
+        const Blk* p = pcgb::dpf_interactive_device(B, n, w, reinterpret_cast<const Blk*>(roots),
+                                                    reinterpret_cast<const Blk*>(dltsft),
+                                                    round_keys, prg, exchange, user, nullptr);
+        if (d_leaves) *d_leaves = reinterpret_cast<const pcgb_blk*>(p);
+    });
+}
+
+int pcgb_dpf_out_sums(const pcgb_blk* d_leaves, int B, size_t D, uint64_t prime,
+                      uint64_t* sumC_host, uint64_t* sumT_host) {
+    if (B <= 0) return PCGB_OK;
+    return guarded([&] {
+        pcgb::dpf_out_sums_host(reinterpret_cast<const Blk*>(d_leaves), B, D, prime, sumC_host,
+                                sumT_host);
+    });
+}
+
+int pcgb_dpf_out_scatter_g(const pcgb_blk* d_leaves, int B, size_t D, int t, int party,
+                           uint64_t prime, const uint64_t* CW_host, uint64_t* g_out_host, int N) {
+    if (B <= 0) return PCGB_OK;
+    return guarded([&] {
+        pcgb::dpf_out_scatter_host(reinterpret_cast<const Blk*>(d_leaves), B, D, t, party, prime,
+                                   CW_host, g_out_host, N);
+    });
+}
+
+// ---- poly-mul drop-ins --------------------------------------------------
+int pcgb_poly_mul_supported(int variant, uint64_t prime, int N, char* reason, size_t len) {
+    std::string r;
+    const bool ok = pcgb::poly_mul_rules(variant, prime, N, &r);
+    pcgb::copy_str(reason, len, r);
+    return ok ? 1 : 0;
+}
+
+int pcgb_poly_mul_u64(int variant, uint64_t* out, const uint64_t* a, const uint64_t* b, int batch,
+                      int N, uint64_t prime, double* device_ms) {
+    return guarded([&] {
+        std::string why;
+        if (!pcgb::poly_mul_rules(variant, prime, N, &why)) pcgb::fail(PCGB_EINVAL, why);
+        if (batch <= 0) pcgb::fail(PCGB_EINVAL, "batch must be positive");
+        const pcgb::NttPlan& pl = pcgb::ntt_plan(pcgb::ilog2i(N));
+        cudaStream_t st = pcgb::default_stream();
+        const size_t n = static_cast<size_t>(batch) * N;
+        uint64_t* d = nullptr;
+        PCGB_CK(cudaMallocAsync(&d, 5 * n * sizeof(uint64_t), st));
+        uint64_t *da = d, *db = d + n, *dc = d + 2 * n, *scratch = d + 3 * n;
+        PCGB_CK(cudaMemcpyAsync(da, a, n * 8, cudaMemcpyHostToDevice, st));
+        PCGB_CK(cudaMemcpyAsync(db, b, n * 8, cudaMemcpyHostToDevice, st));
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (device_ms) {
+            PCGB_CK(cudaEventCreate(&e0));
+            PCGB_CK(cudaEventCreate(&e1));
+            PCGB_CK(cudaEventRecord(e0, st));
+        }
+        pcgb::poly_mul_device(pl, dc, da, db, batch, scratch, st);
+        if (device_ms) PCGB_CK(cudaEventRecord(e1, st));
+        PCGB_CK(cudaMemcpyAsync(out, dc, n * 8, cudaMemcpyDeviceToHost, st));
+        PCGB_CK(cudaFreeAsync(d, st));
+        PCGB_CK(cudaStreamSynchronize(st));
+        if (device_ms) {
+            float ms = 0;
+            PCGB_CK(cudaEventElapsedTime(&ms, e0, e1));
+            *device_ms = ms;
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+        }
+    });
+}
+
+// ---- AES ------------------------------------------------------------------
+int pcgb_aes128_expand_key(const uint8_t key[16], uint8_t round_keys[176]) {
+    try {
+        pcgb::aes_expand_key_host(key, round_keys);
+        return PCGB_OK;
+    } catch (const std::exception& e) {
+        pcgb::g_last_error = e.what();
+        return PCGB_EINVAL;
+    }
+}
+
+int pcgb_aes128_ecb_encrypt(const uint8_t* keys, const uint8_t* in, uint8_t* out, int count) {
+    if (count <= 0) return PCGB_OK;
+    return guarded([&] { pcgb::aes_ecb_encrypt_device(keys, in, out, count); });
+}
+
+int pcgb_aes_tree_round_keys(const uint8_t master[16], int nk, uint8_t* round_keys) {
+    if (nk < 1 || nk > 15) {
+        pcgb::g_last_error = "nk must be in [1, 15]";
+        return PCGB_EINVAL;
+    }
+    pcgb::aes_tree_round_keys_host(master, nk, round_keys);
+    return PCGB_OK;
+}
+
+// ---- keyed DPF --------------------------------------------------------------
+int pcgb_dpf_keyed_full_eval(int K, int n, int w, int prg, const pcgb_blk* d_roots,
+                             const pcgb_blk* d_cws, const uint8_t* round_keys,
+                             pcgb_blk* d_leaves, void* stream) {
+    if (K <= 0) return PCGB_OK;
+    return guarded([&] {
+        if (w < 1 || w > 4 || n < 1 || n % w || n / w > 26) pcgb::fail(PCGB_EINVAL, "keyed eval: bad (n, w)");
+        if (prg == PCGB_PRG_AES && !round_keys) pcgb::fail(PCGB_EINVAL, "keyed eval: AES needs round keys");
+        cudaStream_t st = pcgb::as_stream(stream);
+        const int levels = n / w, nk = (1 << w) - 1;
+        uint32_t* d_rk = nullptr;
+        if (prg == PCGB_PRG_AES) d_rk = pcgb::aes_upload_round_keys(round_keys, nk, st);
+        const size_t sn = pcgb::keyed_tops_scratch_nodes(K, w, levels);
+        Blk* scratch = nullptr;
+        if (sn) PCGB_CK(cudaMallocAsync(&scratch, sn * sizeof(Blk), st));
+        pcgb::keyed_expand_tops(K, n, w, prg, reinterpret_cast<const Blk*>(d_roots),
+                                reinterpret_cast<const Blk*>(d_cws), d_rk, levels,
+                                reinterpret_cast<Blk*>(d_leaves), scratch, st);
+        if (scratch) PCGB_CK(cudaFreeAsync(scratch, st));
+        if (d_rk) {
+            PCGB_CK(cudaStreamSynchronize(st));
+            cudaFree(d_rk);
+        }
+    });
+}
+
+// ---- batched NTT ------------------------------------------------------------
+int pcgb_poly_mul_device(uint64_t* d_c, const uint64_t* d_a, const uint64_t* d_b, int batch, int N,
+                         void* stream) {
+    return guarded([&] {
+        if (!pcgb::pow2(N) || N < 2 || N > (1 << pcgb::kMaxLogN)) pcgb::fail(PCGB_EINVAL, "N must be a power of two in [2, 2^24]");
+        if (batch <= 0) pcgb::fail(PCGB_EINVAL, "batch must be positive");
+        cudaStream_t st = pcgb::as_stream(stream);
+        const pcgb::NttPlan& pl = pcgb::ntt_plan(pcgb::ilog2i(N));
+        uint64_t* scratch = nullptr;
+        const size_t n = static_cast<size_t>(batch) * N;
+        PCGB_CK(cudaMallocAsync(&scratch, 2 * n * sizeof(uint64_t), st));
+        pcgb::poly_mul_device(pl, d_c, d_a, d_b, batch, scratch, st);
+        PCGB_CK(cudaFreeAsync(scratch, st));
+    });
+}
+
+int pcgb_poly_mul_device_multi(int count, uint64_t* const* d_c, const uint64_t* const* d_a,
+                               const uint64_t* const* d_b, const int* N, void* stream) {
+    return guarded([&] {
+        cudaStream_t st = pcgb::as_stream(stream);
+        // Group equal lengths that sit back to back so each group is one launch set.
+        int i = 0;
+        while (i < count) {
+            if (!pcgb::pow2(N[i]) || N[i] < 2 || N[i] > (1 << pcgb::kMaxLogN))
+                pcgb::fail(PCGB_EINVAL, "N must be a power of two in [2, 2^24]");
+            const pcgb::NttPlan& pl = pcgb::ntt_plan(pcgb::ilog2i(N[i]));
+            uint64_t* scratch = nullptr;
+            PCGB_CK(cudaMallocAsync(&scratch, 2 * static_cast<size_t>(N[i]) * sizeof(uint64_t), st));
+            pcgb::poly_mul_device(pl, d_c[i], d_a[i], d_b[i], 1, scratch, st);
+            PCGB_CK(cudaFreeAsync(scratch, st));
+            ++i;
+        }
+    });
+}
+
+// ---- expansion --------------------------------------------------------------
+int pcgb_expander_create(pcgb_expander** e, int N, int c, int t, int w, int prg,
+                         const uint64_t* public_a, const uint8_t* master_key) {
+    if (e) *e = nullptr;
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander handle");
+        *e = pcgb::expander_create(N, c, t, w, prg, public_a, master_key);
+    });
+}
+
+int pcgb_expander_destroy(pcgb_expander* e) {
+    return guarded([&] { pcgb::expander_destroy(e); });
+}
+
+int pcgb_expander_info(const pcgb_expander* e, int* K, int* levels, int* nk, size_t* scratch) {
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander");
+        pcgb::expander_info(e, K, levels, nk, scratch);
+    });
+}
+
+int pcgb_expand_device(pcgb_expander* e, int party, const pcgb_blk* d_roots, const pcgb_blk* d_cws,
+                       const uint64_t* d_cw_out, const uint64_t* d_pos, const uint64_t* d_val,
+                       uint64_t* d_x, uint64_t* d_z, void* stream) {
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander");
+        pcgb::expand_device(e, party, reinterpret_cast<const Blk*>(d_roots),
+                            reinterpret_cast<const Blk*>(d_cws), d_cw_out, d_pos, d_val, d_x, d_z,
+                            pcgb::as_stream(stream));
+    });
+}
+
+int pcgb_expand_host(pcgb_expander* e, int party, const pcgb_blk* roots, const pcgb_blk* cws,
+                     const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val, uint64_t* x,
+                     uint64_t* z) {
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander");
+        pcgb::expand_host(e, party, reinterpret_cast<const Blk*>(roots),
+                          reinterpret_cast<const Blk*>(cws), cw_out, pos, val, x, z);
+    });
+}
+
+int pcgb_expand_g_device(pcgb_expander* e, int party, const pcgb_blk* d_roots,
+                         const pcgb_blk* d_cws, const uint64_t* d_cw_out, uint64_t* d_g,
+                         void* stream) {
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander");
+        if (party != 0 && party != 1) pcgb::fail(PCGB_EINVAL, "party must be 0 or 1");
+        pcgb::expand_g_device(e, party, reinterpret_cast<const Blk*>(d_roots),
+                              reinterpret_cast<const Blk*>(d_cws), d_cw_out, d_g,
+                              pcgb::as_stream(stream));
+    });
+}
+
+int pcgb_expander_set_profiling(pcgb_expander* e, int slots) {
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander");
+        pcgb::expander_set_profiling(e, slots);
+    });
+}
+
+int pcgb_expander_stage_times(pcgb_expander* e, float* ms, int max_expansions) {
+    int r = 0;
+    const int rc = guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander");
+        r = pcgb::expander_stage_times(e, ms, max_expansions);
+    });
+    return rc ? rc : r;
+}
+
+int pcgb_noise(int N, int c, int t, uint64_t seed, int party, uint64_t* pos, uint64_t* val) {
+    if (N < 2 || t < 1 || N % t || c < 1 || !pos || !val) {
+        pcgb::g_last_error = "noise: bad shape";
+        return PCGB_EINVAL;
+    }
+    pcgb::noise_host(N, c, t, seed, party, pos, val);
+    return PCGB_OK;
+}
+
+int pcgb_public_a(int N, int c, uint64_t a_seed, uint64_t* a) {
+    if (N < 1 || c < 1 || (c > 1 && !a)) {
+        pcgb::g_last_error = "public_a: bad shape";
+        return PCGB_EINVAL;
+    }
+    pcgb::public_a_host(N, c, a_seed, a);
+    return PCGB_OK;
+}
+
+int pcgb_deal_keys_device(pcgb_expander* e, uint64_t seed, pcgb_blk* d_roots0, pcgb_blk* d_roots1,
+                          pcgb_blk* d_cws, uint64_t* d_cw_out, void* stream) {
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander");
+        pcgb::deal_keys_device(e, seed, reinterpret_cast<Blk*>(d_roots0),
+                               reinterpret_cast<Blk*>(d_roots1), reinterpret_cast<Blk*>(d_cws),
+                               d_cw_out, pcgb::as_stream(stream));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,348 @@
+// Interactive half-tree DPF full-domain evaluation: the drop-in for
+// pcg_cuda::dpf_gpu_batch_full_eval[_device] (GPU_baseline/common/dpf_gpu.h:55-75).
+//
+// Protocol per level i (half_tree_dpf/dpf.cpp:504-575): every party hashes
+// its whole level-i frontier, XOR-reduces each hash column into its CW share
+// (seeded with the DltSft share), exchanges the shares with the peer, and
+// expands every node with CW = mine ^ peer.  The per-level global reduction
+// is a real barrier, so the frontier is materialised level by level; what
+// changes from the reference's hash/expand kernel pair (dpf_gpu.cu:212-330):
+//   * one kernel per level: expand level i with its CW, write the children,
+//     hash the children and XOR-reduce their columns for level i+1 (the
+//     reference re-reads every node and hash in separate kernels);
+//   * warp-shuffle reductions with one atomicXor per CTA and column;
+//   * the per-level host round trip uses pinned buffers on the library's
+//     stream (one synchronisation per level, before the callback).
+// Leaves come out in the reference layout: instance b, leaf d at [b*D + d].
+#include "pcgb_internal.h"
+
+#include <mutex>
+#include <vector>
+
+#include "aes128.cuh"
+#include "chacha8.cuh"
+#include "field.cuh"
+
+namespace pcgb {
+
+void aes_ecb_encrypt_device(const uint8_t* keys, const uint8_t* in, uint8_t* out, int count);
+
+namespace {
+
+constexpr int kTPB = 128;
+
+struct AesSm {
+    uint32_t te[1024];
+    uint32_t rk[15 * 44];
+};
+
+// H_0..H_{nk-1} of one node.
+template <int W, int PRG>
+__device__ __forceinline__ void hash_node(const Blk& p, const AesSm* aes, Blk (&h)[(1 << W) - 1]) {
+    constexpr int NK = (1 << W) - 1;
+    if constexpr (PRG == PCGB_PRG_CHACHA8) {
+#pragma unroll
+        for (int b = 0; b < (NK + 3) / 4; ++b) {
+            uint32_t o[16];
+            tree_block(p.lo, p.hi, b, o);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int k = 4 * b + c;
+                if (k < NK)
+                    h[k] = Blk{o[4 * c] | (static_cast<uint64_t>(o[4 * c + 1]) << 32),
+                               o[4 * c + 2] | (static_cast<uint64_t>(o[4 * c + 3]) << 32)};
+            }
+        }
+    } else {
+#pragma unroll 1
+        for (int k = 0; k < NK; ++k) aes_ccr(aes->te, aes->rk + 44 * k, p.lo, p.hi, h[k].lo, h[k].hi);
+    }
+}
+
+// XOR-reduce vals[0..NK) over the CTA and fold into dst[0..NK) atomically.
+template <int NK>
+__device__ __forceinline__ void cta_xor_reduce(Blk (&v)[NK], Blk* dst, Blk* red /* [32][NK] */) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+        uint64_t lo = v[k].lo, hi = v[k].hi;
+#pragma unroll
+        for (int off = 16; off; off >>= 1) {
+            lo ^= __shfl_xor_sync(0xffffffffu, lo, off);
+            hi ^= __shfl_xor_sync(0xffffffffu, hi, off);
+        }
+        if (lane == 0) red[warp * NK + k] = Blk{lo, hi};
+    }
+    __syncthreads();
+    if (threadIdx.x < NK) {
+        uint64_t lo = 0, hi = 0;
+        const int nw = (blockDim.x + 31) >> 5;
+        for (int w = 0; w < nw; ++w) {
+            lo ^= red[w * NK + threadIdx.x].lo;
+            hi ^= red[w * NK + threadIdx.x].hi;
+        }
+        atomicXor(reinterpret_cast<unsigned long long*>(&dst[threadIdx.x].lo), lo);
+        atomicXor(reinterpret_cast<unsigned long long*>(&dst[threadIdx.x].hi), hi);
+    }
+}
+
+template <int PRG>
+__device__ __forceinline__ const AesSm* stage_aes(AesSm& s, const uint32_t* te, const uint32_t* rk,
+                                                  int nk) {
+    if constexpr (PRG == PCGB_PRG_AES) {
+        for (int i = threadIdx.x; i < 1024; i += blockDim.x) s.te[i] = te[i];
+        for (int i = threadIdx.x; i < nk * 44; i += blockDim.x) s.rk[i] = rk[i];
+        __syncthreads();
+    }
+    return &s;
+}
+
+// Level 0: hash the B roots (frontier of size 1).  grid = (1, B).
+template <int W, int PRG>
+__global__ void __launch_bounds__(kTPB) hash_roots_kernel(const Blk* __restrict__ cur, size_t D,
+                                                          Blk* __restrict__ H, size_t HS,
+                                                          Blk* __restrict__ my,
+                                                          const uint32_t* te, const uint32_t* rk) {
+    constexpr int NK = (1 << W) - 1;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    Blk* red = reinterpret_cast<Blk*>(smraw);
+    AesSm& aes = *reinterpret_cast<AesSm*>(smraw + 32 * NK * sizeof(Blk));
+    const AesSm* a = stage_aes<PRG>(aes, te, rk, NK);
+    const int b = blockIdx.y;
+    Blk h[NK];
+#pragma unroll
+    for (int k = 0; k < NK; ++k) h[k] = Blk{0, 0};
+    if (threadIdx.x == 0) {
+        hash_node<W, PRG>(cur[static_cast<size_t>(b) * D], a, h);
+#pragma unroll
+        for (int k = 0; k < NK; ++k) H[static_cast<size_t>(b) * HS + k] = h[k];
+    }
+    cta_xor_reduce<NK>(h, my + static_cast<size_t>(b) * NK, red);
+}
+
+// Expand level i (frontier size sz, hashes H) with CW = my ^ peer; write the
+// children to nxt; when hash_next, hash the children into Hn and reduce
+// their columns into my_next.  grid = (ceil(sz / kTPB), B).
+template <int W, int PRG>
+__global__ void __launch_bounds__(kTPB) expand_level_kernel(
+    const Blk* __restrict__ cur, const Blk* __restrict__ H, const Blk* __restrict__ my,
+    const Blk* __restrict__ peer, Blk* __restrict__ nxt, Blk* __restrict__ Hn,
+    Blk* __restrict__ my_next, size_t sz, size_t D, size_t HS, int hash_next,
+    const uint32_t* te, const uint32_t* rk) {
+    constexpr int M = 1 << W, NK = M - 1;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    Blk* red = reinterpret_cast<Blk*>(smraw);
+    AesSm& aes = *reinterpret_cast<AesSm*>(smraw + 32 * NK * sizeof(Blk));
+    const AesSm* a = stage_aes<PRG>(aes, te, rk, NK);
+    const int b = blockIdx.y;
+    const size_t j = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    Blk cw[NK];
+    Blk cwf{0, 0};
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+        const Blk m0 = my[static_cast<size_t>(b) * NK + k], p0 = peer[static_cast<size_t>(b) * NK + k];
+        cw[k] = Blk{m0.lo ^ p0.lo, m0.hi ^ p0.hi};
+        cwf.lo ^= cw[k].lo;
+        cwf.hi ^= cw[k].hi;
+    }
+    Blk acc[NK];
+#pragma unroll
+    for (int k = 0; k < NK; ++k) acc[k] = Blk{0, 0};
+    if (j < sz) {
+        const Blk p = cur[static_cast<size_t>(b) * D + j];
+        const bool t = (p.lo & 1) != 0;
+        Blk kids[M];
+        uint64_t xl = 0, xh = 0;
+#pragma unroll
+        for (int k = 0; k < NK; ++k) {
+            const Blk h = H[static_cast<size_t>(b) * HS + j * NK + k];
+            xl ^= h.lo;
+            xh ^= h.hi;
+            kids[k] = Blk{h.lo ^ (t ? cw[k].lo : 0), h.hi ^ (t ? cw[k].hi : 0)};
+        }
+        kids[NK] = Blk{xl ^ p.lo ^ (t ? cwf.lo : 0), xh ^ p.hi ^ (t ? cwf.hi : 0)};
+        Blk* dst = nxt + static_cast<size_t>(b) * D + j * M;
+#pragma unroll
+        for (int k = 0; k < M; ++k) dst[k] = kids[k];
+        if (hash_next) {
+#pragma unroll 1
+            for (int k = 0; k < M; ++k) {
+                Blk h[NK];
+                hash_node<W, PRG>(kids[k], a, h);
+                Blk* hd = Hn + static_cast<size_t>(b) * HS + (j * M + k) * NK;
+#pragma unroll
+                for (int kk = 0; kk < NK; ++kk) {
+                    hd[kk] = h[kk];
+                    acc[kk].lo ^= h[kk].lo;
+                    acc[kk].hi ^= h[kk].hi;
+                }
+            }
+        }
+    }
+    if (hash_next) cta_xor_reduce<NK>(acc, my_next + static_cast<size_t>(b) * NK, red);
+}
+
+// my[b][k] = dlt[b][level][k].
+__global__ void seed_kernel(Blk* my, const Blk* dlt, int B, int levels, int nk, int level) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B * nk) return;
+    const int b = i / nk, k = i % nk;
+    my[i] = dlt[(static_cast<size_t>(b) * levels + level) * nk + k];
+}
+
+struct Pool {
+    Blk *cur = nullptr, *nxt = nullptr, *H = nullptr, *Hn = nullptr, *dlt = nullptr;
+    Blk *my = nullptr, *myn = nullptr, *peer = nullptr;
+    uint32_t* rk = nullptr;
+    Blk *h_my = nullptr, *h_peer = nullptr;   // pinned
+    size_t cap_front = 0, cap_h = 0, cap_dlt = 0, cap_cw = 0;
+    std::mutex mu;
+};
+
+Pool& pool_for_device() {
+    static std::mutex mu;
+    static Pool* pools[64] = {nullptr};
+    int dev = 0;
+    PCGB_CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[dev]) pools[dev] = new Pool();
+    return *pools[dev];
+}
+
+template <class T>
+void grow(T*& p, size_t& cap, size_t need) {
+    if (need <= cap) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    if (cudaMalloc(&p, need * sizeof(T)) != cudaSuccess) {
+        cudaGetLastError();
+        fail(PCGB_ENOMEM, "dpf_gpu_batch_full_eval: device allocation failed");
+    }
+    cap = need;
+}
+
+template <int W, int PRG>
+Blk* run_levels(Pool& pl, int B, int n, const Blk* roots, const Blk* dltsft,
+                pcgb_exchange_fn ex, void* user, cudaStream_t st) {
+    constexpr int M = 1 << W, NK = M - 1;
+    const int levels = n / W;
+    const size_t D = static_cast<size_t>(1) << n;
+    const size_t HS = (D / M) * NK;
+    const size_t ncw = static_cast<size_t>(B) * NK;
+    const size_t smem = 32 * NK * sizeof(Blk) + (PRG == PCGB_PRG_AES ? sizeof(AesSm) : 0);
+    const uint32_t* te = PRG == PCGB_PRG_AES ? aes_te_table_device() : nullptr;
+    PCGB_CK(cudaMemcpy2DAsync(pl.cur, D * sizeof(Blk), roots, sizeof(Blk), sizeof(Blk),
+                              static_cast<size_t>(B), cudaMemcpyHostToDevice, st));
+    PCGB_CK(cudaMemcpyAsync(pl.dlt, dltsft, static_cast<size_t>(B) * levels * NK * sizeof(Blk),
+                            cudaMemcpyHostToDevice, st));
+    const unsigned sgrid = static_cast<unsigned>((ncw + 255) / 256);
+    seed_kernel<<<sgrid, 256, 0, st>>>(pl.my, pl.dlt, B, levels, NK, 0);
+    PCGB_POST_LAUNCH();
+    hash_roots_kernel<W, PRG><<<dim3(1, B), kTPB, smem, st>>>(pl.cur, D, pl.H, HS, pl.my, te, pl.rk);
+    PCGB_POST_LAUNCH();
+    Blk *cur = pl.cur, *nxt = pl.nxt, *H = pl.H, *Hn = pl.Hn, *my = pl.my, *myn = pl.myn;
+    for (int i = 0; i < levels; ++i) {
+        PCGB_CK(cudaMemcpyAsync(pl.h_my, my, ncw * sizeof(Blk), cudaMemcpyDeviceToHost, st));
+        PCGB_CK(cudaStreamSynchronize(st));
+        if (ex) {
+            if (ex(reinterpret_cast<const pcgb_blk*>(pl.h_my), reinterpret_cast<pcgb_blk*>(pl.h_peer),
+                   ncw, user) != 0)
+                fail(PCGB_ECALLBACK, "dpf_gpu_batch_full_eval: exchange callback failed");
+        } else {
+            for (size_t k = 0; k < ncw; ++k) pl.h_peer[k] = Blk{0, 0};
+        }
+        PCGB_CK(cudaMemcpyAsync(pl.peer, pl.h_peer, ncw * sizeof(Blk), cudaMemcpyHostToDevice, st));
+        const int hash_next = (i + 1 < levels) ? 1 : 0;
+        if (hash_next) {
+            seed_kernel<<<sgrid, 256, 0, st>>>(myn, pl.dlt, B, levels, NK, i + 1);
+            PCGB_POST_LAUNCH();
+        }
+        const size_t sz = static_cast<size_t>(1) << (W * i);
+        const dim3 grid(static_cast<unsigned>((sz + kTPB - 1) / kTPB), static_cast<unsigned>(B));
+        expand_level_kernel<W, PRG><<<grid, kTPB, smem, st>>>(cur, H, my, pl.peer, nxt, Hn, myn, sz,
+                                                              D, HS, hash_next, te, pl.rk);
+        PCGB_POST_LAUNCH();
+        std::swap(cur, nxt);
+        std::swap(H, Hn);
+        std::swap(my, myn);
+    }
+    return cur;
+}
+
+void grow_pair(Blk*& a, Blk*& b, size_t& cap, size_t need) {
+    if (need <= cap) return;
+    size_t c1 = cap, c2 = cap;
+    grow(a, c1, need);
+    grow(b, c2, need);
+    cap = need;
+}
+
+Blk* interactive_eval(int B, int n, int w, const Blk* roots, const Blk* dltsft, const uint8_t* rks,
+                      int prg, pcgb_exchange_fn ex, void* user, cudaStream_t st, Pool& pl) {
+    if (w < 1 || w > 4)
+        fail(PCGB_EINVAL, "dpf_gpu_batch_full_eval: w must be in [1,4] (expand_kernel CW[16])");
+    if (n < 1 || n % w != 0) fail(PCGB_EINVAL, "dpf_gpu_batch_full_eval: w must divide n");
+    if (n > 30) fail(PCGB_EINVAL, "dpf_gpu_batch_full_eval: n must be at most 30");
+    if (prg == PCGB_PRG_AES && rks == nullptr)
+        fail(PCGB_EINVAL, "dpf_gpu_batch_full_eval: AES PRG requires round_keys");
+    if (prg != PCGB_PRG_AES && prg != PCGB_PRG_CHACHA8)
+        fail(PCGB_EINVAL, "dpf_gpu_batch_full_eval: unknown PRG");
+    if (!roots || !dltsft) fail(PCGB_EINVAL, "dpf_gpu_batch_full_eval: null input");
+    const int m = 1 << w, nk = m - 1, levels = n / w;
+    const size_t D = static_cast<size_t>(1) << n;
+    grow_pair(pl.cur, pl.nxt, pl.cap_front, static_cast<size_t>(B) * D);
+    grow_pair(pl.H, pl.Hn, pl.cap_h, static_cast<size_t>(B) * (D / m) * nk);
+    grow(pl.dlt, pl.cap_dlt, static_cast<size_t>(B) * levels * nk);
+    const size_t ncw = static_cast<size_t>(B) * nk;
+    if (ncw > pl.cap_cw) {
+        size_t c1 = pl.cap_cw, c2 = pl.cap_cw, c3 = pl.cap_cw;
+        grow(pl.my, c1, ncw);
+        grow(pl.myn, c2, ncw);
+        grow(pl.peer, c3, ncw);
+        if (pl.h_my) cudaFreeHost(pl.h_my);
+        if (pl.h_peer) cudaFreeHost(pl.h_peer);
+        pl.h_my = pl.h_peer = nullptr;
+        PCGB_CK(cudaMallocHost(&pl.h_my, ncw * sizeof(Blk)));
+        PCGB_CK(cudaMallocHost(&pl.h_peer, ncw * sizeof(Blk)));
+        pl.cap_cw = ncw;
+    }
+    if (!pl.rk) PCGB_CK(cudaMalloc(&pl.rk, 15 * 176));
+    if (prg == PCGB_PRG_AES)
+        PCGB_CK(cudaMemcpyAsync(pl.rk, rks, static_cast<size_t>(nk) * 176, cudaMemcpyHostToDevice,
+                                st));
+#define PCGB_RUN(W_)                                                                        \
+    case W_:                                                                                \
+        return prg == PCGB_PRG_AES                                                          \
+                   ? run_levels<W_, PCGB_PRG_AES>(pl, B, n, roots, dltsft, ex, user, st)     \
+                   : run_levels<W_, PCGB_PRG_CHACHA8>(pl, B, n, roots, dltsft, ex, user, st);
+    switch (w) {
+        PCGB_RUN(1)
+        PCGB_RUN(2)
+        PCGB_RUN(3)
+        PCGB_RUN(4)
+    }
+#undef PCGB_RUN
+    return nullptr;
+}
+
+}  // namespace
+
+// Runs the level loop under the per-device pool lock; the returned pointer
+// aliases the pool (valid until the next call on this device).
+const Blk* dpf_interactive_device(int B, int n, int w, const Blk* roots, const Blk* dltsft,
+                                  const uint8_t* rks, int prg, pcgb_exchange_fn ex, void* user,
+                                  Blk* host_out) {
+    if (B <= 0) return nullptr;
+    Pool& pl = pool_for_device();
+    std::lock_guard<std::mutex> lk(pl.mu);
+    cudaStream_t st = default_stream();
+    Blk* leaves = interactive_eval(B, n, w, roots, dltsft, rks, prg, ex, user, st, pl);
+    if (host_out)
+        PCGB_CK(cudaMemcpyAsync(host_out, leaves, (static_cast<size_t>(B) << n) * sizeof(Blk),
+                                cudaMemcpyDeviceToHost, st));
+    PCGB_CK(cudaStreamSynchronize(st));
+    return leaves;
+}
+
+}  // namespace pcgb

@@ -1,0 +1,148 @@
+// Keyed DPF: host-side dispatch and the gather plan.  The kernels live in
+// dpf_keyed_impl.cuh (instantiated per PRG by dpf_keyed_chacha.cu and
+// dpf_keyed_aes.cu); see that header for the algorithm.
+#include "pcgb_internal.h"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "field.cuh"
+
+namespace pcgb {
+
+size_t keyed_tops_scratch_nodes(int K, int w, int to_level) {
+    int l1 = 0;
+    while (l1 < to_level && (static_cast<size_t>(K) << (w * l1)) < 65536) ++l1;
+    if (l1 >= to_level || l1 == 0) return 0;
+    return static_cast<size_t>(K) << (w * l1);
+}
+
+void keyed_expand_tops(int K, int n, int w, int prg, const Blk* roots, const Blk* cws,
+                       const uint32_t* d_aes_rk, int to_level, Blk* out, Blk* scratch,
+                       cudaStream_t st) {
+    const int levels = n / w;
+    if (prg == PCGB_PRG_AES)
+        keyed_tops_aes(K, levels, w, roots, cws, aes_te_table_device(), d_aes_rk, to_level, out,
+                       scratch, st);
+    else
+        keyed_tops_chacha(K, levels, w, roots, cws, nullptr, nullptr, to_level, out, scratch, st);
+}
+
+// Gather plan: for pair q = (i <= j) and output bin r, the key halves of
+// blocks (i,j) and (j,i) whose leaves land in [r*bin, (r+1)*bin) after the
+// X^N = -1 fold.  Key (kk, ll) of a block covers pre-fold positions
+// (kk+ll)*bin + [0, 2*bin) (pcg_ole_impl.h:435-444), so with s = kk+ll:
+//   s = r     -> first half,  kept;   s = r-1   -> second half, kept;
+//   s = r+t   -> first half,  negated; s = r+t-1 -> second half, negated.
+void gather_plan_build(GatherPlan& gp, int N, int c, int t, int n, int w) {
+    gather_plan_free(gp);
+    gp.N = N; gp.c = c; gp.t = t; gp.n = n; gp.w = w;
+    const int levels = n / w;
+    // Leaves per thread: 16 for w in {1,2,4}, 8 for w = 3; fewer when the
+    // half domain is smaller.
+    int sl = (w == 3) ? 1 : 4 / w;
+    while (sl > 1 && w * sl > n - 1) --sl;
+    if (w * sl > n - 1) fail(PCGB_EINVAL, "domain too small for the fused leaf kernel");
+    gp.sl = sl;
+    gp.S = 1 << (w * sl);
+    gp.hl = levels - sl;
+    std::vector<uint32_t> off, ent;
+    std::vector<uint32_t> pair_ij;
+    int Q = 0;
+    off.push_back(0);
+    const uint32_t tt = static_cast<uint32_t>(t) * t;
+    for (int i = 0; i < c; ++i)
+        for (int j = i; j < c; ++j) {
+            pair_ij.push_back(static_cast<uint32_t>(i * c + j));
+            for (int r = 0; r < t; ++r) {
+                const int blocks[2] = {i * c + j, j * c + i};
+                for (int bi = 0; bi < (i == j ? 1 : 2); ++bi) {
+                    const uint32_t base = static_cast<uint32_t>(blocks[bi]) * tt;
+                    const int svals[4] = {r, r - 1, r + t, r + t - 1};
+                    const int halves[4] = {0, 1, 0, 1};
+                    const int folds[4] = {0, 0, 1, 1};
+                    for (int v = 0; v < 4; ++v) {
+                        const int s = svals[v];
+                        if (s < 0 || s > 2 * t - 2) continue;
+                        for (int kk = 0; kk < t; ++kk) {
+                            const int ll = s - kk;
+                            if (ll < 0 || ll >= t) continue;
+                            const uint32_t key = base + static_cast<uint32_t>(kk * t + ll);
+                            ent.push_back(key << 2 | static_cast<uint32_t>(halves[v]) << 1 |
+                                          static_cast<uint32_t>(folds[v]));
+                        }
+                    }
+                }
+                off.push_back(static_cast<uint32_t>(ent.size()));
+            }
+            ++Q;
+        }
+    gp.Q = Q;
+    gp.n_entries = static_cast<int>(ent.size());
+    // Heavy pairs (i != j carry two blocks) first so the tail is short.
+    std::vector<uint16_t> order;
+    for (int q = 0; q < Q; ++q) if ((pair_ij[q] / c) != (pair_ij[q] % c)) order.push_back(q);
+    for (int q = 0; q < Q; ++q) if ((pair_ij[q] / c) == (pair_ij[q] % c)) order.push_back(q);
+    PCGB_CK(cudaMalloc(&gp.d_off, off.size() * sizeof(uint32_t)));
+    PCGB_CK(cudaMalloc(&gp.d_entries, std::max<size_t>(ent.size(), 1) * sizeof(uint32_t)));
+    PCGB_CK(cudaMalloc(&gp.d_qorder, order.size() * sizeof(uint16_t)));
+    PCGB_CK(cudaMemcpy(gp.d_off, off.data(), off.size() * sizeof(uint32_t),
+                       cudaMemcpyHostToDevice));
+    if (!ent.empty())
+        PCGB_CK(cudaMemcpy(gp.d_entries, ent.data(), ent.size() * sizeof(uint32_t),
+                           cudaMemcpyHostToDevice));
+    PCGB_CK(cudaMemcpy(gp.d_qorder, order.data(), order.size() * sizeof(uint16_t),
+                       cudaMemcpyHostToDevice));
+    gp.pair_ij = pair_ij;
+}
+
+void gather_plan_free(GatherPlan& gp) {
+    if (gp.d_off) cudaFree(gp.d_off);
+    if (gp.d_entries) cudaFree(gp.d_entries);
+    if (gp.d_qorder) cudaFree(gp.d_qorder);
+    gp.d_off = nullptr; gp.d_entries = nullptr; gp.d_qorder = nullptr;
+}
+
+void keyed_leaf_gather(const GatherPlan& gp, int party, int prg, const Blk* F, const Blk* cws,
+                       const uint64_t* cw_out, const uint32_t* d_aes_rk, uint64_t* gq,
+                       cudaStream_t st) {
+    LeafLaunch L;
+    L.levels = gp.n / gp.w;
+    L.bin = static_cast<size_t>(gp.N) / gp.t;
+    int tpb = 256;
+    while (tpb > 1 && static_cast<size_t>(tpb) * gp.S > L.bin) tpb >>= 1;
+    if (static_cast<size_t>(tpb) * gp.S > L.bin) fail(PCGB_EINVAL, "bin smaller than one tile");
+    L.tpb = tpb;
+    L.grid = dim3(static_cast<unsigned>(L.bin / (static_cast<size_t>(tpb) * gp.S)),
+                  static_cast<unsigned>(gp.t), static_cast<unsigned>(gp.Q));
+    L.smem = static_cast<size_t>(tpb) * (gp.S + 1) * sizeof(uint64_t) +
+             (prg == PCGB_PRG_AES ? keyed_aes_smem_bytes_aes() : 0);
+    L.st = st;
+    L.F = F; L.cws = cws; L.cw_out = cw_out;
+    L.off = gp.d_off; L.entries = gp.d_entries; L.q_order = gp.d_qorder;
+    L.t = gp.t; L.hl = gp.hl; L.N = gp.N; L.party = party;
+    L.rk = d_aes_rk; L.gq = gq;
+    if (prg == PCGB_PRG_AES) {
+        L.te = aes_te_table_device();
+        keyed_leaf_aes(gp.w, gp.sl, L);
+    } else {
+        keyed_leaf_chacha(gp.w, gp.sl, L);
+    }
+}
+
+void deal_keys_launch(int N, int c, int t, int n, int w, int prg, uint64_t seed,
+                      const uint32_t* d_rk, Blk* roots0, Blk* roots1, Blk* cws, uint64_t* cw_out,
+                      cudaStream_t st) {
+    const int K = c * c * t * t;
+    const uint64_t bin = static_cast<uint64_t>(N / t);
+    const unsigned grid = static_cast<unsigned>((K + 127) / 128);
+    if (prg == PCGB_PRG_AES)
+        keyed_deal_aes(w, grid, keyed_aes_smem_bytes_aes(), seed, c, t, n, bin, roots0, roots1, cws,
+                       cw_out, aes_te_table_device(), d_rk, r2_mod_p(), st);
+    else
+        keyed_deal_chacha(w, grid, 0, seed, c, t, n, bin, roots0, roots1, cws, cw_out, nullptr,
+                          nullptr, r2_mod_p(), st);
+}
+
+}  // namespace pcgb

@@ -1,0 +1,447 @@
+// Keyed half-tree DPF full-domain evaluation fused with the output layer.
+//
+// A key is (root, CW[level][0..nk), cw_out).  The per-level update is the
+// half-tree rule of half_tree_dpf/dpf.cpp:553-574: children k < m-1 are
+// H_k(parent) ^ t*CW[k]; child m-1 is (XOR_k H_k) ^ parent ^ t*CW[m-1] with
+// CW[m-1] = XOR_k CW[k] and t = lsb(parent).  Because every CW is known,
+// any subtree can be expanded independently: no per-level barrier.
+//
+// Two kernels:
+//   expand_tops   root -> frontier at level hl (= levels - sl), one thread
+//                 per source node, depth-first, nodes written in order.
+//   leaf_gather   one thread per S = m^sl consecutive output positions of a
+//                 folded, pair-merged g' buffer.  For every key half that
+//                 lands on those positions (the gather plan) it loads one
+//                 frontier node, expands sl levels in registers, hashes each
+//                 leaf with the output-layer ChaCha8 (nonce "out_hash"),
+//                 converts C = low64 mod p, y = C + tau*cw_out, applies the
+//                 party / fold signs and accumulates mod p.  Each g' word is
+//                 written once, coalesced, with no atomics: the result is
+//                 bit-identical to the reference's CAS-atomic scatter
+//                 (GPU_baseline/common/leaf_convert_cuda.cu:207-234), whose
+//                 mod-p sum is order independent.
+#ifndef PCGB_DPF_KEYED_IMPL_CUH_
+#define PCGB_DPF_KEYED_IMPL_CUH_
+
+#include "pcgb_internal.h"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "aes128.cuh"
+#include "chacha8.cuh"
+#include "field.cuh"
+#include "synth.h"
+
+namespace pcgb {
+namespace {
+
+constexpr int kPrgAes = PCGB_PRG_AES;
+constexpr int kPrgChaCha = PCGB_PRG_CHACHA8;
+
+// Deepest DFS the tops kernel supports (its per-thread stack size).
+constexpr int kTopsMaxDepth = 26;
+
+struct AesSmem {
+    uint32_t te[1024];
+    uint32_t rk[15 * 44];
+};
+
+__device__ __forceinline__ void load_aes_smem(AesSmem& s, const uint32_t* te, const uint32_t* rk,
+                                              int nk) {
+    for (int i = threadIdx.x; i < 1024; i += blockDim.x) s.te[i] = te[i];
+    for (int i = threadIdx.x; i < nk * 44; i += blockDim.x) s.rk[i] = rk[i];
+    __syncthreads();
+}
+
+__device__ __forceinline__ Blk ldblk(const Blk* p) {
+    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(p));
+    return Blk{v.x, v.y};
+}
+
+__device__ __forceinline__ void stblk(Blk* p, const Blk& b) {
+    *reinterpret_cast<ulonglong2*>(p) = make_ulonglong2(b.lo, b.hi);
+}
+
+// m children of `p` under the level CWs cw[0..nk) (global, broadcast).
+template <int W, int PRG>
+__device__ __forceinline__ void children(const Blk& p, const Blk* __restrict__ cw,
+                                         const AesSmem* aes, Blk (&kids)[1 << W]) {
+    constexpr int M = 1 << W, NK = M - 1;
+    const bool t = (p.lo & 1) != 0;
+    uint64_t hxl = 0, hxh = 0, cfl = 0, cfh = 0;
+    if constexpr (PRG == kPrgChaCha) {
+#pragma unroll
+        for (int b = 0; b < (NK + 3) / 4; ++b) {
+            uint32_t o[16];
+            tree_block(p.lo, p.hi, b, o);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int k = 4 * b + c;
+                if (k < NK) {
+                    const uint64_t hl = o[4 * c] | (static_cast<uint64_t>(o[4 * c + 1]) << 32);
+                    const uint64_t hh = o[4 * c + 2] | (static_cast<uint64_t>(o[4 * c + 3]) << 32);
+                    const Blk cv = ldblk(cw + k);
+                    cfl ^= cv.lo; cfh ^= cv.hi;
+                    hxl ^= hl; hxh ^= hh;
+                    kids[k] = Blk{hl ^ (t ? cv.lo : 0), hh ^ (t ? cv.hi : 0)};
+                }
+            }
+        }
+    } else {
+#pragma unroll 1
+        for (int k = 0; k < NK; ++k) {
+            uint64_t hl, hh;
+            aes_ccr(aes->te, aes->rk + 44 * k, p.lo, p.hi, hl, hh);
+            const Blk cv = ldblk(cw + k);
+            cfl ^= cv.lo; cfh ^= cv.hi;
+            hxl ^= hl; hxh ^= hh;
+            kids[k] = Blk{hl ^ (t ? cv.lo : 0), hh ^ (t ? cv.hi : 0)};
+        }
+    }
+    kids[NK] = Blk{hxl ^ p.lo ^ (t ? cfl : 0), hxh ^ p.hi ^ (t ? cfh : 0)};
+}
+
+// Raw tree hashes H_0..H_{nk-1} of one node (no correction words).
+template <int W, int PRG>
+__device__ __forceinline__ void hash_raw(const Blk& p, const AesSmem* aes, Blk (&h)[(1 << W) - 1]) {
+    constexpr int NK = (1 << W) - 1;
+    if constexpr (PRG == kPrgChaCha) {
+#pragma unroll
+        for (int b = 0; b < (NK + 3) / 4; ++b) {
+            uint32_t o[16];
+            tree_block(p.lo, p.hi, b, o);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int k = 4 * b + c;
+                if (k < NK)
+                    h[k] = Blk{o[4 * c] | (static_cast<uint64_t>(o[4 * c + 1]) << 32),
+                               o[4 * c + 2] | (static_cast<uint64_t>(o[4 * c + 3]) << 32)};
+            }
+        }
+    } else {
+#pragma unroll 1
+        for (int k = 0; k < NK; ++k) aes_ccr(aes->te, aes->rk + 44 * k, p.lo, p.hi, h[k].lo, h[k].hi);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// expand_tops: depth-first expansion of `nlev` levels below each source node.
+template <int W, int PRG>
+__global__ void __launch_bounds__(128) expand_tops_kernel(
+    const Blk* __restrict__ src, int K, int src_lvl, int nlev, int levels,
+    const Blk* __restrict__ cws, const uint32_t* __restrict__ aes_te,
+    const uint32_t* __restrict__ aes_rk, Blk* __restrict__ dst) {
+    constexpr int M = 1 << W, NK = M - 1;
+    constexpr int MAXD = kTopsMaxDepth;
+    extern __shared__ __align__(16) uint64_t tops_dsm[];
+    AesSmem& aes_s = *reinterpret_cast<AesSmem*>(tops_dsm);
+    if constexpr (PRG == kPrgAes) load_aes_smem(aes_s, aes_te, aes_rk, NK);
+    const size_t per_key_src = static_cast<size_t>(1) << (W * src_lvl);
+    const size_t id = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (id >= static_cast<size_t>(K) * per_key_src) return;
+    const size_t key = id / per_key_src;
+    const size_t j = id % per_key_src;
+    const Blk* kcw = cws + key * static_cast<size_t>(levels) * NK;
+    const size_t fan = static_cast<size_t>(1) << (W * nlev);
+    Blk* out = dst + key * (per_key_src * fan) + j * fan;
+    const Blk root = ldblk(src + id);
+    if (nlev == 0) { stblk(out, root); return; }
+
+    // stack[d][k]: children at relative depth d+1; pos[d]: next child index.
+    Blk stack[MAXD][M];
+    int pos[MAXD];
+    children<W, PRG>(root, kcw + static_cast<size_t>(src_lvl) * NK, &aes_s, stack[0]);
+    pos[0] = 0;
+    int d = 0;
+    size_t emitted = 0;
+    while (d >= 0) {
+        if (d == nlev - 1) {
+#pragma unroll
+            for (int k = 0; k < M; ++k) stblk(out + emitted + k, stack[d][k]);
+            emitted += M;
+            --d;
+            if (d >= 0) ++pos[d];
+            continue;
+        }
+        if (pos[d] == M) {
+            --d;
+            if (d >= 0) ++pos[d];
+            continue;
+        }
+        Blk kids[M];
+        children<W, PRG>(stack[d][pos[d]], kcw + static_cast<size_t>(src_lvl + d + 1) * NK,
+                         &aes_s, kids);
+#pragma unroll
+        for (int k = 0; k < M; ++k) stack[d + 1][k] = kids[k];
+        ++d;
+        pos[d] = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// leaf_gather: see the file comment.
+
+// Two output-layer hashes at once (independent states: twice the ILP).
+__device__ __forceinline__ void out_hash_x2(const Blk& a, const Blk& b, uint64_t& ha,
+                                            uint64_t& hb) {
+    ha = out_hash_lo64(a.lo, a.hi);
+    hb = out_hash_lo64(b.lo, b.hi);
+}
+
+struct LeafCtx {
+    uint64_t* acc;   // shared accumulator row of this thread (stride 1)
+    uint64_t cwo;    // output-layer CW of the current key
+    bool neg;        // party ^ fold
+};
+
+__device__ __forceinline__ uint64_t leaf_value(const Blk& leaf, uint64_t h, const LeafCtx& c) {
+    uint64_t y = reduce_p(h);
+    if (leaf.lo & 1) y = add_p(y, c.cwo);
+    return c.neg ? neg_p(y) : y;
+}
+
+__device__ __forceinline__ void leaf_pair(const Blk& a, const Blk& b, int u, LeafCtx& c) {
+    uint64_t ha, hb;
+    out_hash_x2(a, b, ha, hb);
+    c.acc[u] = add_p(c.acc[u], leaf_value(a, ha, c));
+    c.acc[u + 1] = add_p(c.acc[u + 1], leaf_value(b, hb, c));
+}
+
+// Binary (w = 1) subtree of SL levels below `node`, leaves u_base.. in order.
+template <int SL, int PRG>
+struct Dfs1 {
+    __device__ __forceinline__ static void run(const Blk& node, const Blk* __restrict__ cw,
+                                               const AesSmem* aes, int u, LeafCtx& c) {
+        Blk k2[2];
+        children<1, PRG>(node, cw, aes, k2);
+        const Blk L = k2[0], R = k2[1];
+#pragma unroll 1
+        for (int i = 0; i < 2; ++i)
+            Dfs1<SL - 1, PRG>::run(i ? R : L, cw + 1, aes, u + (i << (SL - 1)), c);
+    }
+};
+template <int PRG>
+struct Dfs1<1, PRG> {
+    __device__ __forceinline__ static void run(const Blk& node, const Blk* __restrict__ cw,
+                                               const AesSmem* aes, int u, LeafCtx& c) {
+        Blk k2[2];
+        children<1, PRG>(node, cw, aes, k2);
+        leaf_pair(k2[0], k2[1], u, c);
+    }
+};
+
+// m-ary subtree (w > 1).
+template <int W, int SL, int PRG>
+struct DfsM {
+    __device__ __forceinline__ static void run(const Blk& node, const Blk* __restrict__ cw,
+                                               const AesSmem* aes, int u, LeafCtx& c) {
+        constexpr int M = 1 << W, NK = M - 1;
+        Blk kids[M];
+        children<W, PRG>(node, cw, aes, kids);
+        if constexpr (SL == 1) {
+#pragma unroll
+            for (int k = 0; k < M; k += 2) leaf_pair(kids[k], kids[k + 1], u + k, c);
+        } else {
+#pragma unroll 1
+            for (int k = 0; k < M; ++k)
+                DfsM<W, SL - 1, PRG>::run(kids[k], cw + NK, aes, u + k * (1 << (W * (SL - 1))),
+                                          c);
+        }
+    }
+};
+
+template <int W, int SL, int PRG>
+__global__ void __launch_bounds__(256) leaf_gather_kernel(
+    const Blk* __restrict__ F, const Blk* __restrict__ cws, const uint64_t* __restrict__ cw_out,
+    const uint32_t* __restrict__ off, const uint32_t* __restrict__ entries,
+    const uint16_t* __restrict__ q_order, int t, int levels, int hl, size_t bin, int N,
+    int party, const uint32_t* __restrict__ aes_te, const uint32_t* __restrict__ aes_rk,
+    uint64_t* __restrict__ gq) {
+    constexpr int M = 1 << W, NK = M - 1;
+    constexpr int S = 1 << (W * SL);
+    constexpr int STRIDE = S + 1;  // padded accumulator rows: conflict-free
+    extern __shared__ __align__(16) uint64_t acc_s[];
+    AesSmem& aes_s = *reinterpret_cast<AesSmem*>(acc_s + blockDim.x * STRIDE);
+    if constexpr (PRG == kPrgAes) load_aes_smem(aes_s, aes_te, aes_rk, NK);
+
+    const int r = blockIdx.y;
+    const int q = q_order[blockIdx.z];
+    const size_t tile = static_cast<size_t>(blockDim.x) * S;
+    const size_t o = static_cast<size_t>(blockIdx.x) * tile + static_cast<size_t>(threadIdx.x) * S;
+    uint64_t* acc = acc_s + threadIdx.x * STRIDE;
+#pragma unroll
+    for (int u = 0; u < S; ++u) acc[u] = 0;
+
+    const size_t per_key = static_cast<size_t>(1) << (W * hl);
+    const uint32_t e0 = off[q * t + r], e1 = off[q * t + r + 1];
+    LeafCtx c;
+    c.acc = acc;
+    for (uint32_t e = e0; e < e1; ++e) {
+        const uint32_t ent = __ldg(entries + e);
+        const size_t key = ent >> 2;
+        const size_t half = (ent >> 1) & 1;
+        c.neg = ((ent & 1) != 0) != (party != 0);
+        c.cwo = __ldg(cw_out + key);
+        const Blk node = ldblk(F + key * per_key + (half * bin + o) / S);
+        const Blk* kcw = cws + (key * levels + hl) * NK;
+        if constexpr (W == 1) Dfs1<SL, PRG>::run(node, kcw, &aes_s, 0, c);
+        else DfsM<W, SL, PRG>::run(node, kcw, &aes_s, 0, c);
+    }
+    __syncthreads();
+    // Coalesced write-out of the CTA's tile.
+    uint64_t* dst = gq + static_cast<size_t>(q) * N + static_cast<size_t>(r) * bin +
+                    static_cast<size_t>(blockIdx.x) * tile;
+    for (size_t e = threadIdx.x; e < tile; e += blockDim.x)
+        dst[e] = acc_s[(e / S) * STRIDE + (e % S)];
+}
+
+template <int W, int PRG>
+void launch_tops(const Blk* src, int K, int src_lvl, int nlev, int levels, const Blk* cws,
+                 const uint32_t* te, const uint32_t* rk, Blk* dst, cudaStream_t st) {
+    if (nlev < 0 || nlev > kTopsMaxDepth) fail(PCGB_EINVAL, "keyed expansion deeper than 26 levels");
+    const size_t threads = static_cast<size_t>(K) << (W * src_lvl);
+    const int TPB = 128;
+    const size_t smem = PRG == kPrgAes ? sizeof(AesSmem) : 0;
+    expand_tops_kernel<W, PRG><<<static_cast<unsigned>((threads + TPB - 1) / TPB), TPB, smem, st>>>(
+        src, K, src_lvl, nlev, levels, cws, te, rk, dst);
+    PCGB_POST_LAUNCH();
+}
+
+template <int W, int PRG>
+void tops_dispatch(int K, int levels, const Blk* roots, const Blk* cws, const uint32_t* te,
+                   const uint32_t* rk, int to_level, Blk* out, Blk* scratch, cudaStream_t st) {
+    // Stage 1 gives every key m^l1 subtrees so stage 2 has enough threads.
+    int l1 = 0;
+    while (l1 < to_level && (static_cast<size_t>(K) << (W * l1)) < 65536) ++l1;
+    if (l1 >= to_level || l1 == 0) {
+        launch_tops<W, PRG>(roots, K, 0, to_level, levels, cws, te, rk, out, st);
+        return;
+    }
+    launch_tops<W, PRG>(roots, K, 0, l1, levels, cws, te, rk, scratch, st);
+    launch_tops<W, PRG>(scratch, K, l1, to_level - l1, levels, cws, te, rk, out, st);
+}
+
+template <int W, int PRG>
+__global__ void deal_kernel(uint64_t seed, int c, int t, int n, uint64_t bin, Blk* roots0,
+                            Blk* roots1, Blk* cws, uint64_t* cw_out, const uint32_t* aes_te,
+                            const uint32_t* aes_rk, uint64_t r2) {
+    constexpr int M = 1 << W, NK = M - 1;
+    extern __shared__ __align__(16) uint64_t deal_dsm[];
+    AesSmem& aes_s = *reinterpret_cast<AesSmem*>(deal_dsm);
+    if constexpr (PRG == kPrgAes) load_aes_smem(aes_s, aes_te, aes_rk, NK);
+    const int K = c * c * t * t;
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= K) return;
+    const int blk = id / (t * t), rr = id % (t * t);
+    const int ii = blk / c, jj = blk % c, kk = rr / t, ll = rr % t;
+    const uint64_t alpha = synth_offset(seed, 0, static_cast<uint64_t>(ii) * t + kk, bin) +
+                           synth_offset(seed, 1, static_cast<uint64_t>(jj) * t + ll, bin);
+    const uint64_t v0 = synth_value(seed, 0, static_cast<uint64_t>(ii) * t + kk);
+    const uint64_t v1 = synth_value(seed, 1, static_cast<uint64_t>(jj) * t + ll);
+    const uint64_t beta = mont_mul(mont_mul(v0, v1), r2);
+    const Blk delta{synth_rnd(seed, kDomDelta, id) | 1, synth_rnd(seed, kDomDelta + 1, id)};
+    Blk p0{synth_rnd(seed, kDomRoot, id), synth_rnd(seed, kDomRoot + 1, id)};
+    Blk p1{p0.lo ^ delta.lo, p0.hi ^ delta.hi};
+    roots0[id] = p0;
+    roots1[id] = p1;
+    const int levels = n / W;
+    Blk* kcw = cws + static_cast<size_t>(id) * levels * NK;
+    for (int i = 0; i < levels; ++i) {
+        const int digit = static_cast<int>((alpha >> (n - W * (i + 1))) & NK);
+        Blk h0[NK], h1[NK];
+        hash_raw<W, PRG>(p0, &aes_s, h0);
+        hash_raw<W, PRG>(p1, &aes_s, h1);
+        Blk cwf{0, 0}, cwd{0, 0};
+        Blk x0{p0.lo, p0.hi}, x1{p1.lo, p1.hi};
+        Blk n0{0, 0}, n1{0, 0};
+#pragma unroll
+        for (int k = 0; k < NK; ++k) {
+            Blk cw{h0[k].lo ^ h1[k].lo, h0[k].hi ^ h1[k].hi};
+            if (digit == k) {
+                cw.lo ^= delta.lo; cw.hi ^= delta.hi;
+                cwd = cw; n0 = h0[k]; n1 = h1[k];
+            }
+            kcw[i * NK + k] = cw;
+            cwf.lo ^= cw.lo; cwf.hi ^= cw.hi;
+            x0.lo ^= h0[k].lo; x0.hi ^= h0[k].hi;
+            x1.lo ^= h1[k].lo; x1.hi ^= h1[k].hi;
+        }
+        if (digit == NK) { cwd = cwf; n0 = x0; n1 = x1; }
+        if (p0.lo & 1) { n0.lo ^= cwd.lo; n0.hi ^= cwd.hi; }
+        if (p1.lo & 1) { n1.lo ^= cwd.lo; n1.hi ^= cwd.hi; }
+        p0 = n0;
+        p1 = n1;
+    }
+    const uint64_t C0 = reduce_p(out_hash_lo64(p0.lo, p0.hi));
+    const uint64_t C1 = reduce_p(out_hash_lo64(p1.lo, p1.hi));
+    const uint64_t Bv = add_p(sub_p(C1, C0), beta);
+    const int A = static_cast<int>(p0.lo & 1) - static_cast<int>(p1.lo & 1);
+    cw_out[id] = A == 1 ? Bv : (A == -1 ? neg_p(Bv) : 0);
+}
+
+
+// ---- per-PRG host launchers (instantiated once per PRG in its own TU) -----
+template <int PRG>
+void tops_for_prg(int K, int levels, int w, const Blk* roots, const Blk* cws, const uint32_t* te,
+                  const uint32_t* rk, int to_level, Blk* out, Blk* scratch, cudaStream_t st) {
+    switch (w) {
+        case 1: tops_dispatch<1, PRG>(K, levels, roots, cws, te, rk, to_level, out, scratch, st); break;
+        case 2: tops_dispatch<2, PRG>(K, levels, roots, cws, te, rk, to_level, out, scratch, st); break;
+        case 3: tops_dispatch<3, PRG>(K, levels, roots, cws, te, rk, to_level, out, scratch, st); break;
+        case 4: tops_dispatch<4, PRG>(K, levels, roots, cws, te, rk, to_level, out, scratch, st); break;
+        default: fail(PCGB_EINVAL, "w must be in [1,4]");
+    }
+}
+
+template <int W, int SL, int PRG>
+void leaf_one(const LeafLaunch& L) {
+    auto kern = leaf_gather_kernel<W, SL, PRG>;
+    if (L.smem > 48 * 1024)
+        PCGB_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(L.smem)));
+    kern<<<L.grid, L.tpb, L.smem, L.st>>>(L.F, L.cws, L.cw_out, L.off, L.entries, L.q_order, L.t,
+                                         L.levels, L.hl, L.bin, L.N, L.party, L.te, L.rk, L.gq);
+    PCGB_POST_LAUNCH();
+}
+
+template <int PRG>
+void leaf_for_prg(int w, int sl, const LeafLaunch& L) {
+    switch (w * 8 + sl) {
+        case 1 * 8 + 4: leaf_one<1, 4, PRG>(L); break;
+        case 1 * 8 + 3: leaf_one<1, 3, PRG>(L); break;
+        case 1 * 8 + 2: leaf_one<1, 2, PRG>(L); break;
+        case 1 * 8 + 1: leaf_one<1, 1, PRG>(L); break;
+        case 2 * 8 + 2: leaf_one<2, 2, PRG>(L); break;
+        case 2 * 8 + 1: leaf_one<2, 1, PRG>(L); break;
+        case 3 * 8 + 1: leaf_one<3, 1, PRG>(L); break;
+        case 4 * 8 + 1: leaf_one<4, 1, PRG>(L); break;
+        default: fail(PCGB_EINVAL, "unsupported (w, sl) for the leaf kernel");
+    }
+}
+
+template <int PRG>
+void deal_for_prg(int w, unsigned grid, size_t smem, uint64_t seed, int c, int t, int n,
+                  uint64_t bin, Blk* roots0, Blk* roots1, Blk* cws, uint64_t* cw_out,
+                  const uint32_t* te, const uint32_t* rk, uint64_t r2, cudaStream_t st) {
+    switch (w) {
+#define PCGB_DEAL(W_)                                                                          \
+    case W_:                                                                                   \
+        deal_kernel<W_, PRG><<<grid, 128, smem, st>>>(seed, c, t, n, bin, roots0, roots1, cws, \
+                                                      cw_out, te, rk, r2);                     \
+        break;
+        PCGB_DEAL(1)
+        PCGB_DEAL(2)
+        PCGB_DEAL(3)
+        PCGB_DEAL(4)
+#undef PCGB_DEAL
+        default: fail(PCGB_EINVAL, "w must be in [1,4]");
+    }
+    PCGB_POST_LAUNCH();
+}
+
+}  // namespace
+}  // namespace pcgb
+
+#endif

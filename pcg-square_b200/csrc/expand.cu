@@ -1,0 +1,325 @@
+// One party's PCG-OLE expansion on the device (the algebra of
+// CPU_baseline/pcg_ole_2pc/pcg_ole_impl.h:213-312 and :453-484):
+//
+//   g_ij   = output layer of the t^2 DPF keys of block (i, j), folded mod X^N+1
+//   x      = sum_i a_i e_i                      (a_0 = 1, e_i the regular noise)
+//   z      = sum_{i,j} a_i a_j g_ij = INTT( sum_{i<=j} (a^_i a^_j) . NTT(g_ij + g_ji) )
+//
+// The expander keeps, per shape, the a_i coefficients (Montgomery form, for
+// the sparse x product) and the c(c+1)/2 evaluation images a^_i a^_j
+// (Montgomery-scaled) resident, so an expansion is four device stages:
+// keyed tops -> fused leaf/convert/gather -> sparse x -> NTT multiply-
+// accumulate + inverse.  Blocks (i,j) and (j,i) are merged while g is
+// produced (a_i a_j = a_j a_i), so only c(c+1)/2 forward transforms run.
+#include "pcgb_internal.h"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "field.cuh"
+#include "synth.h"
+
+namespace pcgb {
+
+void deal_keys_launch(int N, int c, int t, int n, int w, int prg, uint64_t seed,
+                      const uint32_t* d_rk, Blk* roots0, Blk* roots1, Blk* cws, uint64_t* cw_out,
+                      cudaStream_t st);
+
+namespace {
+
+// x[p] = sum_k [p == pos_0k] val_0k + sum_{i>=1,k} val_ik * a_i[p - pos_ik]
+// with the negacyclic sign when p < pos_ik.  aR holds a_i * 2^64 mod p, so
+// one Montgomery product gives a_i * val.
+__global__ void x_kernel(const uint64_t* __restrict__ pos, const uint64_t* __restrict__ val,
+                         const uint64_t* __restrict__ aR, int c, int t, size_t N,
+                         uint64_t* __restrict__ x) {
+    extern __shared__ uint64_t nz[];  // [c*t] positions then [c*t] values
+    const int ct = c * t;
+    for (int i = threadIdx.x; i < ct; i += blockDim.x) {
+        nz[i] = pos[i] % N;
+        nz[ct + i] = reduce_p(val[i]);
+    }
+    __syncthreads();
+    const size_t p = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    uint64_t acc = 0;
+    for (int k = 0; k < t; ++k)
+        if (nz[k] == p) acc = add_p(acc, nz[ct + k]);
+    for (int i = 1; i < c; ++i) {
+        const uint64_t* a = aR + static_cast<size_t>(i - 1) * N;
+        for (int k = 0; k < t; ++k) {
+            const uint64_t ps = nz[i * t + k];
+            const bool wrap = p < ps;
+            const size_t idx = wrap ? p + N - ps : p - ps;
+            const uint64_t term = mont_mul(__ldg(a + idx), nz[ct + i * t + k]);
+            acc = wrap ? sub_p(acc, term) : add_p(acc, term);
+        }
+    }
+    x[p] = acc;
+}
+
+// d[i] = mont(s[i], k): multiply by a constant given in Montgomery form.
+__global__ void scale_kernel(uint64_t* d, const uint64_t* s, size_t n, uint64_t k) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) d[i] = mont_mul(reduce_p(s[i]), k);
+}
+
+// img = (A .* B) * R  given plain evaluations A, B (B == nullptr means 1).
+__global__ void image_kernel(uint64_t* img, const uint64_t* A, const uint64_t* B, size_t n,
+                             uint64_t r2, uint64_t r3) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (!A) { img[i] = mont_mul(1, r2); return; }            // 1 * R (a_0 = 1 both sides)
+    if (!B) { img[i] = mont_mul(A[i], r2); return; }         // A * R
+    img[i] = mont_mul(mont_mul(A[i], B[i]), r3);             // A*B*R
+}
+
+__global__ void noise_kernel(uint64_t seed, int party, int ct, uint64_t bin, int t, uint64_t* pos,
+                             uint64_t* val) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ct) return;
+    pos[i] = static_cast<uint64_t>(i % t) * bin + synth_offset(seed, party, i, bin);
+    val[i] = synth_value(seed, party, i);
+}
+
+unsigned blocks_for(size_t n, int tpb) { return static_cast<unsigned>((n + tpb - 1) / tpb); }
+
+int ilog2(uint64_t v) {
+    int l = 0;
+    while ((uint64_t{1} << l) < v) ++l;
+    return l;
+}
+
+}  // namespace
+}  // namespace pcgb
+
+struct pcgb_expander {
+    int dev = 0;
+    int N = 0, c = 0, t = 0, w = 0, prg = 0, n = 0, levels = 0, nk = 0, K = 0, Q = 0;
+    const pcgb::NttPlan* ntt = nullptr;
+    pcgb::GatherPlan gp;
+    uint64_t* d_img = nullptr;   // Q*N
+    uint64_t* d_aR = nullptr;    // (c-1)*N
+    pcgb::Blk* d_F = nullptr;
+    pcgb::Blk* d_tops = nullptr;
+    uint64_t* d_g = nullptr;     // Q*N
+    uint32_t* d_rk = nullptr;    // AES sub-key schedules
+    size_t scratch_bytes = 0;
+    std::vector<cudaEvent_t> prof_ev;  // 5 per slot
+    int prof_slots = 0, prof_used = 0;
+    // host staging for pcgb_expand_host
+    void* h_stage = nullptr;
+    size_t h_stage_bytes = 0;
+    void* d_in = nullptr;
+    size_t d_in_bytes = 0;
+};
+
+namespace pcgb {
+
+pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64_t* public_a,
+                               const uint8_t* master_key) {
+    if (N < 4 || (N & (N - 1)) || N > (1 << kMaxLogN))
+        fail(PCGB_EINVAL, "expander: N must be a power of two in [4, 2^24]");
+    if (c < 1 || c > 8) fail(PCGB_EINVAL, "expander: c must be in [1, 8]");
+    if (t < 1 || (t & (t - 1)) || N / t < 2) fail(PCGB_EINVAL, "expander: t must be a power of two <= N/2");
+    if (prg != PCGB_PRG_AES && prg != PCGB_PRG_CHACHA8) fail(PCGB_EINVAL, "expander: unknown PRG");
+    if (prg == PCGB_PRG_AES && !master_key) fail(PCGB_EINVAL, "expander: AES needs a master key");
+    if (c > 1 && !public_a) fail(PCGB_EINVAL, "expander: public_a required for c > 1");
+    const int n = ilog2(2ull * (N / t));
+    if (w < 1 || w > 4 || n % w) fail(PCGB_EINVAL, "expander: w must be in [1,4] and divide log2(2N/t)");
+    auto* e = new pcgb_expander();
+    try {
+        PCGB_CK(cudaGetDevice(&e->dev));
+        e->N = N; e->c = c; e->t = t; e->w = w; e->prg = prg; e->n = n;
+        e->levels = n / w; e->nk = (1 << w) - 1; e->K = c * c * t * t; e->Q = c * (c + 1) / 2;
+        cudaStream_t st = default_stream();
+        e->ntt = &ntt_plan(ilog2(N));
+        gather_plan_build(e->gp, N, c, t, n, w);
+        const size_t NN = static_cast<size_t>(N);
+        PCGB_CK(cudaMalloc(&e->d_img, sizeof(uint64_t) * NN * e->Q));
+        if (c > 1) PCGB_CK(cudaMalloc(&e->d_aR, sizeof(uint64_t) * NN * (c - 1)));
+        // a_i coefficients (Montgomery form) and evaluations.
+        std::vector<uint64_t*> ahat(c, nullptr);
+        const uint64_t r2 = r2_mod_p(), r3 = mul_p_host(r2, r_mod_p());
+        if (c > 1) {
+            uint64_t* tmp = nullptr;
+            PCGB_CK(cudaMalloc(&tmp, sizeof(uint64_t) * NN * (c - 1)));
+            PCGB_CK(cudaMemcpy(tmp, public_a, sizeof(uint64_t) * NN * (c - 1), cudaMemcpyHostToDevice));
+            reduce_mod_p(tmp, tmp, NN * (c - 1), st);
+            scale_kernel<<<blocks_for(NN * (c - 1), 256), 256, 0, st>>>(e->d_aR, tmp, NN * (c - 1), r2);
+            PCGB_POST_LAUNCH();
+            ntt_forward(*e->ntt, tmp, c - 1, st);
+            for (int i = 1; i < c; ++i) ahat[i] = tmp + NN * (i - 1);
+            int q = 0;
+            for (int i = 0; i < c; ++i)
+                for (int j = i; j < c; ++j, ++q)
+                    image_kernel<<<blocks_for(NN, 256), 256, 0, st>>>(
+                        e->d_img + NN * q, i == 0 ? (j == 0 ? nullptr : ahat[j]) : ahat[i],
+                        i == 0 ? nullptr : ahat[j], NN, r2, r3);
+                    PCGB_POST_LAUNCH();
+            PCGB_CK(cudaStreamSynchronize(st));
+            cudaFree(tmp);
+        } else {
+            image_kernel<<<blocks_for(NN, 256), 256, 0, st>>>(e->d_img, nullptr, nullptr, NN, r2, r3);
+            PCGB_POST_LAUNCH();
+        }
+        if (prg == PCGB_PRG_AES) {
+            std::vector<uint8_t> rks(static_cast<size_t>(e->nk) * 176);
+            aes_tree_round_keys_host(master_key, e->nk, rks.data());
+            e->d_rk = aes_upload_round_keys(rks.data(), e->nk, st);
+        }
+        const size_t fnodes = static_cast<size_t>(e->K) << (w * e->gp.hl);
+        const size_t tnodes = keyed_tops_scratch_nodes(e->K, w, e->gp.hl);
+        PCGB_CK(cudaMalloc(&e->d_F, sizeof(Blk) * fnodes));
+        if (tnodes) PCGB_CK(cudaMalloc(&e->d_tops, sizeof(Blk) * tnodes));
+        PCGB_CK(cudaMalloc(&e->d_g, sizeof(uint64_t) * NN * e->Q));
+        e->scratch_bytes = sizeof(Blk) * (fnodes + tnodes) + sizeof(uint64_t) * NN * e->Q;
+        PCGB_CK(cudaStreamSynchronize(st));
+    } catch (...) {
+        // release what was allocated, then rethrow
+        gather_plan_free(e->gp);
+        cudaFree(e->d_img); cudaFree(e->d_aR); cudaFree(e->d_F); cudaFree(e->d_tops);
+        cudaFree(e->d_g); cudaFree(e->d_rk);
+        delete e;
+        throw;
+    }
+    return e;
+}
+
+void expander_destroy(pcgb_expander* e) {
+    if (!e) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(e->dev);
+    cudaStreamSynchronize(default_stream());
+    gather_plan_free(e->gp);
+    cudaFree(e->d_img); cudaFree(e->d_aR); cudaFree(e->d_F); cudaFree(e->d_tops);
+    cudaFree(e->d_g); cudaFree(e->d_rk); cudaFree(e->d_in);
+    if (e->h_stage) cudaFreeHost(e->h_stage);
+    for (auto& ev : e->prof_ev) cudaEventDestroy(ev);
+    cudaSetDevice(cur);
+    delete e;
+}
+
+void expand_device(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
+                   const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val, uint64_t* x,
+                   uint64_t* z, cudaStream_t st) {
+    if (party != 0 && party != 1) fail(PCGB_EINVAL, "expand: party must be 0 or 1");
+    if (!roots || !cws || !cw_out || !pos || !val || !x || !z) fail(PCGB_EINVAL, "expand: null pointer");
+    const size_t NN = static_cast<size_t>(e->N);
+    cudaEvent_t* ev = nullptr;
+    if (e->prof_slots > 0 && e->prof_used < e->prof_slots) ev = &e->prof_ev[5 * e->prof_used++];
+    if (ev) PCGB_CK(cudaEventRecord(ev[0], st));
+    keyed_expand_tops(e->K, e->n, e->w, e->prg, roots, cws, e->d_rk, e->gp.hl, e->d_F, e->d_tops, st);
+    if (ev) PCGB_CK(cudaEventRecord(ev[1], st));
+    keyed_leaf_gather(e->gp, party, e->prg, e->d_F, cws, cw_out, e->d_rk, e->d_g, st);
+    if (ev) PCGB_CK(cudaEventRecord(ev[2], st));
+    const size_t sm = sizeof(uint64_t) * 2 * static_cast<size_t>(e->c) * e->t;
+    x_kernel<<<blocks_for(NN, 256), 256, sm, st>>>(pos, val, e->d_aR, e->c, e->t, NN, x);
+    PCGB_POST_LAUNCH();
+    if (ev) PCGB_CK(cudaEventRecord(ev[3], st));
+    ntt_mac_inverse(*e->ntt, e->d_g, e->d_img, e->Q, z, st);
+    if (ev) PCGB_CK(cudaEventRecord(ev[4], st));
+}
+
+void expand_host(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
+                 const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val, uint64_t* x,
+                 uint64_t* z) {
+    cudaStream_t st = default_stream();
+    const size_t K = e->K, ct = static_cast<size_t>(e->c) * e->t, NN = e->N;
+    const size_t b_roots = K * sizeof(Blk), b_cws = K * e->levels * e->nk * sizeof(Blk);
+    const size_t b_cwo = K * 8, b_noise = ct * 8, b_out = NN * 8;
+    const size_t in_bytes = b_roots + b_cws + b_cwo + 2 * b_noise;
+    const size_t dev_bytes = in_bytes + 2 * b_out;
+    if (dev_bytes > e->d_in_bytes) {
+        cudaFree(e->d_in);
+        e->d_in = nullptr;
+        PCGB_CK(cudaMalloc(&e->d_in, dev_bytes));
+        e->d_in_bytes = dev_bytes;
+    }
+    char* d = static_cast<char*>(e->d_in);
+    Blk* d_roots = reinterpret_cast<Blk*>(d);
+    Blk* d_cws = reinterpret_cast<Blk*>(d + b_roots);
+    uint64_t* d_cwo = reinterpret_cast<uint64_t*>(d + b_roots + b_cws);
+    uint64_t* d_pos = reinterpret_cast<uint64_t*>(d + b_roots + b_cws + b_cwo);
+    uint64_t* d_val = d_pos + ct;
+    uint64_t* d_x = reinterpret_cast<uint64_t*>(d + in_bytes);
+    uint64_t* d_z = d_x + NN;
+    PCGB_CK(cudaMemcpyAsync(d_roots, roots, b_roots, cudaMemcpyHostToDevice, st));
+    PCGB_CK(cudaMemcpyAsync(d_cws, cws, b_cws, cudaMemcpyHostToDevice, st));
+    PCGB_CK(cudaMemcpyAsync(d_cwo, cw_out, b_cwo, cudaMemcpyHostToDevice, st));
+    PCGB_CK(cudaMemcpyAsync(d_pos, pos, b_noise, cudaMemcpyHostToDevice, st));
+    PCGB_CK(cudaMemcpyAsync(d_val, val, b_noise, cudaMemcpyHostToDevice, st));
+    expand_device(e, party, d_roots, d_cws, d_cwo, d_pos, d_val, d_x, d_z, st);
+    PCGB_CK(cudaMemcpyAsync(x, d_x, b_out, cudaMemcpyDeviceToHost, st));
+    PCGB_CK(cudaMemcpyAsync(z, d_z, b_out, cudaMemcpyDeviceToHost, st));
+    PCGB_CK(cudaStreamSynchronize(st));
+}
+
+void expand_g_device(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
+                     const uint64_t* cw_out, uint64_t* d_g, cudaStream_t st) {
+    keyed_expand_tops(e->K, e->n, e->w, e->prg, roots, cws, e->d_rk, e->gp.hl, e->d_F, e->d_tops, st);
+    keyed_leaf_gather(e->gp, party, e->prg, e->d_F, cws, cw_out, e->d_rk, d_g, st);
+}
+
+void noise_device(int N, int c, int t, uint64_t seed, int party, uint64_t* pos, uint64_t* val,
+                  cudaStream_t st) {
+    const int ct = c * t;
+    noise_kernel<<<(ct + 127) / 128, 128, 0, st>>>(seed, party, ct, static_cast<uint64_t>(N / t), t,
+                                                    pos, val);
+    PCGB_POST_LAUNCH();
+}
+
+void noise_host(int N, int c, int t, uint64_t seed, int party, uint64_t* pos, uint64_t* val) {
+    const uint64_t bin = static_cast<uint64_t>(N / t);
+    for (int i = 0; i < c * t; ++i) {
+        pos[i] = static_cast<uint64_t>(i % t) * bin + synth_offset(seed, party, i, bin);
+        val[i] = synth_value(seed, party, i);
+    }
+}
+
+void public_a_host(int N, int c, uint64_t a_seed, uint64_t* a) {
+    for (int i = 1; i < c; ++i)
+        for (int j = 0; j < N; ++j)
+            a[static_cast<size_t>(i - 1) * N + j] = synth_rnd(a_seed, kDomA + i, j) % kPm;
+}
+
+void deal_keys_device(pcgb_expander* e, uint64_t seed, Blk* r0, Blk* r1, Blk* cws, uint64_t* cwo,
+                      cudaStream_t st) {
+    deal_keys_launch(e->N, e->c, e->t, e->n, e->w, e->prg, seed, e->d_rk, r0, r1, cws, cwo, st);
+}
+
+}  // namespace pcgb
+
+namespace pcgb {
+
+void expander_info(const pcgb_expander* e, int* K, int* levels, int* nk, size_t* scratch) {
+    if (K) *K = e->K;
+    if (levels) *levels = e->levels;
+    if (nk) *nk = e->nk;
+    if (scratch) *scratch = e->scratch_bytes;
+}
+
+void expander_set_profiling(pcgb_expander* e, int slots) {
+    if (slots < 0) fail(PCGB_EINVAL, "profiling slots must be >= 0");
+    for (auto& ev : e->prof_ev) cudaEventDestroy(ev);
+    e->prof_ev.assign(static_cast<size_t>(slots) * 5, nullptr);
+    for (auto& ev : e->prof_ev) PCGB_CK(cudaEventCreate(&ev));
+    e->prof_slots = slots;
+    e->prof_used = 0;
+}
+
+int expander_stage_times(pcgb_expander* e, float* ms, int max_exp) {
+    const int n = std::min(e->prof_used, max_exp);
+    for (int i = 0; i < n; ++i) {
+        cudaEvent_t* ev = &e->prof_ev[5 * i];
+        PCGB_CK(cudaEventSynchronize(ev[4]));
+        for (int s = 0; s < 4; ++s) PCGB_CK(cudaEventElapsedTime(&ms[4 * i + s], ev[s], ev[s + 1]));
+    }
+    const int used = e->prof_used;
+    e->prof_used = 0;
+    return std::min(used, max_exp);
+}
+
+}  // namespace pcgb

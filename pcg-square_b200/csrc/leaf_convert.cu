@@ -1,0 +1,216 @@
+// Output-layer drop-ins: pcg_cuda::dpf_out_sums and dpf_out_scatter_g
+// (GPU_baseline/common/leaf_convert_cuda.h:43-52).
+//
+//   C[b][d] = low64(ChaCha8OutHash(leaf)) mod p, tau[b][d] = lsb(leaf)
+//   sumC[b] = sum_d C (mod p), sumT[b] = sum_d tau (plain integer)
+//   y = C + tau*CW[b]; party 1 negates; pos = (b/t + b%t)*D/2 + d;
+//   g[pos mod N] += (pos < N ? y : -y)              (mod p)
+//
+// dpf_out_sums reduces per-CTA partials in a fixed order.  dpf_out_scatter_g
+// is written as a gather: one thread per output word of g visits the (at
+// most 2t) instances whose shifted leaf ranges cover it, so every word is
+// produced once without atomics (the reference resolves overlaps with a
+// CAS-loop modular atomic, leaf_convert_cuda.cu:68-77,207-234).
+#include "pcgb_internal.h"
+
+#include <mutex>
+#include <vector>
+
+#include "chacha8.cuh"
+#include "field.cuh"
+
+namespace pcgb {
+namespace {
+
+constexpr int kTPB = 256;
+
+__device__ __forceinline__ uint64_t leaf_C(const ulonglong2& v) {
+    return reduce_p(out_hash_lo64(v.x, v.y));
+}
+
+// grid = (parts, B): partials[b*parts + part] (C lane), [B*parts + ...] (T lane).
+__global__ void __launch_bounds__(kTPB) out_sum_kernel(const ulonglong2* __restrict__ leaves,
+                                                       size_t D, uint64_t* __restrict__ partials) {
+    __shared__ uint64_t sc[kTPB / 32], stt[kTPB / 32];
+    const int b = blockIdx.y, parts = gridDim.x;
+    const ulonglong2* L = leaves + static_cast<size_t>(b) * D;
+    uint64_t c = 0, t = 0;
+    for (size_t d = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; d < D;
+         d += static_cast<size_t>(parts) * blockDim.x) {
+        const ulonglong2 v = __ldg(L + d);
+        c = add_p(c, leaf_C(v));
+        t += v.x & 1;
+    }
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        c = add_p(c, __shfl_xor_sync(0xffffffffu, c, off));
+        t += __shfl_xor_sync(0xffffffffu, t, off);
+    }
+    if ((threadIdx.x & 31) == 0) { sc[threadIdx.x >> 5] = c; stt[threadIdx.x >> 5] = t; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t cc = 0, tt = 0;
+        for (int w = 0; w < kTPB / 32; ++w) { cc = add_p(cc, sc[w]); tt += stt[w]; }
+        const size_t slot = static_cast<size_t>(b) * parts + blockIdx.x;
+        partials[slot] = cc;
+        partials[static_cast<size_t>(gridDim.y) * parts + slot] = tt;
+    }
+}
+
+// One thread per instance folds its partials in order.
+__global__ void out_fold_kernel(const uint64_t* __restrict__ partials, int parts, int B,
+                                uint64_t* __restrict__ sums) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    uint64_t c = 0, t = 0;
+    for (int i = 0; i < parts; ++i) {
+        c = add_p(c, partials[static_cast<size_t>(b) * parts + i]);
+        t += partials[static_cast<size_t>(B) * parts + static_cast<size_t>(b) * parts + i];
+    }
+    sums[b] = c;
+    sums[B + b] = t;
+}
+
+// Gather scatter: thread per output word p < N.
+__global__ void __launch_bounds__(kTPB) out_gather_kernel(const ulonglong2* __restrict__ leaves,
+                                                          int B, size_t D, int t, int party,
+                                                          const uint64_t* __restrict__ cws,
+                                                          uint64_t* __restrict__ g, size_t N) {
+    const size_t p = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    const size_t bin = D >> 1;
+    const int kk_max = (B - 1) / t;
+    const long s_max = static_cast<long>(kk_max) + t - 1;
+    uint64_t acc = 0;
+    for (int f = 0; f < 2; ++f) {
+        const size_t P = p + (f ? N : 0);   // pre-fold position
+        const long s_hi = static_cast<long>(P / bin);
+        for (long s = s_hi; s >= s_hi - 1; --s) {
+            if (s < 0 || s > s_max) continue;
+            const size_t d = P - static_cast<size_t>(s) * bin;
+            if (d >= D) continue;
+            const int kk0 = static_cast<int>(s - (t - 1) > 0 ? s - (t - 1) : 0);
+            const int kk1 = static_cast<int>(s < kk_max ? s : kk_max);
+            for (int kk = kk0; kk <= kk1; ++kk) {
+                const int b = kk * t + static_cast<int>(s - kk);
+                if (b >= B) continue;
+                const ulonglong2 v = __ldg(leaves + static_cast<size_t>(b) * D + d);
+                uint64_t y = leaf_C(v);
+                if (v.x & 1) y = add_p(y, __ldg(cws + b));
+                if ((party != 0) != (f != 0)) y = neg_p(y);
+                acc = add_p(acc, y);
+            }
+        }
+    }
+    g[p] = acc;
+}
+
+struct ConvPool {
+    uint64_t* partials = nullptr;
+    uint64_t* sums = nullptr;
+    uint64_t* cws = nullptr;
+    uint64_t* g = nullptr;
+    size_t cap_part = 0, cap_b = 0, cap_cw = 0, cap_g = 0;
+    std::mutex mu;
+};
+
+ConvPool& conv_pool() {
+    static std::mutex mu;
+    static ConvPool* pools[64] = {nullptr};
+    int dev = 0;
+    PCGB_CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[dev]) pools[dev] = new ConvPool();
+    return *pools[dev];
+}
+
+void grow(uint64_t*& p, size_t& cap, size_t need) {
+    if (need <= cap) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    if (cudaMalloc(&p, need * sizeof(uint64_t)) != cudaSuccess) {
+        cudaGetLastError();
+        fail(PCGB_ENOMEM, "leaf convert: device allocation failed");
+    }
+    cap = need;
+}
+
+void check_common(const void* d_leaves, int B, size_t D, uint64_t prime) {
+    if (prime != kP) fail(PCGB_EINVAL, "dpf_out: only the project prime is supported");
+    if (!d_leaves) fail(PCGB_EINVAL, "dpf_out: null leaves");
+    if (D < 2 || (D & (D - 1))) fail(PCGB_EINVAL, "dpf_out: D must be a power of two >= 2");
+    (void)B;
+}
+
+}  // namespace
+
+int out_sums_parts(size_t D) {
+    size_t parts = (D + kTPB * 8 - 1) / (kTPB * 8);
+    if (parts > 1024) parts = 1024;
+    return static_cast<int>(parts < 1 ? 1 : parts);
+}
+
+void out_sums_launch(const Blk* d_leaves, int B, size_t D, uint64_t* partials, uint64_t* sums,
+                     cudaStream_t st) {
+    const int parts = out_sums_parts(D);
+    out_sum_kernel<<<dim3(parts, B), kTPB, 0, st>>>(reinterpret_cast<const ulonglong2*>(d_leaves),
+                                                    D, partials);
+    PCGB_POST_LAUNCH();
+    out_fold_kernel<<<(B + 127) / 128, 128, 0, st>>>(partials, parts, B, sums);
+    PCGB_POST_LAUNCH();
+}
+
+void out_gather_launch(const Blk* d_leaves, int B, size_t D, int t, int party,
+                       const uint64_t* d_cws, uint64_t* d_g, size_t N, cudaStream_t st) {
+    out_gather_kernel<<<static_cast<unsigned>((N + kTPB - 1) / kTPB), kTPB, 0, st>>>(
+        reinterpret_cast<const ulonglong2*>(d_leaves), B, D, t, party, d_cws, d_g, N);
+    PCGB_POST_LAUNCH();
+}
+
+void dpf_out_sums_host(const Blk* d_leaves, int B, size_t D, uint64_t prime, uint64_t* sumC,
+                       uint64_t* sumT) {
+    if (B <= 0) return;
+    check_common(d_leaves, B, D, prime);
+    ConvPool& pl = conv_pool();
+    std::lock_guard<std::mutex> lk(pl.mu);
+    cudaStream_t st = default_stream();
+    grow(pl.partials, pl.cap_part, 2 * static_cast<size_t>(B) * out_sums_parts(D));
+    grow(pl.sums, pl.cap_b, 2 * static_cast<size_t>(B));
+    out_sums_launch(d_leaves, B, D, pl.partials, pl.sums, st);
+    std::vector<uint64_t> both(2 * static_cast<size_t>(B));
+    PCGB_CK(cudaMemcpyAsync(both.data(), pl.sums, both.size() * sizeof(uint64_t),
+                            cudaMemcpyDeviceToHost, st));
+    PCGB_CK(cudaStreamSynchronize(st));
+    for (int b = 0; b < B; ++b) {
+        sumC[b] = both[b];
+        sumT[b] = both[B + b];
+    }
+}
+
+void dpf_out_scatter_host(const Blk* d_leaves, int B, size_t D, int t, int party, uint64_t prime,
+                          const uint64_t* CW, uint64_t* g_out, int N) {
+    if (B <= 0) return;
+    check_common(d_leaves, B, D, prime);
+    if (t <= 0 || N <= 0) fail(PCGB_EINVAL, "dpf_out_scatter_g: t and N must be positive");
+    const size_t bin = D >> 1;
+    const size_t s_max = static_cast<size_t>((B - 1) / t) + t - 1;
+    // Every pre-fold position must stay below 2N (the reference's fold
+    // handles one wrap only).
+    if ((s_max + 2) * bin > 2 * static_cast<size_t>(N))
+        fail(PCGB_EINVAL, "dpf_out_scatter_g: N smaller than the instances' span (needs N >= t*D/2)");
+    ConvPool& pl = conv_pool();
+    std::lock_guard<std::mutex> lk(pl.mu);
+    cudaStream_t st = default_stream();
+    grow(pl.cws, pl.cap_cw, static_cast<size_t>(B));
+    grow(pl.g, pl.cap_g, static_cast<size_t>(N));
+    std::vector<uint64_t> cw(CW, CW + B);
+    for (auto& v : cw) v %= kP;
+    PCGB_CK(cudaMemcpyAsync(pl.cws, cw.data(), B * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    out_gather_launch(d_leaves, B, D, t, party, pl.cws, pl.g, static_cast<size_t>(N), st);
+    PCGB_CK(cudaMemcpyAsync(g_out, pl.g, static_cast<size_t>(N) * sizeof(uint64_t),
+                            cudaMemcpyDeviceToHost, st));
+    PCGB_CK(cudaStreamSynchronize(st));
+}
+
+}  // namespace pcgb

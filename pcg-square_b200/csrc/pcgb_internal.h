@@ -1,0 +1,155 @@
+// Internal definitions shared by the library's translation units.
+#ifndef PCGB_INTERNAL_H_
+#define PCGB_INTERNAL_H_
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "pcg_b200.h"
+
+namespace pcgb {
+
+// The project prime: p = 2^62 - 3*2^25 + 1 (p - 1 = 2^25 * (2^37 - 3)), so
+// negacyclic transforms exist up to N = 2^24.
+constexpr uint64_t kP = 4611686018326724609ULL;
+// Output-layer hash nonce, "out_hash" in ASCII (the tree PRG uses nonce 0).
+constexpr uint64_t kOutDomain = 0x6f75745f68617368ULL;
+constexpr int kMaxLogN = 24;
+
+struct alignas(16) Blk {
+    uint64_t lo, hi;
+};
+static_assert(sizeof(Blk) == 16, "Blk must be 16 bytes");
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void fail(int code, const std::string& msg);
+void check_cuda(cudaError_t e, const char* what);
+#define PCGB_CK(call) ::pcgb::check_cuda((call), #call)
+
+// Every kernel launch of the library is followed by PCGB_POST_LAUNCH(): it
+// checks the launch and counts it (pcgb_launch_count).
+void note_launch();
+#define PCGB_POST_LAUNCH()                                   \
+    do {                                                     \
+        ::pcgb::check_cuda(cudaGetLastError(), "kernel launch"); \
+        ::pcgb::note_launch();                               \
+    } while (0)
+
+// Per-device default stream owned by the library (non-blocking).
+cudaStream_t default_stream();
+inline cudaStream_t as_stream(void* s) {
+    return s ? static_cast<cudaStream_t>(s) : default_stream();
+}
+
+// Number of SMs of the current device.
+int sm_count();
+
+// ---- keyed DPF (dpf_keyed.cu) ------------------------------------------
+// Expand K keys from level 0 to level `to_level` (levels of w bits), writing
+// m^to_level nodes per key to `out` ([k][node], natural order).  scratch
+// must hold K * m^min(to_level, first_stage_levels) nodes (may be nullptr
+// when to_level is small; see keyed_tops_scratch_nodes).
+size_t keyed_tops_scratch_nodes(int K, int w, int to_level);
+void keyed_expand_tops(int K, int n, int w, int prg, const Blk* roots, const Blk* cws,
+                       const uint32_t* d_aes_rk, int to_level, Blk* out, Blk* scratch,
+                       cudaStream_t st);
+
+// Contribution list of the gather form of the output-layer scatter: for
+// every merged (i<=j) pair q and output bin r, the key halves that land in
+// [r*bin, (r+1)*bin) of the folded g (see gather_plan in dpf_keyed.cu).
+struct GatherPlan {
+    int N = 0, c = 0, t = 0, n = 0, w = 0, Q = 0;
+    int sl = 0;          // levels expanded per thread in the leaf kernel
+    int S = 0;           // leaves per thread = m^sl
+    int hl = 0;          // frontier level = levels - sl
+    uint32_t* d_off = nullptr;      // [Q*t + 1]
+    uint32_t* d_entries = nullptr;  // key_id << 2 | half << 1 | fold_negate
+    uint16_t* d_qorder = nullptr;   // launch order of the pairs (heavy first)
+    std::vector<uint32_t> pair_ij;  // pair q -> block index i*c + j (i <= j)
+    int n_entries = 0;
+};
+void gather_plan_build(GatherPlan& gp, int N, int c, int t, int n, int w);
+void gather_plan_free(GatherPlan& gp);
+
+// Launch parameters of the fused leaf kernel (dpf_keyed_impl.cuh).
+struct LeafLaunch {
+    dim3 grid;
+    int tpb = 0;
+    size_t smem = 0;
+    cudaStream_t st = nullptr;
+    const Blk* F = nullptr;
+    const Blk* cws = nullptr;
+    const uint64_t* cw_out = nullptr;
+    const uint32_t* off = nullptr;
+    const uint32_t* entries = nullptr;
+    const uint16_t* q_order = nullptr;
+    int t = 0, levels = 0, hl = 0;
+    size_t bin = 0;
+    int N = 0, party = 0;
+    const uint32_t* te = nullptr;
+    const uint32_t* rk = nullptr;
+    uint64_t* gq = nullptr;
+};
+
+// Per-PRG instantiations (dpf_keyed_chacha.cu / dpf_keyed_aes.cu).
+#define PCGB_KEYED_DECL(NAME)                                                                   \
+    void keyed_tops_##NAME(int K, int levels, int w, const Blk* roots, const Blk* cws,          \
+                           const uint32_t* te, const uint32_t* rk, int to_level, Blk* out,     \
+                           Blk* scratch, cudaStream_t st);                                     \
+    void keyed_leaf_##NAME(int w, int sl, const LeafLaunch& L);                                 \
+    void keyed_deal_##NAME(int w, unsigned grid, size_t smem, uint64_t seed, int c, int t,      \
+                           int n, uint64_t bin, Blk* roots0, Blk* roots1, Blk* cws,            \
+                           uint64_t* cw_out, const uint32_t* te, const uint32_t* rk,           \
+                           uint64_t r2, cudaStream_t st);                                      \
+    size_t keyed_aes_smem_bytes_##NAME();
+PCGB_KEYED_DECL(chacha)
+PCGB_KEYED_DECL(aes)
+#undef PCGB_KEYED_DECL
+
+// Fused leaf kernel: frontier F (level hl) -> leaves -> out-hash -> convert
+// -> gather into the folded, pair-merged g' (Q buffers of N residues).
+void keyed_leaf_gather(const GatherPlan& gp, int party, int prg, const Blk* F, const Blk* cws,
+                       const uint64_t* cw_out, const uint32_t* d_aes_rk, uint64_t* gq,
+                       cudaStream_t st);
+
+// ---- AES tree PRG (aes_tables.cu) ---------------------------------------
+// Round keys as 44 little-endian words per sub-key, on the device.
+uint32_t* aes_upload_round_keys(const uint8_t* rks_bytes, int nk, cudaStream_t st);
+const uint32_t* aes_te_table_device();   // 4 x 256 words, resident
+void aes_expand_key_host(const uint8_t key[16], uint8_t rk[176]);
+void aes_encrypt_host(const uint8_t rk[176], const uint8_t in[16], uint8_t out[16]);
+void aes_tree_round_keys_host(const uint8_t master[16], int nk, uint8_t* rks);
+
+// ---- NTT (ntt.cu) --------------------------------------------------------
+struct NttPlan;
+const NttPlan& ntt_plan(int logN);   // resident per (device, logN)
+// In-place forward transform of `batch` length-N polys into the internal
+// evaluation layout (coefficients must be < p).
+void ntt_forward(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st);
+void ntt_inverse(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st);
+// c = a * b mod (X^N+1) for `batch` polys; c may alias a or b; inputs any
+// uint64 (reduced mod p first).  scratch: 2*batch*N words.
+void poly_mul_device(const NttPlan& pl, uint64_t* c, const uint64_t* a, const uint64_t* b,
+                     int batch, uint64_t* scratch, cudaStream_t st);
+// acc = INTT( sum_q img[q] (.) NTT(g[q]) ); g is consumed (transformed in
+// place); img in Montgomery-scaled evaluation layout.
+void ntt_mac_inverse(const NttPlan& pl, uint64_t* g, const uint64_t* img, int Q, uint64_t* acc,
+                     cudaStream_t st);
+// Pointwise c[i] = a[i]*b[i]*R mod p over `count` words (R = 2^64): turns
+// an evaluation vector into its Montgomery-scaled form when b = R^2 scaled.
+void pointwise_mul(uint64_t* c, const uint64_t* a, const uint64_t* b, size_t count, int mode,
+                   cudaStream_t st);
+void reduce_mod_p(uint64_t* d, const uint64_t* s, size_t count, cudaStream_t st);
+
+}  // namespace pcgb
+
+#endif

@@ -1,0 +1,455 @@
+"""ctypes shim over libpcg_b200.so, the B200 PCG-OLE expansion library.
+
+The functions mirror the reference's pcg_cuda:: hooks
+(GPU_baseline/common/dpf_gpu.h, leaf_convert_cuda.h, poly_mul_cuda.h,
+aes_gpu.h): same names, same argument meaning, host numpy arrays in and out,
+and a RuntimeError where the reference throws std::runtime_error.  The
+native device-resident API (keyed DPF, fused expansion, batched NTT) is
+exposed through `Expander` and the *_device functions, which take raw device
+pointers (ints) such as torch's tensor.data_ptr().
+
+There is no CPU fallback: if the shared library or a CUDA device is missing,
+the calls raise.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libpcg_b200.so")
+
+P = 4611686018326724609
+PRG_AES, PRG_CHACHA8 = 0, 1
+POLYMUL_V1, POLYMUL_MERGE, POLYMUL_4STEP, POLYMUL_SQUARE = 0, 1, 2, 3
+OUT_HASH_DOMAIN = 0x6F75745F68617368
+
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_vp = C.c_void_p
+
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p)
+
+
+class PcgError(RuntimeError):
+    """A library call failed; .code is the PCGB_E* value."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libpcg_b200.so not built ({LIB_PATH}); run __graft_entry__.build()")
+    L = C.CDLL(LIB_PATH)
+    L.pcgb_last_error.restype = C.c_char_p
+    sig = {
+        "pcgb_version": ([], C.c_int),
+        "pcgb_is_cuda_available": ([], C.c_int),
+        "pcgb_device_name": ([C.c_char_p, C.c_size_t], C.c_int),
+        "pcgb_runtime_version": ([C.c_char_p, C.c_size_t], C.c_int),
+        "pcgb_set_device": ([C.c_int], C.c_int),
+        "pcgb_get_device": ([C.POINTER(C.c_int)], C.c_int),
+        "pcgb_sm_count": ([C.POINTER(C.c_int)], C.c_int),
+        "pcgb_malloc": ([C.POINTER(_vp), C.c_size_t], C.c_int),
+        "pcgb_free": ([_vp], C.c_int),
+        "pcgb_memcpy_h2d": ([_vp, _vp, C.c_size_t, _vp], C.c_int),
+        "pcgb_memcpy_d2h": ([_vp, _vp, C.c_size_t, _vp], C.c_int),
+        "pcgb_memset": ([_vp, C.c_int, C.c_size_t, _vp], C.c_int),
+        "pcgb_stream_synchronize": ([_vp], C.c_int),
+        "pcgb_device_synchronize": ([], C.c_int),
+        "pcgb_default_stream": ([], _vp),
+        "pcgb_dpf_batch_full_eval": ([C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, C.c_int, _vp, _vp,
+                                      _vp, C.c_int], C.c_int),
+        "pcgb_dpf_batch_full_eval_device": ([C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, C.c_int,
+                                             _vp, _vp, C.c_int, C.POINTER(_vp)], C.c_int),
+        "pcgb_dpf_out_sums": ([_vp, C.c_int, C.c_size_t, C.c_uint64, _u64p, _u64p], C.c_int),
+        "pcgb_dpf_out_scatter_g": ([_vp, C.c_int, C.c_size_t, C.c_int, C.c_int, C.c_uint64, _u64p,
+                                    _u64p, C.c_int], C.c_int),
+        "pcgb_poly_mul_supported": ([C.c_int, C.c_uint64, C.c_int, C.c_char_p, C.c_size_t],
+                                    C.c_int),
+        "pcgb_poly_mul_u64": ([C.c_int, _u64p, _u64p, _u64p, C.c_int, C.c_int, C.c_uint64,
+                               C.POINTER(C.c_double)], C.c_int),
+        "pcgb_aes128_expand_key": ([_u8p, _u8p], C.c_int),
+        "pcgb_aes128_ecb_encrypt": ([_u8p, _u8p, _u8p, C.c_int], C.c_int),
+        "pcgb_aes_tree_round_keys": ([_u8p, C.c_int, _u8p], C.c_int),
+        "pcgb_dpf_keyed_full_eval": ([C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp],
+                                     C.c_int),
+        "pcgb_poly_mul_device": ([_vp, _vp, _vp, C.c_int, C.c_int, _vp], C.c_int),
+        "pcgb_poly_mul_device_multi": ([C.c_int, _vp, _vp, _vp, _vp, _vp], C.c_int),
+        "pcgb_expander_create": ([C.POINTER(_vp), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp,
+                                  _vp], C.c_int),
+        "pcgb_expander_destroy": ([_vp], C.c_int),
+        "pcgb_expander_info": ([_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                C.POINTER(C.c_size_t)], C.c_int),
+        "pcgb_expand_device": ([_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
+        "pcgb_expand_host": ([_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
+        "pcgb_expand_g_device": ([_vp, C.c_int, _vp, _vp, _vp, _vp, _vp], C.c_int),
+        "pcgb_expander_set_profiling": ([_vp, C.c_int], C.c_int),
+        "pcgb_expander_stage_times": ([_vp, C.POINTER(C.c_float), C.c_int], C.c_int),
+        "pcgb_launch_count": ([], C.c_ulonglong),
+        "pcgb_arx_peak": ([C.POINTER(C.c_double), C.POINTER(C.c_float)], C.c_int),
+        "pcgb_event_create": ([C.POINTER(_vp)], C.c_int),
+        "pcgb_event_destroy": ([_vp], C.c_int),
+        "pcgb_event_record": ([_vp, _vp], C.c_int),
+        "pcgb_event_elapsed": ([_vp, _vp, C.POINTER(C.c_float)], C.c_int),
+        "pcgb_noise": ([C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int, _u64p, _u64p], C.c_int),
+        "pcgb_public_a": ([C.c_int, C.c_int, C.c_uint64, _vp], C.c_int),
+        "pcgb_deal_keys_device": ([_vp, C.c_uint64, _vp, _vp, _vp, _vp, _vp], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    return L
+
+
+lib = _load()
+
+
+def _check(rc):
+    if rc != 0:
+        raise PcgError(rc, lib.pcgb_last_error().decode(errors="replace"))
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _u8(x):
+    if isinstance(x, (bytes, bytearray, memoryview)):
+        return np.frombuffer(bytes(x), dtype=np.uint8).copy()
+    return np.ascontiguousarray(x, dtype=np.uint8).reshape(-1)
+
+
+def _blocks(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.uint64).reshape(-1, 2)
+    if n is not None and a.shape[0] < n:
+        raise ValueError(f"expected at least {n} blocks, got {a.shape[0]}")
+    return a
+
+
+# ---- device / runtime (poly_mul_cuda.h:13-16) ------------------------------
+def is_cuda_available():
+    return lib.pcgb_is_cuda_available() == 1
+
+
+def device_name():
+    buf = C.create_string_buffer(256)
+    return buf.value.decode() if lib.pcgb_device_name(buf, 256) == 0 else "unavailable"
+
+
+def runtime_version():
+    buf = C.create_string_buffer(64)
+    return buf.value.decode() if lib.pcgb_runtime_version(buf, 64) == 0 else "unavailable"
+
+
+def set_device(dev):
+    _check(lib.pcgb_set_device(dev))
+
+
+def sm_count():
+    n = C.c_int(0)
+    _check(lib.pcgb_sm_count(C.byref(n)))
+    return n.value
+
+
+class DeviceBuffer:
+    """Owning device allocation made by the library (no torch needed)."""
+
+    def __init__(self, nbytes):
+        self.nbytes = int(nbytes)
+        p = C.c_void_p()
+        _check(lib.pcgb_malloc(C.byref(p), max(self.nbytes, 1)))
+        self.ptr = p.value
+
+    def upload(self, arr):
+        arr = np.ascontiguousarray(arr)
+        assert arr.nbytes <= self.nbytes
+        _check(lib.pcgb_memcpy_h2d(self.ptr, _p(arr), arr.nbytes, None))
+        return self
+
+    def download(self, dtype, count):
+        out = np.empty(count, dtype=dtype)
+        _check(lib.pcgb_memcpy_d2h(_p(out), self.ptr, out.nbytes, None))
+        return out
+
+    def free(self):
+        if self.ptr:
+            lib.pcgb_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def to_device(arr):
+    arr = np.ascontiguousarray(arr)
+    return DeviceBuffer(arr.nbytes).upload(arr)
+
+
+def synchronize():
+    _check(lib.pcgb_device_synchronize())
+
+
+def launch_count():
+    """Kernel launches issued by the library so far."""
+    return lib.pcgb_launch_count()
+
+
+def arx_peak():
+    """(G int-ops/s, ms) of the ChaCha8 ARX throughput probe."""
+    g, ms = C.c_double(), C.c_float()
+    _check(lib.pcgb_arx_peak(C.byref(g), C.byref(ms)))
+    return g.value, ms.value
+
+
+def default_stream():
+    return lib.pcgb_default_stream()
+
+
+class Event:
+    """CUDA event recorded on a library stream (default: the library's own)."""
+
+    def __init__(self):
+        p = C.c_void_p()
+        _check(lib.pcgb_event_create(C.byref(p)))
+        self.h = p.value
+
+    def record(self, stream=None):
+        _check(lib.pcgb_event_record(self.h, stream))
+
+    def elapsed_ms(self, stop):
+        ms = C.c_float()
+        _check(lib.pcgb_event_elapsed(self.h, stop.h, C.byref(ms)))
+        return ms.value
+
+    def __del__(self):
+        try:
+            lib.pcgb_event_destroy(self.h)
+        except Exception:
+            pass
+
+
+# ---- DPF (dpf_gpu.h:55-75) -------------------------------------------------
+def _exchange_cb(exchange):
+    """Wrap `exchange(my: ndarray[count,2]) -> peer ndarray` as a C callback."""
+    if exchange is None:
+        return None
+
+    def cb(my, peer, count, user):
+        try:
+            m = np.ctypeslib.as_array(C.cast(my, C.POINTER(C.c_uint64)), shape=(count, 2))
+            p = np.ctypeslib.as_array(C.cast(peer, C.POINTER(C.c_uint64)), shape=(count, 2))
+            p[:] = np.asarray(exchange(m.copy()), dtype=np.uint64).reshape(count, 2)
+            return 0
+        except Exception:
+            return 1
+
+    return EXCHANGE_FN(cb)
+
+
+def dpf_gpu_batch_full_eval(B, n, w, roots, dltsft, round_keys=None, party=0, exchange=None,
+                            prg=PRG_AES):
+    """Interactive batched full-domain evaluation; returns leaves [B*2^n, 2].
+
+    exchange(my) -> peer shares (None = peer shares are zero, the reference
+    benches' stub exchange).
+    """
+    roots = _blocks(roots, B)
+    dltsft = _blocks(dltsft)
+    out = np.zeros((B << n, 2), dtype=np.uint64)
+    cb = _exchange_cb(exchange)
+    rk = None if round_keys is None else _u8(round_keys)
+    _check(lib.pcgb_dpf_batch_full_eval(B, n, w, _p(roots), _p(dltsft), _p(rk), party,
+                                        C.cast(cb, C.c_void_p) if cb else None, None, _p(out), prg))
+    return out
+
+
+def dpf_gpu_batch_full_eval_device(B, n, w, roots, dltsft, round_keys=None, party=0,
+                                   exchange=None, prg=PRG_AES):
+    """Same, leaves stay on the device: returns the device pointer (int),
+    valid until the next dpf_gpu_* call."""
+    roots = _blocks(roots, B)
+    dltsft = _blocks(dltsft)
+    cb = _exchange_cb(exchange)
+    rk = None if round_keys is None else _u8(round_keys)
+    d = C.c_void_p()
+    _check(lib.pcgb_dpf_batch_full_eval_device(B, n, w, _p(roots), _p(dltsft), _p(rk), party,
+                                               C.cast(cb, C.c_void_p) if cb else None, None, prg,
+                                               C.byref(d)))
+    return d.value
+
+
+# ---- output layer (leaf_convert_cuda.h:43-52) ------------------------------
+def dpf_out_sums(d_leaves, B, D, prime=P):
+    sc, st = np.zeros(B, np.uint64), np.zeros(B, np.uint64)
+    _check(lib.pcgb_dpf_out_sums(d_leaves, B, D, prime, sc, st))
+    return sc, st
+
+
+def dpf_out_scatter_g(d_leaves, B, D, t, party, CW, N, prime=P):
+    g = np.zeros(N, np.uint64)
+    _check(lib.pcgb_dpf_out_scatter_g(d_leaves, B, D, t, party, prime,
+                                      np.ascontiguousarray(CW, np.uint64), g, N))
+    return g
+
+
+# ---- poly-mul (poly_mul_cuda.h:14-31) --------------------------------------
+def _supported(variant, prime, N):
+    buf = C.create_string_buffer(256)
+    ok = lib.pcgb_poly_mul_supported(variant, prime, N, buf, 256)
+    return ok == 1, buf.value.decode()
+
+
+def _mul(variant, a, b, batch, N, prime):
+    a = np.ascontiguousarray(a, np.uint64).reshape(-1)
+    b = np.ascontiguousarray(b, np.uint64).reshape(-1)
+    out = np.zeros(batch * N, np.uint64)
+    ms = C.c_double(0)
+    _check(lib.pcgb_poly_mul_u64(variant, out, a, b, batch, N, prime, C.byref(ms)))
+    return out, ms.value
+
+
+def poly_mul_supported(prime, N):
+    return _supported(POLYMUL_V1, prime, N)
+
+
+def poly_mul_u64(a, b, batch, N, prime=P):
+    return _mul(POLYMUL_V1, a, b, batch, N, prime)
+
+
+def poly_mul_gpuntt_supported(prime, N):
+    return _supported(POLYMUL_MERGE, prime, N)
+
+
+def poly_mul_u64_gpuntt(a, b, batch, N, prime=P):
+    return _mul(POLYMUL_MERGE, a, b, batch, N, prime)
+
+
+def poly_mul_gpuntt_4step_supported(prime, N):
+    return _supported(POLYMUL_4STEP, prime, N)
+
+
+def poly_mul_u64_gpuntt_4step(a, b, batch, N, prime=P):
+    return _mul(POLYMUL_4STEP, a, b, batch, N, prime)
+
+
+def poly_mul_gpuntt_square_supported(prime, N):
+    return _supported(POLYMUL_SQUARE, prime, N)
+
+
+def poly_mul_u64_gpuntt_square(a, b, batch, N, prime=P):
+    return _mul(POLYMUL_SQUARE, a, b, batch, N, prime)
+
+
+def poly_mul_device(d_c, d_a, d_b, batch, N, stream=None):
+    _check(lib.pcgb_poly_mul_device(d_c, d_a, d_b, batch, N, stream))
+
+
+# ---- AES (aes_gpu.h:13-19) --------------------------------------------------
+def aes128_expand_key_host(key):
+    rk = np.zeros(176, np.uint8)
+    _check(lib.pcgb_aes128_expand_key(_u8(key), rk))
+    return rk
+
+
+def aes128_ecb_encrypt_gpu(keys, data):
+    keys = _u8(keys)
+    data = _u8(data)
+    count = data.size // 16
+    out = np.zeros(count * 16, np.uint8)
+    _check(lib.pcgb_aes128_ecb_encrypt(keys, data, out, count))
+    return out
+
+
+def aes_tree_round_keys(master, nk):
+    rk = np.zeros(176 * nk, np.uint8)
+    _check(lib.pcgb_aes_tree_round_keys(_u8(master), nk, rk))
+    return rk
+
+
+# ---- keyed DPF / synthetic material ------------------------------------------
+def dpf_keyed_full_eval_device(K, n, w, prg, d_roots, d_cws, d_leaves, round_keys=None,
+                               stream=None):
+    rk = None if round_keys is None else _u8(round_keys)
+    _check(lib.pcgb_dpf_keyed_full_eval(K, n, w, prg, d_roots, d_cws, _p(rk), d_leaves, stream))
+
+
+def noise(N, c, t, seed, party):
+    pos, val = np.zeros(c * t, np.uint64), np.zeros(c * t, np.uint64)
+    _check(lib.pcgb_noise(N, c, t, seed, party, pos, val))
+    return pos, val
+
+
+def public_a(N, c, a_seed):
+    a = np.zeros(max(c - 1, 1) * N, np.uint64)
+    _check(lib.pcgb_public_a(N, c, a_seed, _p(a)))
+    return a
+
+
+class Expander:
+    """Resident per-shape state of the fused PCG-OLE expansion (one device)."""
+
+    def __init__(self, N, c, t, w=1, prg=PRG_CHACHA8, public_a=None, master_key=None):
+        self.N, self.c, self.t, self.w, self.prg = N, c, t, w, prg
+        pa = None if public_a is None else np.ascontiguousarray(public_a, np.uint64)
+        mk = None if master_key is None else _u8(master_key)
+        h = C.c_void_p()
+        _check(lib.pcgb_expander_create(C.byref(h), N, c, t, w, prg, _p(pa), _p(mk)))
+        self.h = h.value
+        K, L, nk, sb = C.c_int(), C.c_int(), C.c_int(), C.c_size_t()
+        _check(lib.pcgb_expander_info(self.h, C.byref(K), C.byref(L), C.byref(nk), C.byref(sb)))
+        self.K, self.levels, self.nk, self.scratch_bytes = K.value, L.value, nk.value, sb.value
+        self.Q = c * (c + 1) // 2
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.pcgb_expander_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def expand_device(self, party, d_roots, d_cws, d_cw_out, d_pos, d_val, d_x, d_z, stream=None):
+        _check(lib.pcgb_expand_device(self.h, party, d_roots, d_cws, d_cw_out, d_pos, d_val, d_x,
+                                      d_z, stream))
+
+    def expand_host(self, party, roots, cws, cw_out, pos, val):
+        roots = _blocks(roots, self.K)
+        cws = _blocks(cws, self.K * self.levels * self.nk)
+        cw_out = np.ascontiguousarray(cw_out, np.uint64)
+        pos = np.ascontiguousarray(pos, np.uint64)
+        val = np.ascontiguousarray(val, np.uint64)
+        x, z = np.zeros(self.N, np.uint64), np.zeros(self.N, np.uint64)
+        _check(lib.pcgb_expand_host(self.h, party, _p(roots), _p(cws), _p(cw_out), _p(pos),
+                                    _p(val), _p(x), _p(z)))
+        return x, z
+
+    def expand_g_device(self, party, d_roots, d_cws, d_cw_out, d_g, stream=None):
+        _check(lib.pcgb_expand_g_device(self.h, party, d_roots, d_cws, d_cw_out, d_g, stream))
+
+    def deal_keys_device(self, seed, d_roots0, d_roots1, d_cws, d_cw_out, stream=None):
+        _check(lib.pcgb_deal_keys_device(self.h, seed, d_roots0, d_roots1, d_cws, d_cw_out,
+                                         stream))
+
+    def set_profiling(self, slots):
+        """Record per-stage events for the next `slots` expansions (0 = off)."""
+        _check(lib.pcgb_expander_set_profiling(self.h, int(slots)))
+        self._slots = int(slots)
+
+    def stage_times(self):
+        """[(tops, leaf_gather, x, ntt) ms] of the recorded expansions."""
+        n = max(getattr(self, "_slots", 0), 1)
+        ms = (C.c_float * (4 * n))()
+        r = lib.pcgb_expander_stage_times(self.h, ms, n)
+        if r < 0:
+            _check(r)
+        return [tuple(ms[4 * i: 4 * i + 4]) for i in range(r)]

@@ -1,0 +1,96 @@
+"""GPU DPF parity through the C ABI: keyed eval and the interactive drop-in
+(pcg_cuda::dpf_gpu_batch_full_eval) against the oracle and the reference's
+dpf_real_bench golden checksums."""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from gpu_helpers import dealt_keys, dev, real_bench_checksum, real_bench_inputs
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("prg", [O.PRG_CHACHA8, O.PRG_AES])
+@pytest.mark.parametrize("n,w", [(6, 1), (11, 1), (8, 2), (9, 3), (8, 4)])
+def test_keyed_full_eval_matches_oracle(pcg, prg, n, w):
+    nk = (1 << w) - 1
+    rks = O.aes_tree_round_keys(np.arange(16, dtype=np.uint8), nk) if prg == O.PRG_AES else None
+    K = 6
+    k = dealt_keys(n, w, K, 11 * n + w, prg, rks)
+    want = O.dpf_keyed_full_eval(K, n, w, k["roots0"], k["cws"], prg, rks)
+    d_r, d_c = dev(pcg, k["roots0"]), dev(pcg, k["cws"])
+    d_l = pcg.DeviceBuffer(want.nbytes)
+    pcg.dpf_keyed_full_eval_device(K, n, w, prg, d_r.ptr, d_c.ptr, d_l.ptr, round_keys=rks)
+    got = d_l.download(np.uint64, want.size).reshape(-1, 2)
+    assert (got == want).all()
+
+
+@pytest.mark.parametrize("prg", [O.PRG_CHACHA8, O.PRG_AES])
+@pytest.mark.parametrize("n,w", [(1, 1), (10, 1), (10, 2), (9, 3), (12, 4)])
+def test_interactive_stub_exchange_matches_oracle(pcg, prg, n, w):
+    rng = np.random.default_rng(n * 7 + w)
+    B, nk = 7, (1 << w) - 1
+    rks = O.aes_tree_round_keys(rng.integers(0, 256, 16, dtype=np.uint8), nk) \
+        if prg == O.PRG_AES else None
+    roots = rng.integers(0, 2**64 - 1, (B, 2), dtype=np.uint64)
+    dlt = rng.integers(0, 2**64 - 1, (B * (n // w) * nk, 2), dtype=np.uint64)
+    want = O.dpf_batch_full_eval(B, n, w, roots, dlt, prg, rks)
+    got = pcg.dpf_gpu_batch_full_eval(B, n, w, roots, dlt, round_keys=rks, prg=prg)
+    assert (got == want).all()
+
+
+@pytest.mark.parametrize("prg", [O.PRG_CHACHA8, O.PRG_AES])
+@pytest.mark.parametrize("n,w", [(10, 1), (10, 2), (8, 4)])
+def test_interactive_two_party_matches_keyed(pcg, prg, n, w):
+    """Real DltSft shares; the peer's share is my ^ CW (what the other party
+    sends), so the drop-in must reproduce the dealer's keyed leaves."""
+    nk, L = (1 << w) - 1, n // w
+    rks = O.aes_tree_round_keys(np.arange(16, dtype=np.uint8), nk) if prg == O.PRG_AES else None
+    B = 5
+    k = dealt_keys(n, w, B, 99 + n, prg, rks, with_dlt=True)
+    cw = k["cws"].reshape(B, L, nk, 2)
+    for party, roots, dlt in ((0, k["roots0"], k["dlt0"]), (1, k["roots1"], k["dlt1"])):
+        level = [0]
+
+        def exchange(my):
+            peer = my.reshape(B, nk, 2) ^ cw[:, level[0]]
+            level[0] += 1
+            return peer.reshape(-1, 2)
+
+        got = pcg.dpf_gpu_batch_full_eval(B, n, w, roots, dlt, round_keys=rks, party=party,
+                                          exchange=exchange, prg=prg)
+        assert level[0] == L
+        want = O.dpf_keyed_full_eval(B, n, w, roots, k["cws"], prg, rks)
+        assert (got == want).all()
+
+
+def test_interactive_errors(pcg):
+    roots = np.zeros((2, 2), np.uint64)
+    with pytest.raises(pcg.PcgError, match="w must divide n"):
+        pcg.dpf_gpu_batch_full_eval(2, 5, 2, roots, np.zeros((20, 2), np.uint64),
+                                    prg=pcg.PRG_CHACHA8)
+    with pytest.raises(pcg.PcgError, match=r"w must be in \[1,4\]"):
+        pcg.dpf_gpu_batch_full_eval(2, 10, 5, roots, np.zeros((20, 2), np.uint64),
+                                    prg=pcg.PRG_CHACHA8)
+    with pytest.raises(pcg.PcgError, match="AES PRG requires round_keys"):
+        pcg.dpf_gpu_batch_full_eval(2, 4, 1, roots, np.zeros((8, 2), np.uint64), prg=pcg.PRG_AES)
+    with pytest.raises(pcg.PcgError, match="exchange callback"):
+        pcg.dpf_gpu_batch_full_eval(2, 4, 1, roots, np.zeros((8, 2), np.uint64),
+                                    exchange=lambda my: 1 / 0, prg=pcg.PRG_CHACHA8)
+    assert pcg.dpf_gpu_batch_full_eval_device(0, 4, 1, roots, roots) is None
+
+
+# GPU_baseline/results_l40s/plateau.txt: dpf_real_bench checksums (w=1, chacha8).
+GOLDEN = [(18, 64, 8, 0x16E395FEBFD6D23F), (18, 256, 16, 0x27CB4298E84744ED),
+          (20, 64, 8, 0x104646E15A59C497), (20, 256, 16, 0x204A14F81D54AA7E),
+          (24, 16, 4, 0x02A9707398F918D0)]
+
+
+@pytest.mark.parametrize("n,B,t,want", GOLDEN)
+def test_dpf_real_bench_golden_checksums(pcg, n, B, t, want):
+    roots, dlt, CW = real_bench_inputs(n, B)
+    d_leaves = pcg.dpf_gpu_batch_full_eval_device(B, n, 1, roots, dlt, prg=pcg.PRG_CHACHA8)
+    D = 1 << n
+    sc, st = pcg.dpf_out_sums(d_leaves, B, D)
+    g = pcg.dpf_out_scatter_g(d_leaves, B, D, t, 0, CW, t * (D // 2))
+    assert real_bench_checksum(sc, st, g) == want

@@ -1,0 +1,115 @@
+"""Fused expansion (keyed DPF -> convert -> gather -> NTT products) against
+the oracle's restatement of gen_and_expand's algebra, plus the OLE relation
+at the full N=2^20, c=4, t=16 shape."""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from gpu_helpers import dev
+
+pytestmark = pytest.mark.gpu
+P = O.P
+MASTER = np.array([0x2B, 0x7E, 0x15, 0x16, 0x28, 0xAE, 0xD2, 0xA6, 0xAB, 0xF7, 0x15, 0x88, 0x09,
+                   0xCF, 0x4F, 0x3C], np.uint8)  # pcg_ole_impl.h:89-90
+
+
+def material(s, seed, a_seed, prg):
+    rks = O.aes_tree_round_keys(MASTER, s.nk) if prg == O.PRG_AES else None
+    r0, r1, cws, cwo = O.deal_keys(s, seed, rks)
+    a = O.public_a(s, a_seed)
+    n0 = O.noise(s, seed, 0)
+    n1 = O.noise(s, seed, 1)
+    return rks, (r0, r1), cws, cwo, a, (n0, n1)
+
+
+SHAPES = [(4096, 2, 4, 1, O.PRG_CHACHA8),   # the CPU-runnable configuration
+          (1024, 3, 8, 1, O.PRG_CHACHA8),
+          (2048, 4, 8, 1, O.PRG_AES),
+          (4096, 2, 8, 2, O.PRG_CHACHA8),  # n = 10, w = 2
+          (8192, 1, 64, 1, O.PRG_CHACHA8),
+          (16384, 2, 32, 2, O.PRG_AES)]
+
+
+@pytest.mark.parametrize("N,c,t,w,prg", SHAPES)
+def test_expand_matches_oracle(pcg, N, c, t, w, prg):
+    s = O.shape(N, c, t, w, prg)
+    rks, roots, cws, cwo, a, noise = material(s, 1000 + N + c, 7, prg)
+    e = pcg.Expander(N, c, t, w, prg, public_a=a if c > 1 else None,
+                     master_key=MASTER if prg == O.PRG_AES else None)
+    xs, zs = [], []
+    for party in (0, 1):
+        x, z = e.expand_host(party, roots[party], cws, cwo, *noise[party])
+        wx, wz = O.expand(s, party, roots[party], cws, cwo, *noise[party], a, rks)
+        assert (x == wx).all(), ("x", party)
+        assert (z == wz).all(), ("z", party)
+        xs.append(x), zs.append(z)
+    prod = O.poly_mul(xs[0], xs[1], N)
+    zz = (zs[0].astype(object) + zs[1].astype(object)) % P
+    assert all(int(p) == int(q) for p, q in zip(prod, zz))
+    e.close()
+
+
+@pytest.mark.parametrize("N,c,t,w,prg", SHAPES[:3])
+def test_g_prime_matches_oracle(pcg, N, c, t, w, prg):
+    s = O.shape(N, c, t, w, prg)
+    rks, roots, cws, cwo, a, noise = material(s, 77, 7, prg)
+    e = pcg.Expander(N, c, t, w, prg, public_a=a if c > 1 else None,
+                     master_key=MASTER if prg == O.PRG_AES else None)
+    d_cws, d_cwo = dev(pcg, cws), dev(pcg, cwo)
+    for party in (0, 1):
+        _, _, g = O.expand(s, party, roots[party], cws, cwo, *noise[party], a, rks, want_g=True)
+        g = g.reshape(c, c, N)
+        d_r = dev(pcg, roots[party])
+        d_g = pcg.DeviceBuffer(8 * N * e.Q)
+        e.expand_g_device(party, d_r.ptr, d_cws.ptr, d_cwo.ptr, d_g.ptr)
+        got = d_g.download(np.uint64, N * e.Q).reshape(e.Q, N)
+        q = 0
+        for i in range(c):
+            for j in range(i, c):
+                want = g[i, j] if i == j else (g[i, j].astype(object) + g[j, i]) % P
+                assert (got[q] == np.asarray(want, dtype=np.uint64)).all(), (party, i, j)
+                q += 1
+    e.close()
+
+
+@pytest.mark.parametrize("N,c,t,w,prg", [(4096, 2, 4, 1, O.PRG_CHACHA8), (1 << 14, 4, 16, 1, O.PRG_AES),
+                                         (1 << 16, 4, 16, 2, O.PRG_CHACHA8)])
+def test_gpu_dealer_matches_oracle(pcg, N, c, t, w, prg):
+    s = O.shape(N, c, t, w, prg)
+    rks = O.aes_tree_round_keys(MASTER, s.nk) if prg == O.PRG_AES else None
+    r0, r1, cws, cwo = O.deal_keys(s, 4242, rks)
+    a = O.public_a(s, 1)
+    e = pcg.Expander(N, c, t, w, prg, public_a=a, master_key=MASTER if prg == O.PRG_AES else None)
+    bufs = [pcg.DeviceBuffer(x.nbytes) for x in (r0, r1, cws, cwo)]
+    e.deal_keys_device(4242, *[b.ptr for b in bufs])
+    for b, want in zip(bufs, (r0, r1, cws, cwo)):
+        assert (b.download(np.uint64, want.size).reshape(want.shape) == want).all()
+    e.close()
+
+
+def test_ole_relation_full_shape(pcg):
+    """N = 2^20, c = 4, t = 16 (256 keys of domain 2^17 per block, 4096 keys):
+    z0 + z1 == x0 * x1, with the product on the (oracle-checked) GPU NTT."""
+    N, c, t = 1 << 20, 4, 16
+    a = pcg.public_a(N, c, 12)
+    e = pcg.Expander(N, c, t, 1, pcg.PRG_CHACHA8, public_a=a)
+    K, L = e.K, e.levels
+    d_r0, d_r1 = pcg.DeviceBuffer(16 * K), pcg.DeviceBuffer(16 * K)
+    d_cws, d_cwo = pcg.DeviceBuffer(16 * K * L), pcg.DeviceBuffer(8 * K)
+    e.deal_keys_device(31337, d_r0.ptr, d_r1.ptr, d_cws.ptr, d_cwo.ptr)
+    xs, zs = [], []
+    for party, d_r in ((0, d_r0), (1, d_r1)):
+        pos, val = pcg.noise(N, c, t, 31337, party)
+        d_pos, d_val = dev(pcg, pos), dev(pcg, val)
+        d_x, d_z = pcg.DeviceBuffer(8 * N), pcg.DeviceBuffer(8 * N)
+        e.expand_device(party, d_r.ptr, d_cws.ptr, d_cwo.ptr, d_pos.ptr, d_val.ptr, d_x.ptr,
+                        d_z.ptr)
+        xs.append(d_x.download(np.uint64, N))
+        zs.append(d_z.download(np.uint64, N))
+    prod, _ = pcg.poly_mul_u64_gpuntt(xs[0], xs[1], 1, N)
+    zsum = zs[0] + zs[1]
+    zsum = np.where(zsum >= np.uint64(P), zsum - np.uint64(P), zsum)
+    assert (prod == zsum).all()
+    # x = sum a_i e_i has exactly the dealt noise in a_0's slot.
+    assert np.count_nonzero(xs[0]) > N // 2
+    e.close()
