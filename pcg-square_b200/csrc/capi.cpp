@@ -367,7 +367,7 @@ int pcgb_dpf_keyed_full_eval(int K, int n, int w, int prg, const pcgb_blk* d_roo
                              pcgb_blk* d_leaves, void* stream) {
     if (K <= 0) return PCGB_OK;
     return guarded([&] {
-        if (w < 1 || w > 4 || n < 1 || n % w || n / w > 26) pcgb::fail(PCGB_EINVAL, "keyed eval: bad (n, w)");
+        if (w < 1 || w > 4 || n < 1 || n % w || n > 30) pcgb::fail(PCGB_EINVAL, "keyed eval: bad (n, w)");
         if (prg == PCGB_PRG_AES && !round_keys) pcgb::fail(PCGB_EINVAL, "keyed eval: AES needs round keys");
         cudaStream_t st = pcgb::as_stream(stream);
         const int levels = n / w, nk = (1 << w) - 1;

@@ -40,8 +40,9 @@ namespace {
 constexpr int kPrgAes = PCGB_PRG_AES;
 constexpr int kPrgChaCha = PCGB_PRG_CHACHA8;
 
-// Deepest DFS the tops kernel supports (its per-thread stack size).
-constexpr int kTopsMaxDepth = 26;
+// Per-thread DFS stack depth of the tops kernel: covers n <= 30 for any w.
+template <int W>
+constexpr int tops_max_depth() { return 30 / W + 1; }
 
 struct AesSmem {
     uint32_t te[1024];
@@ -134,7 +135,7 @@ __global__ void __launch_bounds__(128) expand_tops_kernel(
     const Blk* __restrict__ cws, const uint32_t* __restrict__ aes_te,
     const uint32_t* __restrict__ aes_rk, Blk* __restrict__ dst) {
     constexpr int M = 1 << W, NK = M - 1;
-    constexpr int MAXD = kTopsMaxDepth;
+    constexpr int MAXD = tops_max_depth<W>();
     extern __shared__ __align__(16) uint64_t tops_dsm[];
     AesSmem& aes_s = *reinterpret_cast<AesSmem*>(tops_dsm);
     if constexpr (PRG == kPrgAes) load_aes_smem(aes_s, aes_te, aes_rk, NK);
@@ -300,7 +301,7 @@ __global__ void __launch_bounds__(256) leaf_gather_kernel(
 template <int W, int PRG>
 void launch_tops(const Blk* src, int K, int src_lvl, int nlev, int levels, const Blk* cws,
                  const uint32_t* te, const uint32_t* rk, Blk* dst, cudaStream_t st) {
-    if (nlev < 0 || nlev > kTopsMaxDepth) fail(PCGB_EINVAL, "keyed expansion deeper than 26 levels");
+    if (nlev < 0 || nlev >= tops_max_depth<W>()) fail(PCGB_EINVAL, "keyed expansion deeper than the DFS stack");
     const size_t threads = static_cast<size_t>(K) << (W * src_lvl);
     const int TPB = 128;
     const size_t smem = PRG == kPrgAes ? sizeof(AesSmem) : 0;
