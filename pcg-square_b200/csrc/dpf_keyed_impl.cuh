@@ -42,7 +42,7 @@ constexpr int kPrgChaCha = PCGB_PRG_CHACHA8;
 
 // Per-thread DFS stack depth of the tops kernel: covers n <= 30 for any w.
 template <int W>
-constexpr int tops_max_depth() { return 30 / W + 1; }
+__host__ __device__ constexpr int tops_max_depth() { return 30 / W + 1; }
 
 struct AesSmem {
     uint32_t te[1024];
