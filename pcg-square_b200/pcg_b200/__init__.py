@@ -287,15 +287,20 @@ def dpf_gpu_batch_full_eval_device(B, n, w, roots, dltsft, round_keys=None, part
 
 # ---- output layer (leaf_convert_cuda.h:43-52) ------------------------------
 def dpf_out_sums(d_leaves, B, D, prime=P):
+    """Per-instance sumC (mod p) and sumT of the device leaves."""
     sc, st = np.zeros(B, np.uint64), np.zeros(B, np.uint64)
     _check(lib.pcgb_dpf_out_sums(d_leaves, B, D, prime, sc, st))
     return sc, st
 
 
 def dpf_out_scatter_g(d_leaves, B, D, t, party, CW, N, prime=P):
+    """Folded g (N residues) of the B instances' output layer."""
+    CW = np.ascontiguousarray(CW, np.uint64)
+    if B > 0 and CW.size < B:
+        raise ValueError("CW needs B entries")
     g = np.zeros(N, np.uint64)
     _check(lib.pcgb_dpf_out_scatter_g(d_leaves, B, D, t, party, prime,
-                                      np.ascontiguousarray(CW, np.uint64), g, N))
+                                      CW, g, N))
     return g
 
 
@@ -309,6 +314,8 @@ def _supported(variant, prime, N):
 def _mul(variant, a, b, batch, N, prime):
     a = np.ascontiguousarray(a, np.uint64).reshape(-1)
     b = np.ascontiguousarray(b, np.uint64).reshape(-1)
+    if batch > 0 and (a.size < batch * N or b.size < batch * N):
+        raise ValueError(f"poly-mul operands need batch*N = {batch * N} words")
     out = np.zeros(batch * N, np.uint64)
     ms = C.c_double(0)
     _check(lib.pcgb_poly_mul_u64(variant, out, a, b, batch, N, prime, C.byref(ms)))

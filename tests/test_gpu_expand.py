@@ -73,7 +73,7 @@ def test_g_prime_matches_oracle(pcg, N, c, t, w, prg):
 
 
 @pytest.mark.parametrize("N,c,t,w,prg", [(4096, 2, 4, 1, O.PRG_CHACHA8), (1 << 14, 4, 16, 1, O.PRG_AES),
-                                         (1 << 16, 4, 16, 2, O.PRG_CHACHA8)])
+                                         (1 << 15, 4, 16, 2, O.PRG_CHACHA8)])
 def test_gpu_dealer_matches_oracle(pcg, N, c, t, w, prg):
     s = O.shape(N, c, t, w, prg)
     rks = O.aes_tree_round_keys(MASTER, s.nk) if prg == O.PRG_AES else None

@@ -74,7 +74,7 @@ def test_unreduced_inputs(pcg):
 def test_square_verify_schoolbook(pcg, lg):
     """GPU_baseline/square_verify.cu:309-346: vs the schoolbook negacyclic product."""
     N = 1 << lg
-    r = O.mt64(12345 + lg, 6 * N)
+    r = O.mt64(12345 + lg, 8 * N)
     for batch, off in ((1, 0), (3, 2 * N)):
         a = r[off: off + batch * N] % np.uint64(P)
         b = r[off + batch * N: off + 2 * batch * N] % np.uint64(P)

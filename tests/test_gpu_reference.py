@@ -101,8 +101,13 @@ def test_keyed_g_matches_reference_pipeline(pcg, ref):
         assert ref.ref_dpf_batch_full_eval_device(B, n, 1, rts.ctypes.data, dz.ctypes.data, None,
                                                   party, C.cast(cb, C.c_void_p), None, 1,
                                                   C.byref(dl)) == 0
+        # The reference sizes its CW buffer in dpf_out_sums
+        # (leaf_convert_cuda.cu:350), so the pipeline calls it first.
+        sc, st = np.zeros(B, np.uint64), np.zeros(B, np.uint64)
+        assert ref.ref_dpf_out_sums(dl.value, B, D, P, sc, st) == 0
         g = np.zeros(N, np.uint64)
         cwb = np.ascontiguousarray(cwo[blk * B:(blk + 1) * B])
-        assert ref.ref_dpf_out_scatter_g(dl.value, B, D, t, party, P, cwb, g, N) == 0
+        assert ref.ref_dpf_out_scatter_g(dl.value, B, D, t, party, P, cwb, g, N) == 0, \
+            ref.ref_last_error()
         assert (got[0] == g).all()
     e.close()
