@@ -109,6 +109,26 @@ int pcgb_dpf_out_scatter_g(const pcgb_blk* d_leaves, int B, size_t D, int t, int
                            uint64_t prime, const uint64_t* CW_host, uint64_t* g_out_host,
                            int N);
 
+/* Allocation-free variant of pcgb_dpf_out_sums, with no counterpart in the
+ * reference.  It is for callers that must not allocate device memory
+ * themselves or through the library: code whose device memory is owned by a
+ * framework's allocator or capped by a fixed budget, and latency-critical
+ * loops where cudaMalloc's implicit device synchronisation is unacceptable.
+ * The caller passes the leaves and two device output arrays of B words
+ * (d_sumC, d_sumT, same values as sumC_host / sumT_host); the per-CTA
+ * partial sums live in a 1 MiB static device array that every device
+ * loading the library holds until the process exits, which limits B to at
+ * most 65535 instances (larger B is rejected with PCGB_EINVAL).  The call
+ * only enqueues work on `stream`: synchronise before reading the outputs.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls on a device share the array, so
+ * calls that overlap on the GPU (unordered streams) race; each call
+ * overwrites every partial it reads, so nothing needs clearing between
+ * calls.  No cudaMalloc, cudaFree or allocating library routine is used. */
+int pcgb_dpf_out_sums_noalloc(const pcgb_blk* d_leaves, int B, size_t D, uint64_t prime,
+                              uint64_t* d_sumC, uint64_t* d_sumT, void* stream);
+
 /* ---- drop-ins: negacyclic poly-mul (GPU_baseline/common/poly_mul_cuda.h:14-31,
  * plus the merge / 4-step names called from CPU_baseline/pcg_ole_2pc/pcg_ole.h:147,157,226-230).
  * variant selects the supported-size rules of each reference name; all run

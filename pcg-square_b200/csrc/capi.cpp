@@ -24,6 +24,8 @@ void dpf_out_sums_host(const Blk* d_leaves, int B, size_t D, uint64_t prime, uin
 void dpf_out_scatter_host(const Blk* d_leaves, int B, size_t D, int t, int party, uint64_t prime,
                           const uint64_t* CW, uint64_t* g_out, int N);
 void aes_ecb_encrypt_device(const uint8_t* keys, const uint8_t* in, uint8_t* out, int count);
+void dpf_out_sums_noalloc(const Blk* d_leaves, int B, size_t D, uint64_t prime, uint64_t* d_sumC,
+                          uint64_t* d_sumT, cudaStream_t st);
 pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64_t* public_a,
                                const uint8_t* master_key);
 void expander_destroy(pcgb_expander* e);
@@ -290,6 +292,15 @@ int pcgb_dpf_out_scatter_g(const pcgb_blk* d_leaves, int B, size_t D, int t, int
     return guarded([&] {
         pcgb::dpf_out_scatter_host(reinterpret_cast<const Blk*>(d_leaves), B, D, t, party, prime,
                                    CW_host, g_out_host, N);
+    });
+}
+
+int pcgb_dpf_out_sums_noalloc(const pcgb_blk* d_leaves, int B, size_t D, uint64_t prime,
+                              uint64_t* d_sumC, uint64_t* d_sumT, void* stream) {
+    if (B <= 0) return PCGB_OK;
+    return guarded([&] {
+        pcgb::dpf_out_sums_noalloc(reinterpret_cast<const Blk*>(d_leaves), B, D, prime, d_sumC,
+                                   d_sumT, pcgb::as_stream(stream));
     });
 }
 

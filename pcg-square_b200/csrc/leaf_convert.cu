@@ -13,7 +13,9 @@
 // CAS-loop modular atomic, leaf_convert_cuda.cu:68-77,207-234).
 #include "pcgb_internal.h"
 
+#include <algorithm>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "chacha8.cuh"
@@ -186,6 +188,69 @@ void dpf_out_sums_host(const Blk* d_leaves, int B, size_t D, uint64_t prime, uin
         sumC[b] = both[b];
         sumT[b] = both[B + b];
     }
+}
+
+// ---- allocation-free sums ---------------------------------------------------
+// Per-CTA partial sums of pcgb_dpf_out_sums_noalloc.  A file-scope device
+// array: every device that loads the library holds these 1 MiB until the
+// process exits, and all calls on a device share it.
+constexpr size_t kNoAllocScratchWords = size_t{1} << 17;
+static __device__ __align__(256) uint64_t g_noalloc_partials[kNoAllocScratchWords];
+
+namespace {
+
+// Splits the folded sums into the caller's two output arrays.
+__global__ void out_fold_split_kernel(const uint64_t* __restrict__ partials, int parts, int B,
+                                      uint64_t* __restrict__ sumC, uint64_t* __restrict__ sumT) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    uint64_t c = 0, t = 0;
+    for (int i = 0; i < parts; ++i) {
+        c = add_p(c, partials[static_cast<size_t>(b) * parts + i]);
+        t += partials[static_cast<size_t>(B) * parts + static_cast<size_t>(b) * parts + i];
+    }
+    sumC[b] = c;
+    sumT[b] = t;
+}
+
+// Device address of the scratch array on the current device.  Host code
+// only sees a host-side stand-in for g_noalloc_partials, so the address is
+// looked up once per device with that device current.
+uint64_t* noalloc_partials() {
+    static std::mutex mu;
+    static uint64_t* addr[64] = {nullptr};
+    int dev = 0;
+    PCGB_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) fail(PCGB_EINVAL, "device index out of range");
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        PCGB_CK(cudaGetSymbolAddress(&p, g_noalloc_partials));
+        addr[dev] = static_cast<uint64_t*>(p);
+    }
+    return addr[dev];
+}
+
+}  // namespace
+
+void dpf_out_sums_noalloc(const Blk* d_leaves, int B, size_t D, uint64_t prime, uint64_t* d_sumC,
+                          uint64_t* d_sumT, cudaStream_t st) {
+    if (B <= 0) return;
+    check_common(d_leaves, B, D, prime);
+    if (!d_sumC || !d_sumT) fail(PCGB_EINVAL, "dpf_out_sums_noalloc: null output array");
+    const size_t max_b = kNoAllocScratchWords / 2;
+    if (B > 65535 || static_cast<size_t>(B) > max_b)
+        fail(PCGB_EINVAL, "dpf_out_sums_noalloc: B = " + std::to_string(B) +
+                              " exceeds the limit of 65535 instances of the static scratch");
+    // Fewer partials per instance when B is large, so they fit the array.
+    const size_t fit = kNoAllocScratchWords / (2 * static_cast<size_t>(B));
+    const int parts = static_cast<int>(std::min<size_t>(out_sums_parts(D), fit));
+    uint64_t* partials = noalloc_partials();
+    out_sum_kernel<<<dim3(parts, B), kTPB, 0, st>>>(reinterpret_cast<const ulonglong2*>(d_leaves),
+                                                    D, partials);
+    PCGB_POST_LAUNCH();
+    out_fold_split_kernel<<<(B + 127) / 128, 128, 0, st>>>(partials, parts, B, d_sumC, d_sumT);
+    PCGB_POST_LAUNCH();
 }
 
 void dpf_out_scatter_host(const Blk* d_leaves, int B, size_t D, int t, int party, uint64_t prime,

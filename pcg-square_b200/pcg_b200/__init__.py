@@ -67,6 +67,8 @@ def _load():
         "pcgb_dpf_out_sums": ([_vp, C.c_int, C.c_size_t, C.c_uint64, _u64p, _u64p], C.c_int),
         "pcgb_dpf_out_scatter_g": ([_vp, C.c_int, C.c_size_t, C.c_int, C.c_int, C.c_uint64, _u64p,
                                     _u64p, C.c_int], C.c_int),
+        "pcgb_dpf_out_sums_noalloc": ([_vp, C.c_int, C.c_size_t, C.c_uint64, _vp, _vp, _vp],
+                                      C.c_int),
         "pcgb_poly_mul_supported": ([C.c_int, C.c_uint64, C.c_int, C.c_char_p, C.c_size_t],
                                     C.c_int),
         "pcgb_poly_mul_u64": ([C.c_int, _u64p, _u64p, _u64p, C.c_int, C.c_int, C.c_uint64,
