@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-verify", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=200,
+                    help="seeded subsample of the serving stream (0 = skip)")
     # Smaller shapes for profiler captures; the bench line is quoted at the defaults.
     ap.add_argument("--N", type=int, default=N)
     ap.add_argument("--c", type=int, default=C_)
@@ -335,6 +337,10 @@ def run_ours(args, d):
         cpu = {"value": v, "unit": "corr/s", "cores": threads, "kind": "port",
                "sample": desc, "sample_seconds": sec}
 
+    serve = None
+    if d.world == 1 and args.serve_requests > 0:
+        serve = run_serving(L, args.serve_requests)
+
     if d.rank == 0:
         stage_means = [float(np.mean([s[i] for s in stages])) for i in range(4)] if stages else None
         line = {
@@ -355,10 +361,59 @@ def run_ours(args, d):
             "bit_exact_ole_relation": verified,
             "gpu_launches": int(launches),
             "clocks": clk, "roofline": roofline, "roofline_ntt": roofline_ntt,
-            "e2e": e2e, "cpu_baseline": cpu,
+            "e2e": e2e, "cpu_baseline": cpu, "serve": serve,
         }
         print(json.dumps(line), flush=True)
     e.close()
+
+
+SERVE_SHAPES = [(1 << lg, c, t) for lg in (14, 16, 18, 20, 22) for c in (2, 4) for t in (8, 16, 32)]
+
+
+def run_serving(L, n_req, seed=2025, util=0.85):
+    """Serving stream (N in {2^14..2^22}, c in {2,4}, t in {8,16,32}, Poisson
+    arrivals): continuous batching (4 streams) vs one request at a time on the
+    same seeded trace.  Every request deals fresh keys and noise on the GPU;
+    the a_i plans of all 30 shapes are resident before the trace starts."""
+    rng = np.random.default_rng(seed)
+    batched = L.Server(n_streams=4, a_seed=A_SEED)
+    single = L.Server(n_streams=1, max_in_flight=1, a_seed=A_SEED)
+    for shp in SERVE_SHAPES:
+        batched.prepare(*shp)
+        single.prepare(*shp)
+    # Calibrate the arrival rate on the mean one-at-a-time service time.
+    calib = [SERVE_SHAPES[i] for i in rng.integers(len(SERVE_SHAPES), size=24)]
+    res = single.run_trace([(N, c, t, 0, 1000 + i, 0.0) for i, (N, c, t) in enumerate(calib)])
+    svc = float(np.mean([r.done_s - r.start_s for r in res]))
+    rate = util / svc
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    trace = []
+    for i in range(n_req):
+        N, c, t = SERVE_SHAPES[rng.integers(len(SERVE_SHAPES))]
+        trace.append((N, c, t, int(rng.integers(2)), int(rng.integers(1, 2**62)),
+                      float(arrivals[i])))
+    out = {}
+    runs = {}
+    for name, srv in (("batched", batched), ("one_at_a_time", single)):
+        rs = srv.run_trace(trace, timeout_s=900)
+        lat = np.array([r.done_s - r.submit_s for r in rs]) * 1e3
+        span = max(r.done_s for r in rs) - min(r.submit_s for r in rs)
+        out[name] = {"p50_ms": float(np.percentile(lat, 50)),
+                     "p99_ms": float(np.percentile(lat, 99)),
+                     "mean_ms": float(lat.mean()),
+                     "corr_per_s": float(sum(tr[0] for tr in trace) / span)}
+        runs[name] = [(r.digest_x, r.digest_z) for r in rs]
+    batched.close()
+    single.close()
+    out["bit_exact_alone_vs_mix"] = runs["batched"] == runs["one_at_a_time"]
+    out["requests"] = n_req
+    out["arrival_rate_per_s"] = rate
+    out["mean_service_ms_one_at_a_time"] = svc * 1e3
+    out["trace"] = ("seeded subsample of the 10,000-request stream: N uniform over "
+                    "2^14..2^22, c in {2,4}, t in {8,16,32}, Poisson arrivals at "
+                    f"{util:.0%} of one-at-a-time capacity")
+    out["speedup_p99"] = out["one_at_a_time"]["p99_ms"] / out["batched"]["p99_ms"]
+    return out
 
 
 # DRAM bytes per launch of the leaf kernel from the ncu capture summarised in

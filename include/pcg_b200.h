@@ -211,6 +211,46 @@ int pcgb_deal_keys_device(pcgb_expander* e, uint64_t seed, pcgb_blk* d_roots0,
                           pcgb_blk* d_roots1, pcgb_blk* d_cws, uint64_t* d_cw_out,
                           void* stream);
 
+/* ---- native: serving ------------------------------------------------------
+ * Continuous batching of expansion requests of mixed (N, c, t) on one GPU:
+ * requests wait in a FIFO and are admitted onto one of n_streams streams as
+ * soon as a stream is free, fewer than max_in_flight are running and the
+ * request's HBM footprint (keys, noise, outputs, expansion workspace) fits
+ * mem_budget (0 = half of the free memory) next to what is in flight, so
+ * their kernels overlap on the device.  Each request deals fresh keys and
+ * noise on the GPU from its seed (w = 1, ChaCha8), expands one party against
+ * the shape's resident plan (a_i images from a_seed), and reports order-
+ * independent digests of x and z (pcgb_digest_device).  n_streams = 1 with
+ * max_in_flight = 1 is one-request-at-a-time execution. */
+typedef struct pcgb_server pcgb_server;
+typedef struct pcgb_request {
+    int N, c, t, party;
+    uint64_t seed;
+    double arrival_s; /* offset from the start of pcgb_server_run_trace */
+} pcgb_request;
+typedef struct pcgb_result {
+    uint64_t digest_x, digest_z;
+    double submit_s, start_s, done_s; /* seconds since the server started */
+    int status;
+    int reserved;
+} pcgb_result;
+int pcgb_server_create(pcgb_server** s, int n_streams, size_t mem_budget, int max_in_flight,
+                       uint64_t a_seed);
+/* Build (and keep resident) the plan of a shape before requests arrive. */
+int pcgb_server_prepare(pcgb_server* s, int N, int c, int t);
+int pcgb_server_submit(pcgb_server* s, const pcgb_request* r, uint64_t* ticket);
+/* Wait for a ticket (timeout_ms < 0: no limit); PCGB_ETIMEOUT if not done. */
+int pcgb_server_wait(pcgb_server* s, uint64_t ticket, pcgb_result* out, int timeout_ms);
+/* Submit reqs[i] at arrival_s[i] after the call starts, then wait for all. */
+int pcgb_server_run_trace(pcgb_server* s, const pcgb_request* reqs, int n, pcgb_result* out,
+                          double timeout_s);
+int pcgb_server_stats(pcgb_server* s, int* pending, int* in_flight, size_t* bytes_in_flight,
+                      int* plans);
+/* Cancels pending requests, waits up to timeout_ms for in-flight ones. */
+int pcgb_server_destroy(pcgb_server* s, int timeout_ms);
+/* d_out[0] = sum over i of mix64(d_v[i] ^ i*0x9e3779b97f4a7c15) mod 2^64. */
+int pcgb_digest_device(const uint64_t* d_v, size_t n, uint64_t* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

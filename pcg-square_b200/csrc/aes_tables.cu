@@ -141,7 +141,7 @@ const uint32_t* aes_te_table_device() {
     if (!per_dev[dev]) {
         uint32_t* d = nullptr;
         PCGB_CK(cudaMalloc(&d, sizeof(uint32_t) * 1024));
-        PCGB_CK(cudaMemcpy(d, host_tables().te, sizeof(uint32_t) * 1024, cudaMemcpyHostToDevice));
+        upload_blocking(d, host_tables().te, sizeof(uint32_t) * 1024);
         per_dev[dev] = d;
     }
     return per_dev[dev];

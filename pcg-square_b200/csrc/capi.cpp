@@ -45,6 +45,14 @@ void public_a_host(int N, int c, uint64_t a_seed, uint64_t* a);
 void deal_keys_device(pcgb_expander* e, uint64_t seed, Blk* r0, Blk* r1, Blk* cws, uint64_t* cwo,
                       cudaStream_t st);
 unsigned long long launch_count();
+pcgb_server* server_create(int n_streams, size_t budget, int max_in_flight, uint64_t a_seed);
+void server_prepare(pcgb_server* s, int N, int c, int t);
+uint64_t server_submit(pcgb_server* s, const pcgb_request& r);
+int server_wait(pcgb_server* s, uint64_t ticket, pcgb_result* out, int timeout_ms);
+void server_run_trace(pcgb_server* s, const pcgb_request* reqs, int n, pcgb_result* out,
+                      double timeout_s);
+void server_destroy(pcgb_server* s, int timeout_ms);
+void server_stats(pcgb_server* s, int* pending, int* in_flight, size_t* bytes, int* plans);
 double arx_probe(float* ms_out);
 
 namespace {
@@ -113,6 +121,12 @@ cudaStream_t default_stream() {
     if (!streams[dev]) check_cuda(cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking),
                                   "cudaStreamCreate");
     return streams[dev];
+}
+
+void upload_blocking(void* d_dst, const void* src, size_t bytes) {
+    cudaStream_t st = default_stream();
+    check_cuda(cudaMemcpyAsync(d_dst, src, bytes, cudaMemcpyHostToDevice, st), "upload");
+    check_cuda(cudaStreamSynchronize(st), "upload sync");
 }
 
 int sm_count() {
@@ -528,6 +542,69 @@ int pcgb_deal_keys_device(pcgb_expander* e, uint64_t seed, pcgb_blk* d_roots0, p
         pcgb::deal_keys_device(e, seed, reinterpret_cast<Blk*>(d_roots0),
                                reinterpret_cast<Blk*>(d_roots1), reinterpret_cast<Blk*>(d_cws),
                                d_cw_out, pcgb::as_stream(stream));
+    });
+}
+
+// ---- serving ------------------------------------------------------------------
+int pcgb_server_create(pcgb_server** s, int n_streams, size_t mem_budget, int max_in_flight,
+                       uint64_t a_seed) {
+    if (s) *s = nullptr;
+    return guarded([&] {
+        if (!s) pcgb::fail(PCGB_EINVAL, "null server handle");
+        *s = pcgb::server_create(n_streams, mem_budget, max_in_flight, a_seed);
+    });
+}
+
+int pcgb_server_prepare(pcgb_server* s, int N, int c, int t) {
+    return guarded([&] {
+        if (!s) pcgb::fail(PCGB_EINVAL, "null server");
+        pcgb::server_prepare(s, N, c, t);
+    });
+}
+
+int pcgb_server_submit(pcgb_server* s, const pcgb_request* r, uint64_t* ticket) {
+    return guarded([&] {
+        if (!s || !r || !ticket) pcgb::fail(PCGB_EINVAL, "null argument");
+        *ticket = pcgb::server_submit(s, *r);
+    });
+}
+
+int pcgb_server_wait(pcgb_server* s, uint64_t ticket, pcgb_result* out, int timeout_ms) {
+    int rc = PCGB_OK;
+    const int g = guarded([&] {
+        if (!s) pcgb::fail(PCGB_EINVAL, "null server");
+        rc = pcgb::server_wait(s, ticket, out, timeout_ms);
+        if (rc == PCGB_ETIMEOUT) pcgb::fail(PCGB_ETIMEOUT, "server_wait: timed out");
+    });
+    return g;
+}
+
+int pcgb_server_run_trace(pcgb_server* s, const pcgb_request* reqs, int n, pcgb_result* out,
+                          double timeout_s) {
+    return guarded([&] {
+        if (!s || (n > 0 && !reqs)) pcgb::fail(PCGB_EINVAL, "null argument");
+        pcgb::server_run_trace(s, reqs, n, out, timeout_s);
+    });
+}
+
+int pcgb_server_stats(pcgb_server* s, int* pending, int* in_flight, size_t* bytes_in_flight,
+                      int* plans) {
+    return guarded([&] {
+        if (!s) pcgb::fail(PCGB_EINVAL, "null server");
+        pcgb::server_stats(s, pending, in_flight, bytes_in_flight, plans);
+    });
+}
+
+int pcgb_server_destroy(pcgb_server* s, int timeout_ms) {
+    return guarded([&] {
+        if (s) pcgb::server_destroy(s, timeout_ms);
+    });
+}
+
+int pcgb_digest_device(const uint64_t* d_v, size_t n, uint64_t* d_out, void* stream) {
+    return guarded([&] {
+        if (!d_v || !d_out) pcgb::fail(PCGB_EINVAL, "null argument");
+        pcgb::digest_device(d_v, n, d_out, pcgb::as_stream(stream));
     });
 }
 

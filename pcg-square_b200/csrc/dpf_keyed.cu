@@ -87,13 +87,10 @@ void gather_plan_build(GatherPlan& gp, int N, int c, int t, int n, int w) {
     PCGB_CK(cudaMalloc(&gp.d_off, off.size() * sizeof(uint32_t)));
     PCGB_CK(cudaMalloc(&gp.d_entries, std::max<size_t>(ent.size(), 1) * sizeof(uint32_t)));
     PCGB_CK(cudaMalloc(&gp.d_qorder, order.size() * sizeof(uint16_t)));
-    PCGB_CK(cudaMemcpy(gp.d_off, off.data(), off.size() * sizeof(uint32_t),
-                       cudaMemcpyHostToDevice));
+    upload_blocking(gp.d_off, off.data(), off.size() * sizeof(uint32_t));
     if (!ent.empty())
-        PCGB_CK(cudaMemcpy(gp.d_entries, ent.data(), ent.size() * sizeof(uint32_t),
-                           cudaMemcpyHostToDevice));
-    PCGB_CK(cudaMemcpy(gp.d_qorder, order.data(), order.size() * sizeof(uint16_t),
-                       cudaMemcpyHostToDevice));
+        upload_blocking(gp.d_entries, ent.data(), ent.size() * sizeof(uint32_t));
+    upload_blocking(gp.d_qorder, order.data(), order.size() * sizeof(uint16_t));
     gp.pair_ij = pair_ij;
 }
 

@@ -83,6 +83,25 @@ __global__ void noise_kernel(uint64_t seed, int party, int ct, uint64_t bin, int
     val[i] = synth_value(seed, party, i);
 }
 
+// Order-independent 64-bit fingerprint of a word vector: sum (mod 2^64) of
+// mix(v[i] ^ i*phi).  Used to compare outputs across runs without moving
+// them to the host.
+__global__ void digest_kernel(const uint64_t* __restrict__ v, size_t n, unsigned long long* out) {
+    __shared__ unsigned long long part[32];
+    unsigned long long acc = 0;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x)
+        acc += mix64(v[i] ^ (i * 0x9e3779b97f4a7c15ULL));
+    for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long s = 0;
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += part[w];
+        atomicAdd(out, s);
+    }
+}
+
 unsigned blocks_for(size_t n, int tpb) { return static_cast<unsigned>((n + tpb - 1) / tpb); }
 
 int ilog2(uint64_t v) {
@@ -145,7 +164,7 @@ pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64
         if (c > 1) {
             uint64_t* tmp = nullptr;
             PCGB_CK(cudaMalloc(&tmp, sizeof(uint64_t) * NN * (c - 1)));
-            PCGB_CK(cudaMemcpy(tmp, public_a, sizeof(uint64_t) * NN * (c - 1), cudaMemcpyHostToDevice));
+            upload_blocking(tmp, public_a, sizeof(uint64_t) * NN * (c - 1));
             reduce_mod_p(tmp, tmp, NN * (c - 1), st);
             scale_kernel<<<blocks_for(NN * (c - 1), 256), 256, 0, st>>>(e->d_aR, tmp, NN * (c - 1), r2);
             PCGB_POST_LAUNCH();
@@ -169,18 +188,12 @@ pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64
             aes_tree_round_keys_host(master_key, e->nk, rks.data());
             e->d_rk = aes_upload_round_keys(rks.data(), e->nk, st);
         }
-        const size_t fnodes = static_cast<size_t>(e->K) << (w * e->gp.hl);
-        const size_t tnodes = keyed_tops_scratch_nodes(e->K, w, e->gp.hl);
-        PCGB_CK(cudaMalloc(&e->d_F, sizeof(Blk) * fnodes));
-        if (tnodes) PCGB_CK(cudaMalloc(&e->d_tops, sizeof(Blk) * tnodes));
-        PCGB_CK(cudaMalloc(&e->d_g, sizeof(uint64_t) * NN * e->Q));
-        e->scratch_bytes = sizeof(Blk) * (fnodes + tnodes) + sizeof(uint64_t) * NN * e->Q;
+        e->scratch_bytes = workspace_bytes(e);  // allocated on first direct use
         PCGB_CK(cudaStreamSynchronize(st));
     } catch (...) {
         // release what was allocated, then rethrow
         gather_plan_free(e->gp);
-        cudaFree(e->d_img); cudaFree(e->d_aR); cudaFree(e->d_F); cudaFree(e->d_tops);
-        cudaFree(e->d_g); cudaFree(e->d_rk);
+        cudaFree(e->d_img); cudaFree(e->d_aR); cudaFree(e->d_F); cudaFree(e->d_rk);
         delete e;
         throw;
     }
@@ -194,33 +207,73 @@ void expander_destroy(pcgb_expander* e) {
     cudaSetDevice(e->dev);
     cudaStreamSynchronize(default_stream());
     gather_plan_free(e->gp);
-    cudaFree(e->d_img); cudaFree(e->d_aR); cudaFree(e->d_F); cudaFree(e->d_tops);
-    cudaFree(e->d_g); cudaFree(e->d_rk); cudaFree(e->d_in);
+    cudaFree(e->d_img); cudaFree(e->d_aR); cudaFree(e->d_F); cudaFree(e->d_rk);
+    cudaFree(e->d_in);
     if (e->h_stage) cudaFreeHost(e->h_stage);
     for (auto& ev : e->prof_ev) cudaEventDestroy(ev);
     cudaSetDevice(cur);
     delete e;
 }
 
-void expand_device(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
-                   const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val, uint64_t* x,
-                   uint64_t* z, cudaStream_t st) {
+// Scratch of one in-flight expansion: the frontier, the first-stage tops
+// and the g' buffers.  An expander owns one; the server carves one per
+// admitted request so expansions of the same shape can overlap.
+size_t workspace_bytes(const pcgb_expander* e) {
+    const size_t fnodes = static_cast<size_t>(e->K) << (e->w * e->gp.hl);
+    const size_t tnodes = keyed_tops_scratch_nodes(e->K, e->w, e->gp.hl);
+    return sizeof(Blk) * (fnodes + tnodes) + sizeof(uint64_t) * static_cast<size_t>(e->N) * e->Q;
+}
+
+Workspace workspace_carve(const pcgb_expander* e, void* base) {
+    const size_t fnodes = static_cast<size_t>(e->K) << (e->w * e->gp.hl);
+    const size_t tnodes = keyed_tops_scratch_nodes(e->K, e->w, e->gp.hl);
+    Workspace ws;
+    ws.F = static_cast<Blk*>(base);
+    ws.tops = tnodes ? ws.F + fnodes : nullptr;
+    ws.g = reinterpret_cast<uint64_t*>(ws.F + fnodes + tnodes);
+    return ws;
+}
+
+void expand_device_ws(pcgb_expander* e, const Workspace& ws, int party, const Blk* roots,
+                      const Blk* cws, const uint64_t* cw_out, const uint64_t* pos,
+                      const uint64_t* val, uint64_t* x, uint64_t* z, cudaStream_t st) {
     if (party != 0 && party != 1) fail(PCGB_EINVAL, "expand: party must be 0 or 1");
     if (!roots || !cws || !cw_out || !pos || !val || !x || !z) fail(PCGB_EINVAL, "expand: null pointer");
     const size_t NN = static_cast<size_t>(e->N);
     cudaEvent_t* ev = nullptr;
     if (e->prof_slots > 0 && e->prof_used < e->prof_slots) ev = &e->prof_ev[5 * e->prof_used++];
     if (ev) PCGB_CK(cudaEventRecord(ev[0], st));
-    keyed_expand_tops(e->K, e->n, e->w, e->prg, roots, cws, e->d_rk, e->gp.hl, e->d_F, e->d_tops, st);
+    keyed_expand_tops(e->K, e->n, e->w, e->prg, roots, cws, e->d_rk, e->gp.hl, ws.F, ws.tops, st);
     if (ev) PCGB_CK(cudaEventRecord(ev[1], st));
-    keyed_leaf_gather(e->gp, party, e->prg, e->d_F, cws, cw_out, e->d_rk, e->d_g, st);
+    keyed_leaf_gather(e->gp, party, e->prg, ws.F, cws, cw_out, e->d_rk, ws.g, st);
     if (ev) PCGB_CK(cudaEventRecord(ev[2], st));
     const size_t sm = sizeof(uint64_t) * 2 * static_cast<size_t>(e->c) * e->t;
     x_kernel<<<blocks_for(NN, 256), 256, sm, st>>>(pos, val, e->d_aR, e->c, e->t, NN, x);
     PCGB_POST_LAUNCH();
     if (ev) PCGB_CK(cudaEventRecord(ev[3], st));
-    ntt_mac_inverse(*e->ntt, e->d_g, e->d_img, e->Q, z, st);
+    ntt_mac_inverse(*e->ntt, ws.g, e->d_img, e->Q, z, st);
     if (ev) PCGB_CK(cudaEventRecord(ev[4], st));
+}
+
+// The expander's own workspace, allocated on first use (plans held by the
+// server never need it: requests bring their own).
+void ensure_own_workspace(pcgb_expander* e) {
+    if (e->d_F) return;
+    PCGB_CK(cudaMalloc(&e->d_F, e->scratch_bytes));
+    const Workspace ws = workspace_carve(e, e->d_F);
+    e->d_tops = ws.tops;
+    e->d_g = ws.g;
+}
+
+void expand_device(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
+                   const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val, uint64_t* x,
+                   uint64_t* z, cudaStream_t st) {
+    ensure_own_workspace(e);
+    Workspace ws;
+    ws.F = e->d_F;
+    ws.tops = e->d_tops;
+    ws.g = e->d_g;
+    expand_device_ws(e, ws, party, roots, cws, cw_out, pos, val, x, z, st);
 }
 
 void expand_host(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
@@ -259,8 +312,18 @@ void expand_host(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
 
 void expand_g_device(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
                      const uint64_t* cw_out, uint64_t* d_g, cudaStream_t st) {
+    if (!roots || !cws || !cw_out || !d_g) fail(PCGB_EINVAL, "expand_g: null pointer");
+    ensure_own_workspace(e);
     keyed_expand_tops(e->K, e->n, e->w, e->prg, roots, cws, e->d_rk, e->gp.hl, e->d_F, e->d_tops, st);
     keyed_leaf_gather(e->gp, party, e->prg, e->d_F, cws, cw_out, e->d_rk, d_g, st);
+}
+
+// out (device, one word) = digest of d[0..n); accumulates, so zero it first.
+void digest_device(const uint64_t* d, size_t n, uint64_t* out, cudaStream_t st) {
+    PCGB_CK(cudaMemsetAsync(out, 0, sizeof(uint64_t), st));
+    const unsigned grid = static_cast<unsigned>(std::min<size_t>((n + 255) / 256, 1024));
+    digest_kernel<<<grid, 256, 0, st>>>(d, n, reinterpret_cast<unsigned long long*>(out));
+    PCGB_POST_LAUNCH();
 }
 
 void noise_device(int N, int c, int t, uint64_t seed, int party, uint64_t* pos, uint64_t* val,

@@ -287,7 +287,7 @@ ulonglong2* upload_psi_table(uint64_t psi_n, int logn) {
     }
     ulonglong2* d = nullptr;
     PCGB_CK(cudaMalloc(&d, sizeof(ulonglong2) * n));
-    PCGB_CK(cudaMemcpy(d, t.data(), sizeof(ulonglong2) * n, cudaMemcpyHostToDevice));
+    upload_blocking(d, t.data(), sizeof(ulonglong2) * n);
     return d;
 }
 
@@ -317,7 +317,7 @@ NttPlan* build_plan(int logN) {
     for (int b = 0; b < logN + 2; ++b) { powR[b] = mul_p_host(pb, R); pb = mul_p_host(pb, pb); }
     uint64_t* d_pow = nullptr;
     PCGB_CK(cudaMalloc(&d_pow, sizeof(uint64_t) * powR.size()));
-    PCGB_CK(cudaMemcpy(d_pow, powR.data(), sizeof(uint64_t) * powR.size(), cudaMemcpyHostToDevice));
+    upload_blocking(d_pow, powR.data(), sizeof(uint64_t) * powR.size());
     const uint64_t ninvR = mul_p_host(pow_p_host(pl->N % kPm, kPm - 2), R);
     twiddle_kernel<<<static_cast<unsigned>((pl->N + 255) / 256), 256>>>(pl->W, pl->Wi, pl->l1,
                                                                         pl->l2, d_pow, R, ninvR);

@@ -50,6 +50,11 @@ inline cudaStream_t as_stream(void* s) {
     return s ? static_cast<cudaStream_t>(s) : default_stream();
 }
 
+// Host-to-device copy that has landed when the call returns: a plain
+// cudaMemcpy from pageable memory may return before its DMA completes, and
+// work on the library's non-blocking streams is not ordered after it.
+void upload_blocking(void* d_dst, const void* src, size_t bytes);
+
 // Number of SMs of the current device.
 int sm_count();
 
@@ -120,6 +125,28 @@ PCGB_KEYED_DECL(aes)
 void keyed_leaf_gather(const GatherPlan& gp, int party, int prg, const Blk* F, const Blk* cws,
                        const uint64_t* cw_out, const uint32_t* d_aes_rk, uint64_t* gq,
                        cudaStream_t st);
+
+// ---- expander internals (expand.cu) ----------------------------------------
+struct Workspace {
+    Blk* F = nullptr;
+    Blk* tops = nullptr;
+    uint64_t* g = nullptr;
+};
+pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64_t* public_a,
+                               const uint8_t* master_key);
+void expander_destroy(pcgb_expander* e);
+void expander_info(const pcgb_expander* e, int* K, int* levels, int* nk, size_t* scratch);
+size_t workspace_bytes(const pcgb_expander* e);
+Workspace workspace_carve(const pcgb_expander* e, void* base);
+void expand_device_ws(pcgb_expander* e, const Workspace& ws, int party, const Blk* roots,
+                      const Blk* cws, const uint64_t* cw_out, const uint64_t* pos,
+                      const uint64_t* val, uint64_t* x, uint64_t* z, cudaStream_t st);
+void deal_keys_device(pcgb_expander* e, uint64_t seed, Blk* r0, Blk* r1, Blk* cws, uint64_t* cwo,
+                      cudaStream_t st);
+void noise_device(int N, int c, int t, uint64_t seed, int party, uint64_t* pos, uint64_t* val,
+                  cudaStream_t st);
+void public_a_host(int N, int c, uint64_t a_seed, uint64_t* a);
+void digest_device(const uint64_t* d, size_t n, uint64_t* out, cudaStream_t st);
 
 // ---- AES tree PRG (aes_tables.cu) ---------------------------------------
 // Round keys as 44 little-endian words per sub-key, on the device.

@@ -1,0 +1,385 @@
+// Serving loop: continuous batching of PCG-OLE expansion requests on one GPU.
+//
+// A worker thread owns S CUDA streams ("slots").  Requests wait in a FIFO;
+// the head is admitted as soon as a slot is free and its HBM footprint
+// (keys, noise, outputs and the expansion workspace) fits the memory budget
+// next to everything already in flight, so requests that arrive while others
+// are on the GPU start immediately and their kernels overlap on the device.
+// Each admitted request runs on its slot's stream: GPU dealer (fresh seeded
+// keys), noise, the fused expansion against the shape's resident plan (a_i
+// images, gather plan, NTT tables), and a device digest of x and z; a host
+// callback (cudaLaunchHostFunc) stamps the completion time and wakes the
+// worker.  Memory comes from the stream-ordered pool (cudaMallocAsync /
+// cudaFreeAsync on the slot's stream), so a finished request's memory is
+// reused by the next one without a device synchronisation.
+//
+// The reference has no serving path; its one-request-at-a-time flow is
+// GPU_baseline/e2e_full_bench.cu's serial arm.
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+#include "pcg_b200.h"
+#include "pcgb_internal.h"
+
+namespace pcgb {
+namespace {
+
+using clk = std::chrono::steady_clock;
+
+struct Req {
+    uint64_t ticket = 0;
+    pcgb_request r{};
+    int state = 0;  // 0 pending, 1 running, 2 done, 3 failed
+    int slot = -1;
+    size_t bytes = 0;
+    double submit_s = 0, start_s = 0, done_s = 0;
+    uint64_t dx = 0, dz = 0;
+    int status = 0;
+    std::string err;
+};
+
+struct CallbackCtx {
+    pcgb_server* s;
+    Req* r;
+};
+
+size_t align256(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
+
+}  // namespace
+}  // namespace pcgb
+
+struct pcgb_server {
+    int dev = 0;
+    int n_slots = 1;
+    size_t budget = 0;
+    int max_in_flight = 1;
+    uint64_t a_seed = 0;
+    std::vector<cudaStream_t> streams;
+    std::vector<pcgb::Req*> slot_req;
+    uint64_t* h_digest = nullptr;  // pinned, 2 words per slot
+    std::mutex plans_mu;
+    std::map<std::tuple<int, int, int>, pcgb_expander*> plans;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<pcgb::Req*> pending;
+    std::vector<pcgb::Req*> finished;  // filled by host callbacks
+    std::unordered_map<uint64_t, std::unique_ptr<pcgb::Req>> reqs;
+    size_t in_flight_bytes = 0;
+    int in_flight = 0;
+    uint64_t next_ticket = 1;
+    bool stopping = false;
+    std::thread worker;
+    pcgb::clk::time_point t0;
+
+    double now() const {
+        return std::chrono::duration<double>(pcgb::clk::now() - t0).count();
+    }
+};
+
+namespace pcgb {
+namespace {
+
+void validate(const pcgb_request& r) {
+    if (r.N < 16 || (r.N & (r.N - 1)) || r.N > (1 << kMaxLogN))
+        fail(PCGB_EINVAL, "request: N must be a power of two in [16, 2^24]");
+    if (r.c < 1 || r.c > 8) fail(PCGB_EINVAL, "request: c must be in [1, 8]");
+    if (r.t < 1 || (r.t & (r.t - 1)) || r.N / r.t < 4)
+        fail(PCGB_EINVAL, "request: t must be a power of two with N/t >= 4");
+    if (r.party != 0 && r.party != 1) fail(PCGB_EINVAL, "request: party must be 0 or 1");
+}
+
+pcgb_expander* get_plan(pcgb_server* s, int N, int c, int t) {
+    std::lock_guard<std::mutex> lk(s->plans_mu);
+    auto key = std::make_tuple(N, c, t);
+    auto it = s->plans.find(key);
+    if (it != s->plans.end()) return it->second;
+    std::vector<uint64_t> a(static_cast<size_t>(c > 1 ? c - 1 : 1) * N);
+    public_a_host(N, c, s->a_seed, a.data());
+    pcgb_expander* e = expander_create(N, c, t, 1, PCGB_PRG_CHACHA8, a.data(), nullptr);
+    s->plans[key] = e;
+    return e;
+}
+
+// Footprint of one request: dealt keys of both parties, noise, outputs,
+// digests and the expansion workspace.
+size_t footprint(pcgb_expander* e, const pcgb_request& r) {
+    int K = 0, levels = 0, nk = 0;
+    size_t ws = 0;
+    expander_info(e, &K, &levels, &nk, &ws);
+    const size_t ct = static_cast<size_t>(r.c) * r.t;
+    return align256(2 * sizeof(Blk) * K) + align256(sizeof(Blk) * K * levels * nk) +
+           align256(8 * static_cast<size_t>(K)) + align256(16 * ct) +
+           align256(16 * static_cast<size_t>(r.N)) + 256 + align256(ws);
+}
+
+void CUDART_CB on_done(void* p) {
+    auto* ctx = static_cast<CallbackCtx*>(p);
+    pcgb_server* s = ctx->s;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        ctx->r->done_s = s->now();
+        s->finished.push_back(ctx->r);
+    }
+    s->cv_work.notify_one();
+    delete ctx;
+}
+
+// Enqueue one admitted request on its slot's stream (worker thread only).
+void launch(pcgb_server* s, Req* r) {
+    cudaStream_t st = s->streams[r->slot];
+    pcgb_expander* e = get_plan(s, r->r.N, r->r.c, r->r.t);
+    int K = 0, levels = 0, nk = 0;
+    size_t wsb = 0;
+    expander_info(e, &K, &levels, &nk, &wsb);
+    const size_t ct = static_cast<size_t>(r->r.c) * r->r.t, N = r->r.N;
+    char* base = nullptr;
+    PCGB_CK(cudaMallocAsync(reinterpret_cast<void**>(&base), r->bytes, st));
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        char* p = base + off;
+        off += align256(bytes);
+        return p;
+    };
+    Blk* roots = reinterpret_cast<Blk*>(take(2 * sizeof(Blk) * K));
+    Blk* cws = reinterpret_cast<Blk*>(take(sizeof(Blk) * K * levels * nk));
+    uint64_t* cwo = reinterpret_cast<uint64_t*>(take(8 * static_cast<size_t>(K)));
+    uint64_t* pos = reinterpret_cast<uint64_t*>(take(16 * ct));
+    uint64_t* val = pos + ct;
+    uint64_t* x = reinterpret_cast<uint64_t*>(take(16 * N));
+    uint64_t* z = x + N;
+    uint64_t* dig = reinterpret_cast<uint64_t*>(take(16));
+    const Workspace ws = workspace_carve(e, take(wsb));
+    deal_keys_device(e, r->r.seed, roots, roots + K, cws, cwo, st);
+    noise_device(r->r.N, r->r.c, r->r.t, r->r.seed, r->r.party, pos, val, st);
+    expand_device_ws(e, ws, r->r.party, r->r.party ? roots + K : roots, cws, cwo, pos, val, x, z,
+                     st);
+    digest_device(x, N, dig, st);
+    digest_device(z, N, dig + 1, st);
+    PCGB_CK(cudaMemcpyAsync(s->h_digest + 2 * r->slot, dig, 16, cudaMemcpyDeviceToHost, st));
+    PCGB_CK(cudaFreeAsync(base, st));
+    PCGB_CK(cudaLaunchHostFunc(st, on_done, new CallbackCtx{s, r}));
+}
+
+void worker_loop(pcgb_server* s) {
+    cudaSetDevice(s->dev);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        // Completions: collect digests, release memory accounting and slots.
+        for (Req* r : s->finished) {
+            r->dx = s->h_digest[2 * r->slot];
+            r->dz = s->h_digest[2 * r->slot + 1];
+            r->state = 2;
+            s->slot_req[r->slot] = nullptr;
+            s->in_flight_bytes -= r->bytes;
+            --s->in_flight;
+        }
+        if (!s->finished.empty()) {
+            s->finished.clear();
+            s->cv_done.notify_all();
+        }
+        if (s->stopping && s->in_flight == 0 && s->pending.empty()) break;
+        // Admissions (FIFO head first; a request larger than the whole
+        // budget still runs when nothing else is in flight).
+        while (!s->pending.empty() && s->in_flight < s->max_in_flight) {
+            int slot = -1;
+            for (int i = 0; i < s->n_slots; ++i)
+                if (!s->slot_req[i]) { slot = i; break; }
+            if (slot < 0) break;
+            Req* r = s->pending.front();
+            if (s->in_flight > 0 && s->in_flight_bytes + r->bytes > s->budget) break;
+            s->pending.pop_front();
+            r->slot = slot;
+            r->state = 1;
+            r->start_s = s->now();
+            s->slot_req[slot] = r;
+            s->in_flight_bytes += r->bytes;
+            ++s->in_flight;
+            lk.unlock();
+            bool ok = true;
+            std::string msg;
+            try {
+                launch(s, r);
+            } catch (const std::exception& ex) {
+                ok = false;
+                msg = ex.what();
+            }
+            lk.lock();
+            if (!ok) {
+                r->state = 3;
+                r->status = PCGB_ECUDA;
+                r->err = msg;
+                s->slot_req[slot] = nullptr;
+                s->in_flight_bytes -= r->bytes;
+                --s->in_flight;
+                s->cv_done.notify_all();
+            }
+        }
+        // Sleep until something can change: a completion, shutdown, or a
+        // head request that can actually be admitted now (the same rule as
+        // above, footprint included, so the wait never spins while holding
+        // the lock the completion callback needs).
+        s->cv_work.wait(lk, [s] {
+            if (!s->finished.empty() || (s->stopping && s->in_flight == 0)) return true;
+            if (s->pending.empty() || s->in_flight >= s->max_in_flight ||
+                s->in_flight >= s->n_slots)
+                return false;
+            return s->in_flight == 0 || s->in_flight_bytes + s->pending.front()->bytes <= s->budget;
+        });
+    }
+}
+
+}  // namespace
+
+pcgb_server* server_create(int n_streams, size_t budget, int max_in_flight, uint64_t a_seed) {
+    if (n_streams < 1 || n_streams > 64) fail(PCGB_EINVAL, "server: n_streams must be in [1, 64]");
+    if (max_in_flight < 1) fail(PCGB_EINVAL, "server: max_in_flight must be >= 1");
+    auto* s = new pcgb_server();
+    PCGB_CK(cudaGetDevice(&s->dev));
+    s->n_slots = n_streams;
+    s->max_in_flight = max_in_flight;
+    s->a_seed = a_seed;
+    if (budget == 0) {
+        size_t free_b = 0, total_b = 0;
+        PCGB_CK(cudaMemGetInfo(&free_b, &total_b));
+        budget = free_b / 2;
+    }
+    s->budget = budget;
+    // Keep freed pool memory mapped (the default threshold of 0 returns it to
+    // the OS at every synchronisation, so each multi-GB request would map
+    // its memory again).
+    cudaMemPool_t pool = nullptr;
+    PCGB_CK(cudaDeviceGetDefaultMemPool(&pool, s->dev));
+    uint64_t keep = UINT64_MAX;
+    PCGB_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    s->streams.resize(n_streams);
+    s->slot_req.assign(n_streams, nullptr);
+    for (auto& st : s->streams) PCGB_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    PCGB_CK(cudaMallocHost(&s->h_digest, 16 * static_cast<size_t>(n_streams)));
+    s->t0 = clk::now();
+    s->worker = std::thread(worker_loop, s);
+    return s;
+}
+
+void server_prepare(pcgb_server* s, int N, int c, int t) {
+    pcgb_request r{};
+    r.N = N; r.c = c; r.t = t;
+    validate(r);
+    get_plan(s, N, c, t);
+}
+
+uint64_t server_submit(pcgb_server* s, const pcgb_request& r) {
+    validate(r);
+    pcgb_expander* e = get_plan(s, r.N, r.c, r.t);
+    auto req = std::make_unique<Req>();
+    req->r = r;
+    req->bytes = footprint(e, r);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stopping) fail(PCGB_ESTATE, "server: shutting down");
+    req->ticket = s->next_ticket++;
+    req->submit_s = s->now();
+    Req* raw = req.get();
+    s->reqs[raw->ticket] = std::move(req);
+    s->pending.push_back(raw);
+    s->cv_work.notify_one();
+    return raw->ticket;
+}
+
+int server_wait(pcgb_server* s, uint64_t ticket, pcgb_result* out, int timeout_ms) {
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) fail(PCGB_EINVAL, "server: unknown ticket");
+    Req* r = it->second.get();
+    const auto pred = [r] { return r->state >= 2; };
+    if (timeout_ms < 0) s->cv_done.wait(lk, pred);
+    else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred))
+        return PCGB_ETIMEOUT;
+    if (out) {
+        out->digest_x = r->dx;
+        out->digest_z = r->dz;
+        out->submit_s = r->submit_s;
+        out->start_s = r->start_s;
+        out->done_s = r->done_s;
+        out->status = r->state == 2 ? PCGB_OK : r->status;
+    }
+    const int rc = r->state == 2 ? PCGB_OK : r->status;
+    if (rc != PCGB_OK) fail(rc, "request failed: " + r->err);
+    s->reqs.erase(it);
+    return PCGB_OK;
+}
+
+void server_run_trace(pcgb_server* s, const pcgb_request* reqs, int n, pcgb_result* out,
+                      double timeout_s) {
+    std::vector<uint64_t> tickets(n);
+    const auto start = clk::now();
+    for (int i = 0; i < n; ++i) {
+        const auto when = start + std::chrono::duration_cast<clk::duration>(
+                                      std::chrono::duration<double>(reqs[i].arrival_s));
+        std::this_thread::sleep_until(when);
+        tickets[i] = server_submit(s, reqs[i]);
+    }
+    const auto deadline = start + std::chrono::duration_cast<clk::duration>(
+                                      std::chrono::duration<double>(timeout_s));
+    for (int i = 0; i < n; ++i) {
+        const auto left = std::chrono::duration_cast<std::chrono::milliseconds>(deadline - clk::now());
+        const int ms = static_cast<int>(std::max<long long>(0, left.count()));
+        if (server_wait(s, tickets[i], out ? out + i : nullptr, ms) == PCGB_ETIMEOUT)
+            fail(PCGB_ETIMEOUT, "server: trace did not finish within the timeout");
+    }
+}
+
+void server_destroy(pcgb_server* s, int timeout_ms) {
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stopping = true;
+        for (Req* r : s->pending) {  // cancel what has not started
+            r->state = 3;
+            r->status = PCGB_ESTATE;
+            r->err = "cancelled: server shut down";
+        }
+        s->pending.clear();
+        s->cv_done.notify_all();
+    }
+    s->cv_work.notify_all();
+    // The worker exits once in-flight work completed; bound the wait.
+    const auto deadline = clk::now() + std::chrono::milliseconds(timeout_ms);
+    bool drained = false;
+    while (clk::now() < deadline) {
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (s->in_flight == 0) { drained = true; break; }
+        }
+        std::this_thread::sleep_for(std::chrono::milliseconds(1));
+    }
+    s->cv_work.notify_all();
+    if (!drained) {
+        // Leave the object alive rather than free memory the GPU still uses.
+        s->worker.detach();
+        fail(PCGB_ETIMEOUT, "server: in-flight requests did not finish in time");
+    }
+    s->worker.join();
+    for (auto& st : s->streams) cudaStreamSynchronize(st);
+    for (auto& kv : s->plans) expander_destroy(kv.second);
+    for (auto& st : s->streams) cudaStreamDestroy(st);
+    cudaFreeHost(s->h_digest);
+    delete s;
+}
+
+void server_stats(pcgb_server* s, int* pending, int* in_flight, size_t* bytes, int* plans) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (pending) *pending = static_cast<int>(s->pending.size());
+    if (in_flight) *in_flight = s->in_flight;
+    if (bytes) *bytes = s->in_flight_bytes;
+    std::lock_guard<std::mutex> lk2(s->plans_mu);
+    if (plans) *plans = static_cast<int>(s->plans.size());
+}
+
+}  // namespace pcgb

@@ -31,6 +31,17 @@ _vp = C.c_void_p
 EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p)
 
 
+class Request(C.Structure):
+    _fields_ = [("N", C.c_int), ("c", C.c_int), ("t", C.c_int), ("party", C.c_int),
+                ("seed", C.c_uint64), ("arrival_s", C.c_double)]
+
+
+class Result(C.Structure):
+    _fields_ = [("digest_x", C.c_uint64), ("digest_z", C.c_uint64), ("submit_s", C.c_double),
+                ("start_s", C.c_double), ("done_s", C.c_double), ("status", C.c_int),
+                ("reserved", C.c_int)]
+
+
 class PcgError(RuntimeError):
     """A library call failed; .code is the PCGB_E* value."""
 
@@ -99,6 +110,16 @@ def _load():
         "pcgb_noise": ([C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int, _u64p, _u64p], C.c_int),
         "pcgb_public_a": ([C.c_int, C.c_int, C.c_uint64, _vp], C.c_int),
         "pcgb_deal_keys_device": ([_vp, C.c_uint64, _vp, _vp, _vp, _vp, _vp], C.c_int),
+        "pcgb_server_create": ([C.POINTER(_vp), C.c_int, C.c_size_t, C.c_int, C.c_uint64], C.c_int),
+        "pcgb_server_prepare": ([_vp, C.c_int, C.c_int, C.c_int], C.c_int),
+        "pcgb_server_submit": ([_vp, C.POINTER(Request), C.POINTER(C.c_uint64)], C.c_int),
+        "pcgb_server_wait": ([_vp, C.c_uint64, C.POINTER(Result), C.c_int], C.c_int),
+        "pcgb_server_run_trace": ([_vp, C.POINTER(Request), C.c_int, C.POINTER(Result),
+                                   C.c_double], C.c_int),
+        "pcgb_server_stats": ([_vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                               C.POINTER(C.c_size_t), C.POINTER(C.c_int)], C.c_int),
+        "pcgb_server_destroy": ([_vp, C.c_int], C.c_int),
+        "pcgb_digest_device": ([_vp, C.c_size_t, _vp, _vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -462,3 +483,59 @@ class Expander:
         if r < 0:
             _check(r)
         return [tuple(ms[4 * i: 4 * i + 4]) for i in range(r)]
+
+
+def digest_device(d_v, n, stream=None):
+    """Order-independent 64-bit digest of n device words (bit-exactness checks)."""
+    out = DeviceBuffer(8)
+    _check(lib.pcgb_digest_device(d_v, n, out.ptr, stream))
+    _check(lib.pcgb_stream_synchronize(stream))
+    return int(out.download(np.uint64, 1)[0])
+
+
+class Server:
+    """Continuous-batching expansion server on the current device."""
+
+    def __init__(self, n_streams=4, mem_budget=0, max_in_flight=None, a_seed=7):
+        h = C.c_void_p()
+        _check(lib.pcgb_server_create(C.byref(h), n_streams, mem_budget,
+                                      max_in_flight or n_streams, a_seed))
+        self.h = h.value
+
+    def prepare(self, N, c, t):
+        _check(lib.pcgb_server_prepare(self.h, N, c, t))
+
+    def submit(self, N, c, t, seed, party=0):
+        r = Request(N, c, t, party, seed, 0.0)
+        tk = C.c_uint64()
+        _check(lib.pcgb_server_submit(self.h, C.byref(r), C.byref(tk)))
+        return tk.value
+
+    def wait(self, ticket, timeout_ms=-1):
+        res = Result()
+        _check(lib.pcgb_server_wait(self.h, ticket, C.byref(res), timeout_ms))
+        return res
+
+    def run_trace(self, reqs, timeout_s=600.0):
+        """reqs: list of (N, c, t, party, seed, arrival_s); returns list of Result."""
+        arr = (Request * len(reqs))(*[Request(*r) for r in reqs])
+        out = (Result * len(reqs))()
+        _check(lib.pcgb_server_run_trace(self.h, arr, len(reqs), out, timeout_s))
+        return list(out)
+
+    def stats(self):
+        p, f, b, n = C.c_int(), C.c_int(), C.c_size_t(), C.c_int()
+        _check(lib.pcgb_server_stats(self.h, C.byref(p), C.byref(f), C.byref(b), C.byref(n)))
+        return {"pending": p.value, "in_flight": f.value, "bytes_in_flight": b.value,
+                "plans": n.value}
+
+    def close(self, timeout_ms=60000):
+        if getattr(self, "h", None):
+            h, self.h = self.h, None
+            _check(lib.pcgb_server_destroy(h, timeout_ms))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -113,3 +113,51 @@ def test_ole_relation_full_shape(pcg):
     # x = sum a_i e_i has exactly the dealt noise in a_0's slot.
     assert np.count_nonzero(xs[0]) > N // 2
     e.close()
+
+
+def test_full_shape_against_independent_paths(pcg):
+    """N = 2^20, c = 4, t = 16: x against the oracle's products of the same
+    public a and noise; z against sum_q (a_i a_j) * g'_q computed with the
+    poly-mul drop-in on the fused kernel's g' (an independent NTT path); and
+    two separately built expanders agree (resident plans are deterministic)."""
+    N, c, t, seed = 1 << 20, 4, 16, 4242
+    a = pcg.public_a(N, c, 21)
+    e1 = pcg.Expander(N, c, t, 1, pcg.PRG_CHACHA8, public_a=a)
+    K, L = e1.K, e1.levels
+    d_r0, d_r1 = pcg.DeviceBuffer(16 * K), pcg.DeviceBuffer(16 * K)
+    d_cws, d_cwo = pcg.DeviceBuffer(16 * K * L), pcg.DeviceBuffer(8 * K)
+    e1.deal_keys_device(seed, d_r0.ptr, d_r1.ptr, d_cws.ptr, d_cwo.ptr)
+    pos, val = pcg.noise(N, c, t, seed, 0)
+    d_pos, d_val = dev(pcg, pos), dev(pcg, val)
+    outs = []
+    for e in (e1, pcg.Expander(N, c, t, 1, pcg.PRG_CHACHA8, public_a=a)):
+        d_x, d_z = pcg.DeviceBuffer(8 * N), pcg.DeviceBuffer(8 * N)
+        e.expand_device(0, d_r0.ptr, d_cws.ptr, d_cwo.ptr, d_pos.ptr, d_val.ptr, d_x.ptr, d_z.ptr)
+        outs.append((d_x.download(np.uint64, N), d_z.download(np.uint64, N)))
+    x, z = outs[0]
+    assert (outs[1][0] == x).all() and (outs[1][1] == z).all()
+    # x = e_0 + sum_{i>=1} a_i * e_i, on the CPU.
+    want = np.zeros(N, dtype=object)
+    for i in range(c):
+        ei = np.zeros(N, np.uint64)
+        ei[pos[i * t:(i + 1) * t].astype(np.int64)] = val[i * t:(i + 1) * t]
+        if i == 0:
+            prod = ei
+        else:
+            prod = O.poly_mul(a[(i - 1) * N:i * N], ei, N)
+        want = (want + prod.astype(object)) % P
+    assert (x == np.asarray(want, dtype=np.uint64)).all()
+    # z through g' and the drop-in products.
+    d_g = pcg.DeviceBuffer(8 * N * e1.Q)
+    e1.expand_g_device(0, d_r0.ptr, d_cws.ptr, d_cwo.ptr, d_g.ptr)
+    g = d_g.download(np.uint64, N * e1.Q).reshape(e1.Q, N)
+    av = [np.eye(1, N, 0, dtype=np.uint64)[0]] + [a[(i - 1) * N:i * N] for i in range(1, c)]
+    zz = np.zeros(N, dtype=object)
+    q = 0
+    for i in range(c):
+        for j in range(i, c):
+            aa, _ = pcg.poly_mul_u64_gpuntt(av[i], av[j], 1, N)
+            p, _ = pcg.poly_mul_u64_gpuntt(aa, g[q], 1, N)
+            zz = (zz + p.astype(object)) % P
+            q += 1
+    assert (z == np.asarray(zz, dtype=np.uint64)).all()
