@@ -48,8 +48,72 @@ L2_BYTES = 126 * 1024 * 1024
 # Published figure for this metric and shape (1x L40S, serial arm,
 # GPU_baseline/final_l40s/e2e_arms.csv:32): 2^20 / 192.11 ms.
 PUBLISHED = 2 ** 20 / 0.19211
-# ChaCha8 quarter-round ops (4 add, 4 xor, 4 rotate) x 4 QR x 8 rounds.
-OPS_PER_BLOCK = 12 * 4 * 8
+
+
+def chacha8_live_ops(ctr, nonce, words):
+    """ARX ops (32-bit add, xor, rotate) a ChaCha8 block must execute to
+    produce keystream `words` when the key is a 128-bit DPF node followed by
+    128 zero bits (the tree PRG and output hash of CPU_baseline/tree_prg.h:80-148).
+
+    Ops whose inputs are all constants fold away, x+0 and x^0 are free, and
+    only the backward slice of the requested words is counted -- the same
+    pruning the compiler applies to the kernel.  The ALU probe counts every
+    op of its (fully live) double rounds the same way, so achieved/peak
+    compares like with like."""
+    M = 0xFFFFFFFF
+    deps = []
+
+    def node(*ins):
+        deps.append(tuple(x[1] for x in ins if x[0] == "v"))
+        return ("v", len(deps) - 1)
+
+    def add(a, b):
+        if a[0] == "c" and b[0] == "c":
+            return ("c", (a[1] + b[1]) & M)
+        if a == ("c", 0):
+            return b
+        return a if b == ("c", 0) else node(a, b)
+
+    def xor(a, b):
+        if a[0] == "c" and b[0] == "c":
+            return ("c", a[1] ^ b[1])
+        if a == ("c", 0):
+            return b
+        return a if b == ("c", 0) else node(a, b)
+
+    def rot(a, r):
+        return ("c", ((a[1] << r) | (a[1] >> (32 - r))) & M) if a[0] == "c" else node(a)
+
+    key = [node() for _ in range(4)]
+    n_in = len(deps)
+    x = ([("c", v) for v in (0x61707865, 0x3320646E, 0x79622D32, 0x6B206574)] + key +
+         [("c", 0)] * 4 + [("c", ctr), ("c", 0), ("c", nonce[0]), ("c", nonce[1])])
+    init = list(x)
+
+    def qr(a, b, c, d):
+        x[a] = add(x[a], x[b]); x[d] = rot(xor(x[d], x[a]), 16)
+        x[c] = add(x[c], x[d]); x[b] = rot(xor(x[b], x[c]), 12)
+        x[a] = add(x[a], x[b]); x[d] = rot(xor(x[d], x[a]), 8)
+        x[c] = add(x[c], x[d]); x[b] = rot(xor(x[b], x[c]), 7)
+
+    for _ in range(4):
+        for q in ((0, 4, 8, 12), (1, 5, 9, 13), (2, 6, 10, 14), (3, 7, 11, 15),
+                  (0, 5, 10, 15), (1, 6, 11, 12), (2, 7, 8, 13), (3, 4, 9, 14)):
+            qr(*q)
+    stack = [o[1] for o in (add(x[i], init[i]) for i in words) if o[0] == "v"]
+    live = set()
+    while stack:
+        v = stack.pop()
+        if v not in live:
+            live.add(v)
+            stack.extend(deps[v])
+    return sum(1 for v in live if v >= n_in)
+
+
+# Output hash: nonce "out_hash", counter 0, low 64 bits (words 0-1).
+OPS_OUT_HASH = chacha8_live_ops(0, (0x68617368, 0x6F75745F), [0, 1])
+# Binary tree node (w = 1): H_0 = words 0-3 of block 0, nonce 0.
+OPS_TREE_W1 = chacha8_live_ops(0, (0, 0), [0, 1, 2, 3])
 
 
 def parse():
@@ -310,17 +374,21 @@ def run_ours(args, d):
     leaf_ms = float(np.mean([s[1] for s in stages])) if stages else None
     D = 1 << e.levels
     S = 16
-    blocks_per_launch = K * D * (1 + (S - 1) / S)   # out-hash + tree blocks below the frontier
-    ops = blocks_per_launch * OPS_PER_BLOCK
+    # Per leaf: one output hash; per internal node below the frontier (S - 1
+    # of them per S leaves): one tree block.
+    ops = K * D * (OPS_OUT_HASH + OPS_TREE_W1 * (S - 1) / S)
     achieved = ops / (leaf_ms * 1e-3) / 1e12 if leaf_ms else None
     peak = gops_peak / 1e3
     roofline = {"bound": "int_alu", "kernel": "leaf_gather_kernel<1,4,chacha8>",
                 "achieved": achieved, "peak": peak, "unit": "Tops/s",
                 "frac": achieved / peak if achieved else None,
-                "traffic": LEAF_TRAFFIC_BYTES,
+                "traffic": LEAF_DRAM_BYTES_PER_LEAF * K * D,
+                "traffic_unit": "bytes per launch (ncu dram read+write, scaled by leaves)",
                 "peak_source": "ARX probe (pcgb_arx_peak) in this run; MEASURED_PEAKS.json has "
                                "no integer-ALU figure",
-                "ops_per_launch": ops, "launch_ms": leaf_ms}
+                "ops_per_launch": ops, "ops_per_block": {"out_hash": OPS_OUT_HASH,
+                                                         "tree": OPS_TREE_W1},
+                "launch_ms": leaf_ms}
     ntt_ms = float(np.mean([s[3] for s in stages])) if stages else None
     Q = e.Q
     ntt_bytes = 8 * N * (4 * Q + 3)
@@ -416,9 +484,12 @@ def run_serving(L, n_req, seed=2025, util=0.85):
     return out
 
 
-# DRAM bytes per launch of the leaf kernel from the ncu capture summarised in
-# profiles/leaf_gather_N2e20_c4_t16.md (None until captured).
-LEAF_TRAFFIC_BYTES = None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per leaf of one
+# leaf-gather launch, from an ncu capture of the N=2^18, c=4, t=16 case
+# (135.06 MB read + 8.75 MB written for 4096 keys x 2^15 leaves).  The reads
+# are the 16-byte frontier nodes (one per 16 leaves); the traffic scales with
+# the leaf count.
+LEAF_DRAM_BYTES_PER_LEAF = (135.05792e6 + 8.749824e6) / (4096 * 2 ** 15)
 
 
 def hbm_peak():
