@@ -72,6 +72,12 @@ int pcgb_memcpy_d2h(void* dst, const void* d_src, size_t bytes, void* stream);
 int pcgb_memset(void* d_dst, int value, size_t bytes, void* stream);
 int pcgb_stream_synchronize(void* stream);
 int pcgb_device_synchronize(void);
+/* Scratch that the library allocates per call (drop-in poly-mul and DPF
+ * helpers, server requests) comes from a stream-ordered pool of its own on
+ * each device, which keeps freed memory mapped so the next call of the same
+ * size maps nothing.  Returns that memory on the current device to the
+ * driver. */
+int pcgb_trim_pool(void);
 void* pcgb_default_stream(void);
 /* Kernel launches issued by the library since load (all devices). */
 unsigned long long pcgb_launch_count(void);

@@ -162,9 +162,9 @@ void aes_ecb_encrypt_device(const uint8_t* keys, const uint8_t* in, uint8_t* out
     cudaStream_t st = default_stream();
     uint8_t *d_rk = nullptr, *d_in = nullptr, *d_out = nullptr;
     const size_t bytes = static_cast<size_t>(count) * 16;
-    PCGB_CK(cudaMallocAsync(&d_rk, rks.size(), st));
-    PCGB_CK(cudaMallocAsync(&d_in, bytes, st));
-    PCGB_CK(cudaMallocAsync(&d_out, bytes, st));
+    d_rk = static_cast<uint8_t*>(pool_alloc(rks.size(), st));
+    d_in = static_cast<uint8_t*>(pool_alloc(bytes, st));
+    d_out = static_cast<uint8_t*>(pool_alloc(bytes, st));
     PCGB_CK(cudaMemcpyAsync(d_rk, rks.data(), rks.size(), cudaMemcpyHostToDevice, st));
     PCGB_CK(cudaMemcpyAsync(d_in, in, bytes, cudaMemcpyHostToDevice, st));
     aes_ecb_kernel<<<(count + 127) / 128, 128, 0, st>>>(

@@ -52,7 +52,7 @@ double arx_probe(float* ms_out) {
     const int sms = sm_count();
     const int blocks = sms * 8, threads = 256, iters = 4096;
     uint32_t* sink = nullptr;
-    PCGB_CK(cudaMallocAsync(&sink, 4, st));
+    sink = static_cast<uint32_t*>(pool_alloc(4, st));
     arx_probe_kernel<<<blocks, threads, 0, st>>>(1, 64, sink);  // warm-up
     PCGB_POST_LAUNCH();
     cudaEvent_t e0, e1;

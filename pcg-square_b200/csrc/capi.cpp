@@ -123,6 +123,34 @@ cudaStream_t default_stream() {
     return streams[dev];
 }
 
+cudaMemPool_t library_pool() {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {nullptr};
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        check_cuda(cudaMemPoolCreate(&pools[dev], &props), "cudaMemPoolCreate");
+        // The default threshold (0) hands freed memory back at every
+        // synchronisation, so each call would map its scratch again.
+        uint64_t keep = UINT64_MAX;
+        check_cuda(cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep),
+                   "cudaMemPoolSetAttribute");
+    }
+    return pools[dev];
+}
+
+void* pool_alloc(size_t bytes, cudaStream_t st) {
+    void* p = nullptr;
+    check_cuda(cudaMallocFromPoolAsync(&p, bytes, library_pool(), st), "cudaMallocFromPoolAsync");
+    return p;
+}
+
 void upload_blocking(void* d_dst, const void* src, size_t bytes) {
     cudaStream_t st = default_stream();
     check_cuda(cudaMemcpyAsync(d_dst, src, bytes, cudaMemcpyHostToDevice, st), "upload");
@@ -223,6 +251,14 @@ int pcgb_memset(void* d, int v, size_t bytes, void* stream) {
 int pcgb_stream_synchronize(void* stream) {
     return guarded([&] { PCGB_CK(cudaStreamSynchronize(pcgb::as_stream(stream))); });
 }
+int pcgb_trim_pool(void) {
+    return guarded([&] {
+        cudaStream_t st = pcgb::default_stream();
+        PCGB_CK(cudaStreamSynchronize(st));
+        PCGB_CK(cudaMemPoolTrimTo(pcgb::library_pool(), 0));
+    });
+}
+
 int pcgb_device_synchronize(void) { return guarded([&] { PCGB_CK(cudaDeviceSynchronize()); }); }
 void* pcgb_default_stream(void) {
     void* s = nullptr;
@@ -336,7 +372,7 @@ int pcgb_poly_mul_u64(int variant, uint64_t* out, const uint64_t* a, const uint6
         cudaStream_t st = pcgb::default_stream();
         const size_t n = static_cast<size_t>(batch) * N;
         uint64_t* d = nullptr;
-        PCGB_CK(cudaMallocAsync(&d, 5 * n * sizeof(uint64_t), st));
+        d = static_cast<uint64_t*>(pcgb::pool_alloc(5 * n * sizeof(uint64_t), st));
         uint64_t *da = d, *db = d + n, *dc = d + 2 * n, *scratch = d + 3 * n;
         PCGB_CK(cudaMemcpyAsync(da, a, n * 8, cudaMemcpyHostToDevice, st));
         PCGB_CK(cudaMemcpyAsync(db, b, n * 8, cudaMemcpyHostToDevice, st));
@@ -400,7 +436,7 @@ int pcgb_dpf_keyed_full_eval(int K, int n, int w, int prg, const pcgb_blk* d_roo
         if (prg == PCGB_PRG_AES) d_rk = pcgb::aes_upload_round_keys(round_keys, nk, st);
         const size_t sn = pcgb::keyed_tops_scratch_nodes(K, w, levels);
         Blk* scratch = nullptr;
-        if (sn) PCGB_CK(cudaMallocAsync(&scratch, sn * sizeof(Blk), st));
+        if (sn) scratch = static_cast<Blk*>(pcgb::pool_alloc(sn * sizeof(Blk), st));
         pcgb::keyed_expand_tops(K, n, w, prg, reinterpret_cast<const Blk*>(d_roots),
                                 reinterpret_cast<const Blk*>(d_cws), d_rk, levels,
                                 reinterpret_cast<Blk*>(d_leaves), scratch, st);
@@ -422,7 +458,7 @@ int pcgb_poly_mul_device(uint64_t* d_c, const uint64_t* d_a, const uint64_t* d_b
         const pcgb::NttPlan& pl = pcgb::ntt_plan(pcgb::ilog2i(N));
         uint64_t* scratch = nullptr;
         const size_t n = static_cast<size_t>(batch) * N;
-        PCGB_CK(cudaMallocAsync(&scratch, 2 * n * sizeof(uint64_t), st));
+        scratch = static_cast<uint64_t*>(pcgb::pool_alloc(n * sizeof(uint64_t), st));
         pcgb::poly_mul_device(pl, d_c, d_a, d_b, batch, scratch, st);
         PCGB_CK(cudaFreeAsync(scratch, st));
     });
@@ -439,7 +475,7 @@ int pcgb_poly_mul_device_multi(int count, uint64_t* const* d_c, const uint64_t* 
                 pcgb::fail(PCGB_EINVAL, "N must be a power of two in [2, 2^24]");
             const pcgb::NttPlan& pl = pcgb::ntt_plan(pcgb::ilog2i(N[i]));
             uint64_t* scratch = nullptr;
-            PCGB_CK(cudaMallocAsync(&scratch, 2 * static_cast<size_t>(N[i]) * sizeof(uint64_t), st));
+            scratch = static_cast<uint64_t*>(pcgb::pool_alloc(static_cast<size_t>(N[i]) * sizeof(uint64_t), st));
             pcgb::poly_mul_device(pl, d_c[i], d_a[i], d_b[i], 1, scratch, st);
             PCGB_CK(cudaFreeAsync(scratch, st));
             ++i;

@@ -1,6 +1,6 @@
 // Negacyclic NTT over F_p, four-step form, for N = 2^logN (1 <= logN <= 24).
 //
-// N = n1 * n2 with n1 = 2^ceil(logN/2), n2 = 2^floor(logN/2); coefficient j
+// N = n1 * n2 with n1 = 2^floor(logN/2), n2 = 2^ceil(logN/2); coefficient j
 // sits at row j / n2, column j % n2.  With psi a primitive 2N-th root:
 //   column pass: negacyclic NTT of length n1 on every column (root
 //                psi1 = psi^n2), then multiply element (k, j2) by the
@@ -8,23 +8,49 @@
 //   row pass:    negacyclic NTT of length n2 on every row (root psi2 =
 //                psi^n1).
 // Element (k, k2) then holds A(psi^(2*(i1 + n1*i2) + 1)) with i1 = brev(k),
-// i2 = brev(k2): the evaluations of a(x) mod x^N + 1, in a fixed permuted
-// order that every operand of a pointwise product shares.  The inverse runs
-// the passes backwards with inverse roots and folds N^-1 into its twiddle.
+// i2 = brev(k2): the evaluations of a(x) mod x^N + 1.  The row pass stores
+// its outputs in a fixed permuted order (below) that every operand of a
+// pointwise product shares; the inverse runs the passes backwards with
+// inverse roots and folds N^-1 into its twiddle.
 //
 // Each sub-transform is the merged-twist Cooley-Tukey (forward) /
 // Gentleman-Sande (inverse) negacyclic NTT of Longa and Naehrig (CANS 2016,
-// Algorithms 1-2), done in shared memory with Shoup multiplications by
-// precomputed roots.  The passes are two HBM sweeps per transform; the
-// pointwise product with a resident operand is fused into the row pass, as is
-// the multiply-accumulate over several transforms.  Replaces the reference's
-// radix-2 per-stage v1 kernels (GPU_baseline/common/poly_mul_cuda.cu:137-200)
-// and its 20-kernel four-step (poly_mul_gpuntt_square.cu:171-613).
+// Algorithms 1-2) with Harvey's lazy butterflies (J. Symbolic Comput. 60,
+// 2014): forward values live in [0, 4p), inverse values in [0, 2p), which
+// 4p < 2^64 allows, and a Shoup product by a precomputed root costs one high
+// and two low 64-bit multiplies.
+//
+// Register blocking.  A thread owns E = 16 elements of one sub-transform of
+// length n = 2^L (all n when n < 16), so T = n / 16 threads share it.  The L
+// stages run in phases of four (radix 16) entirely in registers; between
+// phases the elements are exchanged through shared memory.  In phase P
+// (first stage s0 = 4P, r = min(4, L - s0) stages) a unit is the 2^r
+// elements g*2^(L-s0) + j + k*tl (tl = 2^(L-s0-r), k < 2^r) that the phase
+// combines; thread t owns units t*U .. t*U+U-1 (U = 16 / 2^r), unit u = (g,
+// j) with g = u / tl, j = u % tl.  Phase 0 owns elements t + T*k, the last
+// phase the 16 consecutive elements 16t .. 16t+15, so global loads and stores
+// coalesce in both the column pass (lanes run over adjacent columns) and the
+// row pass (lanes run over t).  Row-pass outputs of element i are stored at
+// (i % 16) * T + i / 16 -- the permuted evaluation order.  Shared memory holds
+// element i at (i + i/16) * stride, which keeps every exchange free of bank
+// conflicts for the strides used here.
+//
+// The twiddle of stage s and butterfly group i = g*2^q + sub (q = s - s0) is
+// stored at 2^s + sub*2^s0 + g, so the lanes of a warp read the same or
+// adjacent table entries in every phase.
+//
+// The passes are two HBM sweeps per transform; the pointwise product with a
+// resident operand and the multiply-accumulate over several transforms are
+// fused into the row pass, where the forward phases end in the same register
+// layout the inverse phases start from.  Replaces the reference's radix-2
+// per-stage v1 kernels (GPU_baseline/common/poly_mul_cuda.cu:137-200) and its
+// 20-kernel four-step (poly_mul_gpuntt_square.cu:171-613).
 #include "pcgb_internal.h"
 
 #include <map>
 #include <memory>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "field.cuh"
@@ -35,189 +61,293 @@ struct NttPlan {
     int logN = 0, l1 = 0, l2 = 0;
     size_t N = 0;
     int n1 = 0, n2 = 0;
-    ulonglong2* psi1 = nullptr;   // (value, shoup) in bit-reversed order, n1
-    ulonglong2* psi1i = nullptr;
-    ulonglong2* psi2 = nullptr;   // n2
-    ulonglong2* psi2i = nullptr;
+    ulonglong2* tw1 = nullptr;    // column roots (value, shoup), phase-permuted
+    ulonglong2* tw1i = nullptr;
+    ulonglong2* tw2 = nullptr;    // row roots
+    ulonglong2* tw2i = nullptr;
     uint64_t* W = nullptr;        // [n1][n2] forward twiddle, Montgomery form
     uint64_t* Wi = nullptr;       // inverse twiddle * N^-1, Montgomery form
-    int C = 1;                    // columns per CTA in the column passes
-    int R = 1;                    // rows per CTA in the row passes
+    uint64_t* WiR = nullptr;      // Wi * 2^64: for products of two plain transforms
+    std::mutex mu;                // guards the lazy WiR
 };
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr uint64_t k2P = 2 * kPm;
 
-__device__ __forceinline__ ulonglong2 ld2(const ulonglong2* p) { return __ldg(p); }
+// ---- lazy field arithmetic ------------------------------------------------
 
-// Forward negacyclic NTT of `cnt` transforms of length n = 2^logn stored in
-// shared memory at x + c*ld (c < cnt).  All threads of the CTA take part.
-__device__ void smem_fwd(uint64_t* x, int cnt, int ld, int logn, const ulonglong2* __restrict__ psi) {
-    const int half = 1 << (logn - 1);
-    const int total = cnt * half;
-    for (int s = 0; s < logn; ++s) {
-        const int m = 1 << s;            // groups
-        const int lt = logn - 1 - s;     // log2 of butterfly span t
-        for (int b = threadIdx.x; b < total; b += blockDim.x) {
-            const int c = b >> (logn - 1);
-            const int bb = b & (half - 1);
-            const int i = bb >> lt;
-            const int j = bb & ((1 << lt) - 1);
-            uint64_t* y = x + c * ld + (i << (lt + 1)) + j;
-            const ulonglong2 S = ld2(psi + m + i);
-            const uint64_t U = y[0];
-            const uint64_t V = shoup_mul(y[1 << lt], S.x, S.y);
-            y[0] = add_p(U, V);
-            y[1 << lt] = sub_p(U, V);
+__device__ __forceinline__ uint64_t csub(uint64_t a, uint64_t m) { return a >= m ? a - m : a; }
+
+// a*w mod p in [0, 2p) for any 64-bit a; wq = floor(w * 2^64 / p).
+__device__ __forceinline__ uint64_t shoup_lazy(uint64_t a, uint64_t w, uint64_t wq) {
+    const uint64_t q = __umul64hi(a, wq);
+    return a * w - q * kPm;
+}
+
+// Montgomery product a*b*2^-64 in [0, 2p) for a < 4p, b < p.
+__device__ __forceinline__ uint64_t mont_lazy(uint64_t a, uint64_t b) {
+    const uint64_t lo = a * b;
+    const uint64_t hi = __umul64hi(a, b);
+    const uint64_t m = lo * kPNegInv;
+    return hi + __umul64hi(m, kPm) + (lo != 0 ? 1 : 0);
+}
+
+// Forward butterfly: X, Y in [0, 4p) -> X + wY, X - wY in [0, 4p).
+__device__ __forceinline__ void ct_bfly(uint64_t& X, uint64_t& Y, ulonglong2 w) {
+    const uint64_t x = csub(X, k2P);
+    const uint64_t t = shoup_lazy(Y, w.x, w.y);
+    X = x + t;
+    Y = x - t + k2P;
+}
+
+// Inverse butterfly: X, Y in [0, 2p) -> X + Y, (X - Y) w in [0, 2p).
+__device__ __forceinline__ void gs_bfly(uint64_t& X, uint64_t& Y, ulonglong2 w) {
+    const uint64_t s = csub(X + Y, k2P);
+    Y = shoup_lazy(X - Y + k2P, w.x, w.y);
+    X = s;
+}
+
+// ---- phase geometry ----------------------------------------------------------
+
+template <int L>
+struct Geo {
+    static constexpr int n = 1 << L;
+    static constexpr int E = L >= 4 ? 16 : n;         // elements per thread
+    static constexpr int T = n / E;                    // threads per transform
+    static constexpr int NPH = (L + 3) / 4;            // phases (0 when n = 1)
+    static constexpr int PAD = n + n / 16;             // padded smem length
+    __host__ __device__ static constexpr int r(int p) { return L - 4 * p < 4 ? L - 4 * p : 4; }
+};
+
+__host__ __device__ constexpr int last_phase(int L) { return L == 0 ? 0 : (L + 3) / 4 - 1; }
+
+// Element index (within the transform) of register e of thread t in phase P.
+template <int L, int P>
+__device__ __forceinline__ int eidx(int t, int e) {
+    constexpr int s0 = 4 * P, r = Geo<L>::r(P), U = Geo<L>::E >> r, ltl = L - s0 - r;
+    const int v = e >> r, k = e & ((1 << r) - 1);
+    const int u = t * U + v;
+    return ((u >> ltl) << (L - s0)) + (u & ((1 << ltl) - 1)) + (k << ltl);
+}
+
+// Position of element i in the permuted row-output order.
+template <int L>
+__device__ __forceinline__ int perm_pos(int i) {
+    if constexpr (L >= 4) return (i & 15) * Geo<L>::T + (i >> 4);
+    else return i;
+}
+
+template <int L, int P, bool INV>
+__device__ __forceinline__ void run_phase(uint64_t (&x)[Geo<L>::E], int t,
+                                          const ulonglong2* __restrict__ tw) {
+    constexpr int s0 = 4 * P, r = Geo<L>::r(P), U = Geo<L>::E >> r, ltl = L - s0 - r;
+#pragma unroll
+    for (int v = 0; v < U; ++v) {
+        const int g = (t * U + v) >> ltl;
+        const int o = v << r;
+        if constexpr (!INV) {
+#pragma unroll
+            for (int q = 0; q < r; ++q) {
+#pragma unroll
+                for (int sub = 0; sub < (1 << q); ++sub) {
+                    const ulonglong2 w = __ldg(tw + (1 << (s0 + q)) + (sub << s0) + g);
+#pragma unroll
+                    for (int kk = 0; kk < (1 << (r - 1 - q)); ++kk) {
+                        const int k = o + (sub << (r - q)) + kk;
+                        ct_bfly(x[k], x[k + (1 << (r - 1 - q))], w);
+                    }
+                }
+            }
+        } else {
+            // Gentleman-Sande: the same stages, last to first (an ascending
+            // counter keeps the loop fully unrolled and x in registers).
+#pragma unroll
+            for (int qq = 0; qq < r; ++qq) {
+                const int q = r - 1 - qq;
+#pragma unroll
+                for (int sub = 0; sub < (1 << q); ++sub) {
+                    const ulonglong2 w = __ldg(tw + (1 << (s0 + q)) + (sub << s0) + g);
+#pragma unroll
+                    for (int kk = 0; kk < (1 << (r - 1 - q)); ++kk) {
+                        const int k = o + (sub << (r - q)) + kk;
+                        gs_bfly(x[k], x[k + (1 << (r - 1 - q))], w);
+                    }
+                }
+            }
         }
-        __syncthreads();
     }
 }
 
-// Inverse (Gentleman-Sande), no 1/n scaling.
-__device__ void smem_inv(uint64_t* x, int cnt, int ld, int logn, const ulonglong2* __restrict__ psii) {
-    const int half = 1 << (logn - 1);
-    const int total = cnt * half;
-    for (int s = logn - 1; s >= 0; --s) {
-        const int h = 1 << s;             // groups
-        const int lt = logn - 1 - s;      // log2 t
-        for (int b = threadIdx.x; b < total; b += blockDim.x) {
-            const int c = b >> (logn - 1);
-            const int bb = b & (half - 1);
-            const int i = bb >> lt;
-            const int j = bb & ((1 << lt) - 1);
-            uint64_t* y = x + c * ld + (i << (lt + 1)) + j;
-            const ulonglong2 S = ld2(psii + h + i);
-            const uint64_t U = y[0], V = y[1 << lt];
-            y[0] = add_p(U, V);
-            y[1 << lt] = shoup_mul(sub_p(U, V), S.x, S.y);
-        }
-        __syncthreads();
-    }
-}
+// Element i of one transform in shared memory: base[(i + i/16) * S].
+template <int S>
+struct SmemLay {
+    uint64_t* base;
+    __device__ __forceinline__ uint64_t& at(int i) const { return base[(i + (i >> 4)) * S]; }
+};
 
-// Column pass, forward.  grid = (n2 / C, batch).  src may differ from dst;
-// reduce_in maps arbitrary 64-bit inputs into [0, p) first.
-__global__ void __launch_bounds__(kThreads) col_fwd_kernel(const uint64_t* __restrict__ src,
-                                                           uint64_t* __restrict__ dst, int l1,
-                                                           int l2, int C,
-                                                           const ulonglong2* __restrict__ psi1,
-                                                           const uint64_t* __restrict__ W,
-                                                           int reduce_in) {
-    extern __shared__ uint64_t sm[];
-    const int n1 = 1 << l1, n2 = 1 << l2, ld = n1 + 1;
-    const size_t N = static_cast<size_t>(n1) * n2;
-    const uint64_t* s = src + blockIdx.y * N;
-    uint64_t* d = dst + blockIdx.y * N;
-    const int j0 = blockIdx.x * C;
-    for (int e = threadIdx.x; e < n1 * C; e += blockDim.x) {
-        const int k = e / C, c = e - k * C;
-        uint64_t v = s[static_cast<size_t>(k) * n2 + j0 + c];
-        sm[c * ld + k] = reduce_in ? reduce_p(v) : v;
-    }
+// Registers in phase A layout -> shared memory -> registers in phase B layout.
+template <int L, int A, int B, class Lay>
+__device__ __forceinline__ void exchange(uint64_t (&x)[Geo<L>::E], int t, const Lay& lay) {
+#pragma unroll
+    for (int e = 0; e < Geo<L>::E; ++e) lay.at(eidx<L, A>(t, e)) = x[e];
     __syncthreads();
-    if (l1 > 0) smem_fwd(sm, C, ld, l1, psi1);
-    for (int e = threadIdx.x; e < n1 * C; e += blockDim.x) {
-        const int k = e / C, c = e - k * C;
-        const size_t g = static_cast<size_t>(k) * n2 + j0 + c;
-        d[g] = mont_mul(sm[c * ld + k], __ldg(W + g));
-    }
-}
-
-// Column pass, inverse (output in natural coefficient order).
-__global__ void __launch_bounds__(kThreads) col_inv_kernel(uint64_t* __restrict__ d_all, int l1,
-                                                           int l2, int C,
-                                                           const ulonglong2* __restrict__ psi1i) {
-    extern __shared__ uint64_t sm[];
-    const int n1 = 1 << l1, n2 = 1 << l2, ld = n1 + 1;
-    const size_t N = static_cast<size_t>(n1) * n2;
-    uint64_t* d = d_all + blockIdx.y * N;
-    const int j0 = blockIdx.x * C;
-    for (int e = threadIdx.x; e < n1 * C; e += blockDim.x) {
-        const int k = e / C, c = e - k * C;
-        sm[c * ld + k] = d[static_cast<size_t>(k) * n2 + j0 + c];
-    }
+#pragma unroll
+    for (int e = 0; e < Geo<L>::E; ++e) x[e] = lay.at(eidx<L, B>(t, e));
     __syncthreads();
-    if (l1 > 0) smem_inv(sm, C, ld, l1, psi1i);
-    for (int e = threadIdx.x; e < n1 * C; e += blockDim.x) {
-        const int k = e / C, c = e - k * C;
-        d[static_cast<size_t>(k) * n2 + j0 + c] = sm[c * ld + k];
+}
+
+// All forward phases: registers start in phase 0 layout, end in the last.
+template <int L, int P = 0, class Lay>
+__device__ __forceinline__ void forward_all(uint64_t (&x)[Geo<L>::E], int t,
+                                            const ulonglong2* __restrict__ tw, const Lay& lay) {
+    if constexpr (P < Geo<L>::NPH) {
+        if constexpr (P > 0) exchange<L, P - 1, P>(x, t, lay);
+        run_phase<L, P, false>(x, t, tw);
+        forward_all<L, P + 1>(x, t, tw, lay);
     }
 }
 
-// Row pass, forward.  grid = (n1 / R, batch).
-__global__ void __launch_bounds__(kThreads) row_fwd_kernel(uint64_t* __restrict__ d_all, int l1,
-                                                           int l2, int R,
-                                                           const ulonglong2* __restrict__ psi2) {
-    extern __shared__ uint64_t sm[];
-    const int n2 = 1 << l2;
-    const size_t N = static_cast<size_t>(1) << (l1 + l2);
-    uint64_t* d = d_all + blockIdx.y * N + static_cast<size_t>(blockIdx.x) * R * n2;
-    for (int e = threadIdx.x; e < R * n2; e += blockDim.x) sm[e] = d[e];
-    __syncthreads();
-    if (l2 > 0) smem_fwd(sm, R, n2, l2, psi2);
-    for (int e = threadIdx.x; e < R * n2; e += blockDim.x) d[e] = sm[e];
-}
-
-// Row pass, inverse, with the inverse twiddle (and N^-1) applied.
-// If other != nullptr the rows are first forward-transformed and multiplied
-// pointwise by `other` (a fully transformed operand): c = INTT(NTT(b) * a).
-__global__ void __launch_bounds__(kThreads) row_inv_kernel(const uint64_t* __restrict__ src_all,
-                                                           uint64_t* __restrict__ dst_all,
-                                                           const uint64_t* __restrict__ other_all,
-                                                           int l1, int l2, int R,
-                                                           const ulonglong2* __restrict__ psi2,
-                                                           const ulonglong2* __restrict__ psi2i,
-                                                           const uint64_t* __restrict__ Wi,
-                                                           uint64_t r2) {
-    extern __shared__ uint64_t sm[];
-    const int n2 = 1 << l2;
-    const size_t N = static_cast<size_t>(1) << (l1 + l2);
-    const size_t base = blockIdx.y * N + static_cast<size_t>(blockIdx.x) * R * n2;
-    const uint64_t* s = src_all + base;
-    for (int e = threadIdx.x; e < R * n2; e += blockDim.x) sm[e] = s[e];
-    __syncthreads();
-    if (other_all) {
-        if (l2 > 0) smem_fwd(sm, R, n2, l2, psi2);
-        const uint64_t* o = other_all + base;
-        for (int e = threadIdx.x; e < R * n2; e += blockDim.x)
-            sm[e] = mont_mul(mont_mul(sm[e], __ldg(o + e)), r2);
-        __syncthreads();
+// All inverse phases: registers start in the last phase layout, end in phase 0.
+template <int L, int P = Geo<L>::NPH - 1, class Lay>
+__device__ __forceinline__ void inverse_all(uint64_t (&x)[Geo<L>::E], int t,
+                                            const ulonglong2* __restrict__ twi, const Lay& lay) {
+    if constexpr (P >= 0) {
+        if constexpr (P < Geo<L>::NPH - 1) exchange<L, P + 1, P>(x, t, lay);
+        run_phase<L, P, true>(x, t, twi);
+        inverse_all<L, P - 1>(x, t, twi, lay);
     }
-    if (l2 > 0) smem_inv(sm, R, n2, l2, psi2i);
-    uint64_t* d = dst_all + base;
-    const uint64_t* w = Wi + static_cast<size_t>(blockIdx.x) * R * n2;
-    for (int e = threadIdx.x; e < R * n2; e += blockDim.x) d[e] = mont_mul(sm[e], __ldg(w + e));
 }
 
-// Multiply-accumulate row pass: out row = INTT( sum_q NTTrow(g_q) * img_q ),
-// img in Montgomery-scaled form (value * 2^64 mod p).  grid = (n1 / R).
-__global__ void __launch_bounds__(kThreads) row_mac_inv_kernel(
-    const uint64_t* __restrict__ g, const uint64_t* __restrict__ img, int Q, int l1, int l2,
-    int R, const ulonglong2* __restrict__ psi2, const ulonglong2* __restrict__ psi2i,
-    const uint64_t* __restrict__ Wi, uint64_t* __restrict__ out) {
+// ---- kernels -----------------------------------------------------------------
+
+// Columns per CTA of the column passes.  Adjacent columns ride on adjacent
+// lanes: 128-byte row segments up to n1 = 512, then 64, 32 and 16 bytes so
+// that the CTA stays at 512 threads.  (n2 >= n1 = 2^L, so C never exceeds
+// the row length.)
+__host__ __device__ constexpr int col_C(int L) {
+    return L <= 3 ? (1 << L) : (L <= 9 ? 16 : (L == 10 ? 8 : (L == 11 ? 4 : 2)));
+}
+template <int L>
+__host__ __device__ constexpr int col_threads() { return Geo<L>::T * col_C(L); }
+// Transforms per CTA of the row passes (n1 >= 2^(L-1) rows exist).
+template <int L>
+__host__ __device__ constexpr int row_V() {
+    constexpr int half = L >= 1 ? (1 << L) / 2 : 1;
+    return Geo<L>::T >= 64 ? 1 : (64 / Geo<L>::T < half ? 64 / Geo<L>::T : half);
+}
+template <int L>
+__host__ __device__ constexpr int row_threads() { return Geo<L>::T * row_V<L>(); }
+
+// Column pass, forward, then the four-step twiddle.  grid = (n2 / C, batch).
+// src may equal dst (every CTA loads its columns before its first store).
+// REDUCE maps arbitrary 64-bit inputs into [0, p) first; otherwise inputs
+// must be below 4p.  Outputs in [0, p).
+template <int L, bool REDUCE>
+__global__ void __launch_bounds__(col_threads<L>()) col_fwd_kernel(
+    const uint64_t* src, uint64_t* dst, int l2, const ulonglong2* __restrict__ tw,
+    const uint64_t* __restrict__ W) {
+    constexpr int C = col_C(L), E = Geo<L>::E, LP = last_phase(L);
     extern __shared__ uint64_t sm[];
-    const int n2 = 1 << l2;
-    const int len = R * n2;
-    uint64_t* acc = sm + len;
-    const size_t N = static_cast<size_t>(1) << (l1 + l2);
-    const size_t base = static_cast<size_t>(blockIdx.x) * len;
-    for (int e = threadIdx.x; e < len; e += blockDim.x) acc[e] = 0;
+    const int t = threadIdx.x / C, c = threadIdx.x % C;
+    const size_t n2 = size_t{1} << l2;
+    const size_t col = static_cast<size_t>(blockIdx.x) * C + c;
+    const size_t off = static_cast<size_t>(blockIdx.y) * (n2 << L) + col;
+    uint64_t x[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const uint64_t v = src[off + eidx<L, 0>(t, e) * n2];
+        x[e] = REDUCE ? reduce_p(v) : v;
+    }
+    forward_all<L>(x, t, tw, SmemLay<C>{sm + c});
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const size_t i = eidx<L, LP>(t, e);
+        dst[off + i * n2] = csub(mont_lazy(x[e], __ldg(W + i * n2 + col)), kPm);
+    }
+}
+
+// Column pass, inverse, in place (output in natural coefficient order, in
+// [0, p)).
+template <int L>
+__global__ void __launch_bounds__(col_threads<L>()) col_inv_kernel(
+    uint64_t* d, int l2, const ulonglong2* __restrict__ twi) {
+    constexpr int C = col_C(L), E = Geo<L>::E, LP = last_phase(L);
+    extern __shared__ uint64_t sm[];
+    const int t = threadIdx.x / C, c = threadIdx.x % C;
+    const size_t n2 = size_t{1} << l2;
+    const size_t off = static_cast<size_t>(blockIdx.y) * (n2 << L) +
+                       static_cast<size_t>(blockIdx.x) * C + c;
+    uint64_t x[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) x[e] = d[off + eidx<L, LP>(t, e) * n2];
+    inverse_all<L>(x, t, twi, SmemLay<C>{sm + c});
+#pragma unroll
+    for (int e = 0; e < E; ++e) d[off + eidx<L, 0>(t, e) * n2] = csub(x[e], kPm);
+}
+
+// Row pass, forward, in place (each thread reads and writes the same set of
+// positions); outputs in [0, p) in the permuted order.  grid = (n1 / V, batch).
+template <int L>
+__global__ void __launch_bounds__(row_threads<L>()) row_fwd_kernel(
+    uint64_t* d, int l1, const ulonglong2* __restrict__ tw) {
+    constexpr int E = Geo<L>::E, T = Geo<L>::T, V = row_V<L>(), LP = last_phase(L);
+    extern __shared__ uint64_t sm[];
+    const int t = threadIdx.x % T, v = threadIdx.x / T;
+    uint64_t* row = d + static_cast<size_t>(blockIdx.y) * (size_t{1} << (L + l1)) +
+                    (static_cast<size_t>(blockIdx.x) * V + v) * Geo<L>::n;
+    uint64_t x[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) x[e] = row[eidx<L, 0>(t, e)];
+    forward_all<L>(x, t, tw, SmemLay<1>{sm + v * Geo<L>::PAD});
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+        row[perm_pos<L>(eidx<L, LP>(t, e))] = csub(csub(x[e], k2P), kPm);
+}
+
+// Multiply-accumulate row pass:
+//   out row = Wi (.) INTT( sum_q NTT(g_q row) (.) img_q row ),
+// img_q in the permuted evaluation order, Montgomery-scaled so that the
+// Montgomery product gives the plain one.  g rows come from the column pass;
+// out is in [0, p) and may alias g (a CTA reads all its rows before its first
+// store).  grid = (n1 / V, batch): instance b reads g and img at b*Q*N and
+// writes out at b*N.
+template <int L>
+__global__ void __launch_bounds__(row_threads<L>()) row_mac_inv_kernel(
+    const uint64_t* g, const uint64_t* __restrict__ img, int Q, int l1,
+    const ulonglong2* __restrict__ tw, const ulonglong2* __restrict__ twi,
+    const uint64_t* __restrict__ Wi, uint64_t* out) {
+    constexpr int E = Geo<L>::E, T = Geo<L>::T, V = row_V<L>(), LP = last_phase(L);
+    extern __shared__ uint64_t sm[];
+    const int t = threadIdx.x % T, v = threadIdx.x / T;
+    const size_t N = size_t{1} << (L + l1);
+    const size_t base = (static_cast<size_t>(blockIdx.x) * V + v) * Geo<L>::n;
+    g += static_cast<size_t>(blockIdx.y) * Q * N;
+    img += static_cast<size_t>(blockIdx.y) * Q * N;
+    out += static_cast<size_t>(blockIdx.y) * N;
+    const SmemLay<1> lay{sm + v * Geo<L>::PAD};
+    uint64_t acc[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) acc[e] = 0;
     for (int q = 0; q < Q; ++q) {
-        const uint64_t* s = g + q * N + base;
-        for (int e = threadIdx.x; e < len; e += blockDim.x) sm[e] = s[e];
-        __syncthreads();
-        if (l2 > 0) smem_fwd(sm, R, n2, l2, psi2);
+        const uint64_t* gr = g + q * N + base;
         const uint64_t* im = img + q * N + base;
-        for (int e = threadIdx.x; e < len; e += blockDim.x)
-            acc[e] = add_p(acc[e], mont_mul(sm[e], __ldg(im + e)));
-        __syncthreads();
+        uint64_t x[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) x[e] = gr[eidx<L, 0>(t, e)];
+        forward_all<L>(x, t, tw, lay);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const uint64_t m = mont_lazy(x[e], __ldg(im + perm_pos<L>(eidx<L, LP>(t, e))));
+            acc[e] = csub(acc[e] + m, k2P);
+        }
     }
-    if (l2 > 0) smem_inv(acc, R, n2, l2, psi2i);
-    const uint64_t* w = Wi + base;
-    for (int e = threadIdx.x; e < len; e += blockDim.x)
-        out[base + e] = mont_mul(acc[e], __ldg(w + e));
+    inverse_all<L>(acc, t, twi, lay);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const size_t i = base + eidx<L, 0>(t, e);
+        out[i] = csub(mont_lazy(acc[e], __ldg(Wi + i)), kPm);
+    }
 }
 
 // Twiddle tables: W[k*n2 + j2] = psi^(j2*(2*brev(k)+1-n1)) (times R), and
@@ -256,10 +386,18 @@ __global__ void pointwise_kernel(uint64_t* c, const uint64_t* a, const uint64_t*
     c[i] = v;
 }
 
+// d[i] = s[i] * k * R^-1 (Montgomery product with a constant).
+__global__ void scale_const_kernel(uint64_t* d, const uint64_t* s, size_t n, uint64_t k) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) d[i] = mont_mul(s[i], k);
+}
+
 __global__ void reduce_kernel(uint64_t* d, const uint64_t* s, size_t n) {
     const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i < n) d[i] = reduce_p(s[i]);
 }
+
+// ---- host side ---------------------------------------------------------------
 
 uint32_t brev_host(uint32_t x, int bits) {
     uint32_t r = 0;
@@ -274,20 +412,26 @@ uint64_t primitive_root_host() {
         if (pow_p_host(g, (kPm - 1) / 2) != 1 && pow_p_host(g, (kPm - 1) / q2) != 1) return g;
 }
 
-// Roots psi_n^brev(k) (Shoup pairs) for a length-n negacyclic transform.
-ulonglong2* upload_psi_table(uint64_t psi_n, int logn) {
+// Roots of a length-2^logn negacyclic transform with psi_n a primitive
+// 2n-th root: stage s, group i uses psi_n^brev_logn(2^s + i) (Longa-Naehrig
+// table), stored at the phase-permuted slot 2^s + (i % 2^q) * 2^s0 + i / 2^q.
+ulonglong2* upload_root_table(uint64_t psi_n, int logn) {
     const int n = 1 << logn;
     std::vector<uint64_t> pw(n);
     uint64_t a = 1;
     for (int k = 0; k < n; ++k) { pw[k] = a; a = mul_p_host(a, psi_n); }
-    std::vector<ulonglong2> t(n);
-    for (int k = 0; k < n; ++k) {
-        const uint64_t v = pw[brev_host(static_cast<uint32_t>(k), logn)];
-        t[k] = make_ulonglong2(v, shoup_q_host(v));
+    std::vector<ulonglong2> tab(n > 1 ? n : 2, make_ulonglong2(0, 0));
+    for (int s = 0; s < logn; ++s) {
+        const int s0 = 4 * (s / 4), q = s - s0;
+        for (int i = 0; i < (1 << s); ++i) {
+            const uint64_t v = pw[brev_host(static_cast<uint32_t>((1 << s) + i), logn)];
+            const int slot = (1 << s) + ((i & ((1 << q) - 1)) << s0) + (i >> q);
+            tab[slot] = make_ulonglong2(v, shoup_q_host(v));
+        }
     }
     ulonglong2* d = nullptr;
-    PCGB_CK(cudaMalloc(&d, sizeof(ulonglong2) * n));
-    upload_blocking(d, t.data(), sizeof(ulonglong2) * n);
+    PCGB_CK(cudaMalloc(&d, sizeof(ulonglong2) * tab.size()));
+    upload_blocking(d, tab.data(), sizeof(ulonglong2) * tab.size());
     return d;
 }
 
@@ -295,20 +439,17 @@ NttPlan* build_plan(int logN) {
     auto* pl = new NttPlan();
     pl->logN = logN;
     pl->N = static_cast<size_t>(1) << logN;
-    pl->l1 = (logN + 1) / 2;
-    pl->l2 = logN / 2;
+    pl->l1 = logN / 2;
+    pl->l2 = logN - pl->l1;
     pl->n1 = 1 << pl->l1;
     pl->n2 = 1 << pl->l2;
     const uint64_t g = primitive_root_host();
     const uint64_t psi = pow_p_host(g, (kPm - 1) / (2 * pl->N));
     const uint64_t psi_inv = pow_p_host(psi, kPm - 2);
-    pl->psi1 = upload_psi_table(pow_p_host(psi, pl->n2), pl->l1);
-    pl->psi1i = upload_psi_table(pow_p_host(psi_inv, pl->n2), pl->l1);
-    pl->psi2 = upload_psi_table(pow_p_host(psi, pl->n1), pl->l2);
-    pl->psi2i = upload_psi_table(pow_p_host(psi_inv, pl->n1), pl->l2);
-    // Columns per CTA: 8 (64-byte row segments) unless the column is long.
-    pl->C = std::min(pl->n2, std::max(1, std::min(8, 16384 / pl->n1)));
-    pl->R = std::min(pl->n1, std::max(1, 4096 / pl->n2));
+    pl->tw1 = upload_root_table(pow_p_host(psi, pl->n2), pl->l1);
+    pl->tw1i = upload_root_table(pow_p_host(psi_inv, pl->n2), pl->l1);
+    pl->tw2 = upload_root_table(pow_p_host(psi, pl->n1), pl->l2);
+    pl->tw2i = upload_root_table(pow_p_host(psi_inv, pl->n1), pl->l2);
     PCGB_CK(cudaMalloc(&pl->W, sizeof(uint64_t) * pl->N));
     PCGB_CK(cudaMalloc(&pl->Wi, sizeof(uint64_t) * pl->N));
     const uint64_t R = r_mod_p();
@@ -327,47 +468,121 @@ NttPlan* build_plan(int logN) {
     return pl;
 }
 
-size_t col_smem(const NttPlan& pl) { return sizeof(uint64_t) * static_cast<size_t>(pl.n1 + 1) * pl.C; }
-size_t row_smem(const NttPlan& pl) { return sizeof(uint64_t) * static_cast<size_t>(pl.R) * pl.n2; }
+template <int L>
+constexpr size_t col_smem() { return Geo<L>::NPH > 1 ? sizeof(uint64_t) * Geo<L>::PAD * col_C(L) : 0; }
+template <int L>
+constexpr size_t row_smem() { return Geo<L>::NPH > 1 ? sizeof(uint64_t) * Geo<L>::PAD * row_V<L>() : 0; }
 
-void set_smem(const void* f, size_t bytes) {
-    if (bytes > 48 * 1024)
-        PCGB_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+// Dynamic shared memory above 48 KB is opted into once per kernel and device.
+struct OptinOnce {
+    std::mutex mu;
+    std::map<std::pair<const void*, int>, bool> done;
+    template <class K>
+    void operator()(K* kernel, size_t bytes) {
+        if (bytes <= 48 * 1024) return;
+        int dev = 0;
+        PCGB_CK(cudaGetDevice(&dev));
+        std::lock_guard<std::mutex> lk(mu);
+        auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+        if (done[key]) return;
+        PCGB_CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(bytes)));
+        done[key] = true;
+    }
+};
+OptinOnce g_optin;
+
+template <int L>
+void col_fwd_l(const NttPlan& pl, const uint64_t* src, uint64_t* dst, int batch, bool reduce,
+               cudaStream_t st) {
+    constexpr size_t sm = col_smem<L>();
+    const dim3 grid(pl.n2 / col_C(L), batch);
+    if (reduce) {
+        g_optin(col_fwd_kernel<L, true>, sm);
+        col_fwd_kernel<L, true><<<grid, col_threads<L>(), sm, st>>>(src, dst, pl.l2, pl.tw1, pl.W);
+    } else {
+        g_optin(col_fwd_kernel<L, false>, sm);
+        col_fwd_kernel<L, false><<<grid, col_threads<L>(), sm, st>>>(src, dst, pl.l2, pl.tw1, pl.W);
+    }
+    PCGB_POST_LAUNCH();
 }
 
-void col_fwd(const NttPlan& pl, const uint64_t* src, uint64_t* dst, int batch, bool reduce_in,
+template <int L>
+void col_inv_l(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
+    constexpr size_t sm = col_smem<L>();
+    g_optin(col_inv_kernel<L>, sm);
+    col_inv_kernel<L><<<dim3(pl.n2 / col_C(L), batch), col_threads<L>(), sm, st>>>(d, pl.l2,
+                                                                                  pl.tw1i);
+    PCGB_POST_LAUNCH();
+}
+
+template <int L>
+void row_fwd_l(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
+    constexpr size_t sm = row_smem<L>();
+    g_optin(row_fwd_kernel<L>, sm);
+    row_fwd_kernel<L><<<dim3(pl.n1 / row_V<L>(), batch), row_threads<L>(), sm, st>>>(d, pl.l1,
+                                                                                    pl.tw2);
+    PCGB_POST_LAUNCH();
+}
+
+template <int L>
+void row_mac_l(const NttPlan& pl, const uint64_t* g, const uint64_t* img, int Q, int batch,
+               const uint64_t* Wi, uint64_t* out, cudaStream_t st) {
+    constexpr size_t sm = row_smem<L>();
+    g_optin(row_mac_inv_kernel<L>, sm);
+    row_mac_inv_kernel<L><<<dim3(pl.n1 / row_V<L>(), batch), row_threads<L>(), sm, st>>>(
+        g, img, Q, pl.l1, pl.tw2, pl.tw2i, Wi, out);
+    PCGB_POST_LAUNCH();
+}
+
+// Runtime sub-length -> template instance (2^0 .. 2^12).
+template <class F>
+void by_len(int L, F&& f) {
+    switch (L) {
+        case 0: f(std::integral_constant<int, 0>{}); break;
+        case 1: f(std::integral_constant<int, 1>{}); break;
+        case 2: f(std::integral_constant<int, 2>{}); break;
+        case 3: f(std::integral_constant<int, 3>{}); break;
+        case 4: f(std::integral_constant<int, 4>{}); break;
+        case 5: f(std::integral_constant<int, 5>{}); break;
+        case 6: f(std::integral_constant<int, 6>{}); break;
+        case 7: f(std::integral_constant<int, 7>{}); break;
+        case 8: f(std::integral_constant<int, 8>{}); break;
+        case 9: f(std::integral_constant<int, 9>{}); break;
+        case 10: f(std::integral_constant<int, 10>{}); break;
+        case 11: f(std::integral_constant<int, 11>{}); break;
+        case 12: f(std::integral_constant<int, 12>{}); break;
+        default: fail(PCGB_EINVAL, "NTT sub-length out of range");
+    }
+}
+
+void col_fwd(const NttPlan& pl, const uint64_t* src, uint64_t* dst, int batch, bool reduce,
              cudaStream_t st) {
-    const size_t sm = col_smem(pl);
-    set_smem(reinterpret_cast<const void*>(col_fwd_kernel), sm);
-    col_fwd_kernel<<<dim3(pl.n2 / pl.C, batch), kThreads, sm, st>>>(src, dst, pl.l1, pl.l2, pl.C,
-                                                                    pl.psi1, pl.W, reduce_in);
-    PCGB_POST_LAUNCH();
+    by_len(pl.l1, [&](auto L) { col_fwd_l<decltype(L)::value>(pl, src, dst, batch, reduce, st); });
 }
-
 void col_inv(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
-    const size_t sm = col_smem(pl);
-    set_smem(reinterpret_cast<const void*>(col_inv_kernel), sm);
-    col_inv_kernel<<<dim3(pl.n2 / pl.C, batch), kThreads, sm, st>>>(d, pl.l1, pl.l2, pl.C,
-                                                                    pl.psi1i);
-    PCGB_POST_LAUNCH();
+    by_len(pl.l1, [&](auto L) { col_inv_l<decltype(L)::value>(pl, d, batch, st); });
 }
-
 void row_fwd(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
-    const size_t sm = row_smem(pl);
-    set_smem(reinterpret_cast<const void*>(row_fwd_kernel), sm);
-    row_fwd_kernel<<<dim3(pl.n1 / pl.R, batch), kThreads, sm, st>>>(d, pl.l1, pl.l2, pl.R,
-                                                                    pl.psi2);
-    PCGB_POST_LAUNCH();
+    by_len(pl.l2, [&](auto L) { row_fwd_l<decltype(L)::value>(pl, d, batch, st); });
+}
+void row_mac(const NttPlan& pl, const uint64_t* g, const uint64_t* img, int Q, int batch,
+             const uint64_t* Wi, uint64_t* out, cudaStream_t st) {
+    by_len(pl.l2,
+           [&](auto L) { row_mac_l<decltype(L)::value>(pl, g, img, Q, batch, Wi, out, st); });
 }
 
-void row_inv(const NttPlan& pl, const uint64_t* src, uint64_t* dst, const uint64_t* other,
-             int batch, cudaStream_t st) {
-    const size_t sm = row_smem(pl);
-    set_smem(reinterpret_cast<const void*>(row_inv_kernel), sm);
-    row_inv_kernel<<<dim3(pl.n1 / pl.R, batch), kThreads, sm, st>>>(
-        src, dst, other, pl.l1, pl.l2, pl.R, pl.psi2, pl.psi2i, pl.Wi, r2_mod_p());
-    PCGB_POST_LAUNCH();
+const uint64_t* wi_times_r(NttPlan& pl, cudaStream_t st) {
+    std::lock_guard<std::mutex> lk(pl.mu);
+    if (!pl.WiR) {
+        PCGB_CK(cudaMalloc(&pl.WiR, sizeof(uint64_t) * pl.N));
+        scale_const_kernel<<<static_cast<unsigned>((pl.N + 255) / 256), 256, 0, st>>>(
+            pl.WiR, pl.Wi, pl.N, r2_mod_p());
+        PCGB_POST_LAUNCH();
+        PCGB_CK(cudaStreamSynchronize(st));
+    }
+    return pl.WiR;
 }
 
 }  // namespace
@@ -389,31 +604,22 @@ void ntt_forward(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
     row_fwd(pl, d, batch, st);
 }
 
-void ntt_inverse(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
-    row_inv(pl, d, d, nullptr, batch, st);
-    col_inv(pl, d, batch, st);
-}
-
 void poly_mul_device(const NttPlan& pl, uint64_t* c, const uint64_t* a, const uint64_t* b,
                      int batch, uint64_t* scratch, cudaStream_t st) {
-    const size_t n = pl.N * static_cast<size_t>(batch);
-    uint64_t* A = scratch;
-    uint64_t* B = scratch + n;
-    col_fwd(pl, a, A, batch, true, st);
-    row_fwd(pl, A, batch, st);
-    col_fwd(pl, b, B, batch, true, st);
-    row_inv(pl, B, c, A, batch, st);  // c rows = INTT(NTT(B) * A) with the inverse twiddle
+    const uint64_t* wir = wi_times_r(const_cast<NttPlan&>(pl), st);
+    // A = NTT(a) in scratch; c = column pass of b; c = INTT(NTT(c) (.) A).
+    // a is read before c is first written, so c may alias a or b.
+    col_fwd(pl, a, scratch, batch, true, st);
+    row_fwd(pl, scratch, batch, st);
+    col_fwd(pl, b, c, batch, true, st);
+    row_mac(pl, c, scratch, 1, batch, wir, c, st);
     col_inv(pl, c, batch, st);
 }
 
 void ntt_mac_inverse(const NttPlan& pl, uint64_t* g, const uint64_t* img, int Q, uint64_t* acc,
                      cudaStream_t st) {
     col_fwd(pl, g, g, Q, false, st);
-    const size_t sm = 2 * row_smem(pl);
-    set_smem(reinterpret_cast<const void*>(row_mac_inv_kernel), sm);
-    row_mac_inv_kernel<<<pl.n1 / pl.R, kThreads, sm, st>>>(g, img, Q, pl.l1, pl.l2, pl.R, pl.psi2,
-                                                           pl.psi2i, pl.Wi, acc);
-    PCGB_POST_LAUNCH();
+    row_mac(pl, g, img, Q, 1, pl.Wi, acc, st);
     col_inv(pl, acc, 1, st);
 }
 

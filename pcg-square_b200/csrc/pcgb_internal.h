@@ -54,6 +54,11 @@ inline cudaStream_t as_stream(void* s) {
 // cudaMemcpy from pageable memory may return before its DMA completes, and
 // work on the library's non-blocking streams is not ordered after it.
 void upload_blocking(void* d_dst, const void* src, size_t bytes);
+// Stream-ordered allocation from the library's own per-device pool, which
+// keeps freed memory mapped for the next request (release with
+// pcgb_trim_pool).  Free with cudaFreeAsync.
+void* pool_alloc(size_t bytes, cudaStream_t st);
+cudaMemPool_t library_pool();
 
 // Number of SMs of the current device.
 int sm_count();
@@ -162,9 +167,8 @@ const NttPlan& ntt_plan(int logN);   // resident per (device, logN)
 // In-place forward transform of `batch` length-N polys into the internal
 // evaluation layout (coefficients must be < p).
 void ntt_forward(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st);
-void ntt_inverse(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st);
 // c = a * b mod (X^N+1) for `batch` polys; c may alias a or b; inputs any
-// uint64 (reduced mod p first).  scratch: 2*batch*N words.
+// uint64 (reduced mod p first).  scratch: batch*N words.
 void poly_mul_device(const NttPlan& pl, uint64_t* c, const uint64_t* a, const uint64_t* b,
                      int batch, uint64_t* scratch, cudaStream_t st);
 // acc = INTT( sum_q img[q] (.) NTT(g[q]) ); g is consumed (transformed in

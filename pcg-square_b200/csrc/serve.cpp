@@ -9,8 +9,8 @@
 // keys), noise, the fused expansion against the shape's resident plan (a_i
 // images, gather plan, NTT tables), and a device digest of x and z; a host
 // callback (cudaLaunchHostFunc) stamps the completion time and wakes the
-// worker.  Memory comes from the stream-ordered pool (cudaMallocAsync /
-// cudaFreeAsync on the slot's stream), so a finished request's memory is
+// worker.  Memory comes from the library's stream-ordered pool (allocated and
+// freed on the slot's stream), so a finished request's memory is
 // reused by the next one without a device synchronisation.
 //
 // The reference has no serving path; its one-request-at-a-time flow is
@@ -142,7 +142,7 @@ void launch(pcgb_server* s, Req* r) {
     expander_info(e, &K, &levels, &nk, &wsb);
     const size_t ct = static_cast<size_t>(r->r.c) * r->r.t, N = r->r.N;
     char* base = nullptr;
-    PCGB_CK(cudaMallocAsync(reinterpret_cast<void**>(&base), r->bytes, st));
+    base = static_cast<char*>(pool_alloc(r->bytes, st));
     size_t off = 0;
     auto take = [&](size_t bytes) {
         char* p = base + off;
@@ -253,13 +253,6 @@ pcgb_server* server_create(int n_streams, size_t budget, int max_in_flight, uint
         budget = free_b / 2;
     }
     s->budget = budget;
-    // Keep freed pool memory mapped (the default threshold of 0 returns it to
-    // the OS at every synchronisation, so each multi-GB request would map
-    // its memory again).
-    cudaMemPool_t pool = nullptr;
-    PCGB_CK(cudaDeviceGetDefaultMemPool(&pool, s->dev));
-    uint64_t keep = UINT64_MAX;
-    PCGB_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     s->streams.resize(n_streams);
     s->slot_req.assign(n_streams, nullptr);
     for (auto& st : s->streams) PCGB_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));

@@ -70,6 +70,7 @@ def _load():
         "pcgb_memset": ([_vp, C.c_int, C.c_size_t, _vp], C.c_int),
         "pcgb_stream_synchronize": ([_vp], C.c_int),
         "pcgb_device_synchronize": ([], C.c_int),
+        "pcgb_trim_pool": ([], C.c_int),
         "pcgb_default_stream": ([], _vp),
         "pcgb_dpf_batch_full_eval": ([C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, C.c_int, _vp, _vp,
                                       _vp, C.c_int], C.c_int),
@@ -217,6 +218,11 @@ def to_device(arr):
 
 def synchronize():
     _check(lib.pcgb_device_synchronize())
+
+
+def trim_pool():
+    """Return the library pool's cached scratch on the current device."""
+    _check(lib.pcgb_trim_pool())
 
 
 def launch_count():
