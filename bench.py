@@ -127,6 +127,8 @@ def parse():
     ap.add_argument("--no-verify", action="store_true")
     ap.add_argument("--no-polymul", dest="polymul", action="store_false",
                     help="skip the batched 16 x 2^20 poly-mul measurement")
+    ap.add_argument("--polymul-only", action="store_true",
+                    help="only the batched poly-mul measurement (profiler captures)")
     ap.add_argument("--serve-requests", type=int, default=200,
                     help="seeded subsample of the serving stream (0 = skip)")
     # Smaller shapes for profiler captures; the bench line is quoted at the defaults.
@@ -539,6 +541,11 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, d)
+        elif args.polymul_only:
+            import pcg_b200 as L
+            if d.rank == 0:
+                print(json.dumps({"poly_mul": run_polymul(L, steps=args.steps,
+                                                          warmup=args.warmup)}), flush=True)
         else:
             run_ours(args, d)
     finally:
