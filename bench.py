@@ -228,27 +228,32 @@ class Clocks:
 
 
 # ---- CPU baseline (oracle port, bounded sample) ------------------------------
-def cpu_sample(threads, n_blocks=None, keys=None, polymuls=None):
+def cpu_sample(threads, n_blocks=None, keys=None, polymuls=None, shape=None):
     """Times a bounded sample of the oracle's expansion and extrapolates to one
-    full expansion: returns (corr/s, seconds of CPU work, description)."""
+    full expansion: returns (corr/s, seconds of CPU work, description).
+    shape = (N, c, t), default the headline shape."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_lib as O
-    s = O.shape(N, C_, T_)
-    if not hasattr(cpu_sample, "material"):
+    n_, c_, t_ = shape or (N, C_, T_)
+    key = (n_, c_, t_)
+    cache = cpu_sample.__dict__.setdefault("material", {})
+    s = O.shape(n_, c_, t_)
+    if key not in cache:
         r0, _, cws, cwo = O.deal_keys(s, 1000)
-        cpu_sample.material = (r0, cws, cwo, O.public_a(s, A_SEED))
-    r0, cws, cwo, a = cpu_sample.material
-    B = T_ * T_
+        cache[key] = (r0, cws, cwo, O.public_a(s, A_SEED))
+    r0, cws, cwo, a = cache[key]
+    B = t_ * t_
     n_blocks = n_blocks or 1
-    keys = keys or min(B, max(threads, 32))
-    polymuls = polymuls or threads
+    keys = min(B, keys or max(threads, 32))
+    n_products = c_ + 2 * c_ * c_   # step 4 of pcg_ole_impl.h:460-483
+    polymuls = min(n_products, polymuls or threads)
     t_dpf, t_ntt = O.bench_sample(s, 0, r0, cws, cwo, a, n_blocks, keys, polymuls, threads)
-    total_keys = C_ * C_ * B
-    n_products = C_ + 2 * C_ * C_   # step 4 of pcg_ole_impl.h:460-483
+    total_keys = c_ * c_ * B
     t_full = t_dpf * total_keys / (n_blocks * keys) + t_ntt * n_products / polymuls
     desc = (f"{n_blocks * keys} of {total_keys} keys (DPF+convert+scatter) and {polymuls} of "
-            f"{n_products} length-2^20 products, {threads} threads, extrapolated to one expansion")
-    return N / t_full, t_dpf + t_ntt, desc
+            f"{n_products} length-2^{n_.bit_length() - 1} products, {threads} threads, "
+            "extrapolated to one expansion")
+    return n_ / t_full, t_dpf + t_ntt, desc
 
 
 def run_reference(args, d):
@@ -405,7 +410,7 @@ def run_ours(args, d):
     cpu = None
     if d.world == 1 and d.rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        v, sec, desc = cpu_sample(threads)
+        v, sec, desc = cpu_sample(threads, shape=(N, C_, T_))
         cpu = {"value": v, "unit": "corr/s", "cores": threads, "kind": "port",
                "sample": desc, "sample_seconds": sec}
 
@@ -485,9 +490,13 @@ def run_serving(L, n_req, seed=2025, util=0.85):
     for shp in SERVE_SHAPES:
         batched.prepare(*shp)
         single.prepare(*shp)
-    # Calibrate the arrival rate on the mean one-at-a-time service time.
-    calib = [SERVE_SHAPES[i] for i in rng.integers(len(SERVE_SHAPES), size=24)]
-    res = single.run_trace([(N, c, t, 0, 1000 + i, 0.0) for i, (N, c, t) in enumerate(calib)])
+    # Warm both servers on every shape (first launches, pool growth), then
+    # calibrate the arrival rate on the exact mean one-at-a-time service time
+    # of the uniform shape mix: one timed request per shape.
+    warm = [(N, c, t, 0, 900 + i, 0.0) for i, (N, c, t) in enumerate(SERVE_SHAPES)]
+    batched.run_trace(warm)
+    single.run_trace(warm)
+    res = single.run_trace([(N, c, t, 0, 1000 + i, 0.0) for i, (N, c, t) in enumerate(SERVE_SHAPES)])
     svc = float(np.mean([r.done_s - r.start_s for r in res]))
     rate = util / svc
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))

@@ -1,0 +1,156 @@
+"""Batched DPF full-domain evaluation + leaf convert, 4096 keys x 2^16 leaves
+(w = 1), ChaCha8 and AES tree PRGs: the library against the reference's own
+GPU kernels (oracle/_ref/libref_gpu.so, GPU_baseline/common/{dpf_gpu,
+leaf_convert_cuda}.cu compiled unmodified).
+
+TEST INFRASTRUCTURE: a measurement script, not product code.
+
+Keys are random roots and per-level correction words.  The reference's GPU
+entry point is interactive (dpf_gpu.h:55-75): after every level it hands the
+host the current shares and takes the peer's back.  Here the exchange
+returns peer = my ^ CW, which makes the interactive evaluation equal to the
+keyed one, so three paths compute the same leaves:
+
+  ref      reference dpf_gpu_batch_full_eval_device + dpf_out_sums
+  drop_in  the library's dpf_gpu_batch_full_eval_device + dpf_out_sums,
+           same exchange callback
+  keyed    the library's pcgb_dpf_keyed_full_eval (no exchange) +
+           dpf_out_sums
+
+Bit-exactness: per-instance sums (C mod p and T) of all B instances and the
+leaves of the first and last instance must agree across the three paths.
+Times are wall-clock per call with the device synchronised (the interactive
+paths include their per-level host round trips, as the reference's do).
+
+Usage: python oracle/dpf_convert_bench.py [--B 4096] [--n 16] [--iters 3]
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.join(os.path.dirname(HERE), "pcg-square_b200"))
+
+import oracle_lib as O  # noqa: E402
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--B", type=int, default=4096)
+    ap.add_argument("--n", type=int, default=16)
+    ap.add_argument("--iters", type=int, default=3)
+    ap.add_argument("--seed", type=int, default=33)
+    args = ap.parse_args()
+    import pcg_b200 as L
+
+    R = O.ref_gpu()
+    if R is None:
+        raise SystemExit("oracle/_ref/libref_gpu.so not built")
+    B, n, w = args.B, args.n, 1
+    D, levels, nk = 1 << n, n // w, (1 << w) - 1
+    rng = np.random.default_rng(args.seed)
+    roots = rng.integers(0, 2**64 - 1, (B, 2), dtype=np.uint64)
+    cws = rng.integers(0, 2**64 - 1, (B, levels * nk, 2), dtype=np.uint64)
+    zero_dlt = np.zeros((B * levels * nk, 2), np.uint64)
+    d_roots, d_cws = L.to_device(roots), L.to_device(cws)
+    d_keyed = L.DeviceBuffer(16 * B * D)
+
+    EX = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p)
+    out = {"workload": f"{B} keys x 2^{n} leaves, w={w}, DPF full-domain eval + out_sums",
+           "device": L.device_name(), "iters": args.iters}
+
+    for prg_name, prg in (("chacha8", L.PRG_CHACHA8), ("aes", L.PRG_AES)):
+        rks = O.aes_tree_round_keys(rng.integers(0, 256, 16, dtype=np.uint8), nk) \
+            if prg == L.PRG_AES else None
+        level = [0]
+
+        def ex(my, peer, count, user):
+            m = np.ctypeslib.as_array(C.cast(my, C.POINTER(C.c_uint64)), shape=(count, 2))
+            p = np.ctypeslib.as_array(C.cast(peer, C.POINTER(C.c_uint64)), shape=(count, 2))
+            p[:] = m ^ cws[:, level[0]]
+            level[0] += 1
+
+        cb = EX(ex)
+
+        def run_ref():
+            level[0] = 0
+            d = C.c_void_p()
+            rc = R.ref_dpf_batch_full_eval_device(
+                B, n, w, roots.ctypes.data, zero_dlt.ctypes.data,
+                None if rks is None else rks.ctypes.data, 0, C.cast(cb, C.c_void_p), None,
+                1 if prg == L.PRG_CHACHA8 else 0, C.byref(d))
+            assert rc == 0, R.ref_last_error()
+            R.ref_sync()
+            t1 = time.perf_counter()
+            sc, st = np.zeros(B, np.uint64), np.zeros(B, np.uint64)
+            assert R.ref_dpf_out_sums(d.value, B, D, O.P, sc, st) == 0
+            return d.value, sc, st, t1
+
+        def run_drop_in():
+            level[0] = 0
+            d = L.dpf_gpu_batch_full_eval_device(B, n, w, roots, zero_dlt, round_keys=rks,
+                                                 exchange=lambda my: my ^ cws[:, _next(level)],
+                                                 prg=prg)
+            L.synchronize()
+            t1 = time.perf_counter()
+            sc, st = L.dpf_out_sums(d, B, D)
+            return d, sc, st, t1
+
+        def run_keyed():
+            L.dpf_keyed_full_eval_device(B, n, w, prg, d_roots.ptr, d_cws.ptr, d_keyed.ptr,
+                                         round_keys=rks)
+            L.synchronize()
+            t1 = time.perf_counter()
+            sc, st = L.dpf_out_sums(d_keyed.ptr, B, D)
+            return d_keyed.ptr, sc, st, t1
+
+        res = {}
+        for name, fn in (("ref", run_ref), ("drop_in", run_drop_in), ("keyed", run_keyed)):
+            fn()                                   # warm-up
+            ev, cv = [], []
+            for _ in range(args.iters):
+                t0 = time.perf_counter()
+                d, sc, st, t1 = fn()
+                t2 = time.perf_counter()
+                ev.append(t1 - t0)
+                cv.append(t2 - t1)
+            first = _download(L, d, 0, D)
+            last = _download(L, d, (B - 1) * D, D)
+            res[name] = {"eval_ms": 1e3 * float(np.median(ev)),
+                         "convert_ms": 1e3 * float(np.median(cv)),
+                         "sums": (sc.copy(), st.copy()), "leaves": (first, last)}
+        base = res["ref"]
+        entry = {}
+        for name, r in res.items():
+            same = all((a == b).all() for a, b in zip(r["sums"], base["sums"])) and \
+                all((a == b).all() for a, b in zip(r["leaves"], base["leaves"]))
+            entry[name] = {"eval_ms": r["eval_ms"], "convert_ms": r["convert_ms"],
+                           "total_ms": r["eval_ms"] + r["convert_ms"],
+                           "leaves_per_s": B * D / ((r["eval_ms"] + r["convert_ms"]) * 1e-3),
+                           "bit_exact_vs_ref": bool(same)}
+        for name in ("drop_in", "keyed"):
+            entry[name]["speedup_vs_ref"] = entry["ref"]["total_ms"] / entry[name]["total_ms"]
+        out[prg_name] = entry
+    print(json.dumps(out), flush=True)
+
+
+def _next(level):
+    v = level[0]
+    level[0] += 1
+    return v
+
+
+def _download(L, d_ptr, first_blk, count):
+    h = np.empty((count, 2), np.uint64)
+    L.lib.pcgb_memcpy_d2h(h.ctypes.data, d_ptr + 16 * first_blk, h.nbytes, None)
+    return h
+
+
+if __name__ == "__main__":
+    main()

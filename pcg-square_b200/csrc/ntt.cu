@@ -223,7 +223,9 @@ __device__ __forceinline__ void inverse_all(uint64_t (&x)[Geo<L>::E], int t,
 
 // Columns per CTA of the column passes.  Adjacent columns ride on adjacent
 // lanes: 128-byte row segments up to n1 = 512, then 64, 32 and 16 bytes so
-// that the CTA stays at 512 threads.  (n2 >= n1 = 2^L, so C never exceeds
+// that the CTA stays at 512 threads.  The column kernels are register-capped
+// for two CTAs per SM (a few spilled words at n1 >= 512), so one CTA's loads
+// overlap the other's butterflies; measured faster than one uncapped CTA.  (n2 >= n1 = 2^L, so C never exceeds
 // the row length.)
 __host__ __device__ constexpr int col_C(int L) {
     return L <= 3 ? (1 << L) : (L <= 9 ? 16 : (L == 10 ? 8 : (L == 11 ? 4 : 2)));
@@ -244,7 +246,7 @@ __host__ __device__ constexpr int row_threads() { return Geo<L>::T * row_V<L>();
 // REDUCE maps arbitrary 64-bit inputs into [0, p) first; otherwise inputs
 // must be below 4p.  Outputs in [0, p).
 template <int L, bool REDUCE>
-__global__ void __launch_bounds__(col_threads<L>()) col_fwd_kernel(
+__global__ void __launch_bounds__(col_threads<L>(), 2) col_fwd_kernel(
     const uint64_t* src, uint64_t* dst, int l2, const ulonglong2* __restrict__ tw,
     const uint64_t* __restrict__ W) {
     constexpr int C = col_C(L), E = Geo<L>::E, LP = last_phase(L);
@@ -270,7 +272,7 @@ __global__ void __launch_bounds__(col_threads<L>()) col_fwd_kernel(
 // Column pass, inverse, in place (output in natural coefficient order, in
 // [0, p)).
 template <int L>
-__global__ void __launch_bounds__(col_threads<L>()) col_inv_kernel(
+__global__ void __launch_bounds__(col_threads<L>(), 2) col_inv_kernel(
     uint64_t* d, int l2, const ulonglong2* __restrict__ twi) {
     constexpr int C = col_C(L), E = Geo<L>::E, LP = last_phase(L);
     extern __shared__ uint64_t sm[];
@@ -473,21 +475,26 @@ constexpr size_t col_smem() { return Geo<L>::NPH > 1 ? sizeof(uint64_t) * Geo<L>
 template <int L>
 constexpr size_t row_smem() { return Geo<L>::NPH > 1 ? sizeof(uint64_t) * Geo<L>::PAD * row_V<L>() : 0; }
 
-// Dynamic shared memory above 48 KB is opted into once per kernel and device.
+// Once per kernel and device: opt into dynamic shared memory above 48 KB and
+// ask for the largest shared-memory carveout, so the CTAs that the register
+// budget admits are not limited by a smaller L1/shared split.
 struct OptinOnce {
     std::mutex mu;
     std::map<std::pair<const void*, int>, bool> done;
     template <class K>
     void operator()(K* kernel, size_t bytes) {
-        if (bytes <= 48 * 1024) return;
+        if (bytes == 0) return;
         int dev = 0;
         PCGB_CK(cudaGetDevice(&dev));
         std::lock_guard<std::mutex> lk(mu);
         auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
         if (done[key]) return;
-        PCGB_CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel),
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(bytes)));
+        const void* f = reinterpret_cast<const void*>(kernel);
+        if (bytes > 48 * 1024)
+            PCGB_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(bytes)));
+        PCGB_CK(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     cudaSharedmemCarveoutMaxShared));
         done[key] = true;
     }
 };

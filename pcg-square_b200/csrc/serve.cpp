@@ -4,7 +4,9 @@
 // the head is admitted as soon as a slot is free and its HBM footprint
 // (keys, noise, outputs and the expansion workspace) fits the memory budget
 // next to everything already in flight, so requests that arrive while others
-// are on the GPU start immediately and their kernels overlap on the device.
+// are on the GPU start immediately and their kernels overlap on the device;
+// small requests run on high-priority streams so that they are not queued
+// behind the CTAs of a large one.
 // Each admitted request runs on its slot's stream: GPU dealer (fresh seeded
 // keys), noise, the fused expansion against the shape's resident plan (a_i
 // images, gather plan, NTT tables), and a device digest of x and z; a host
@@ -63,7 +65,8 @@ struct pcgb_server {
     size_t budget = 0;
     int max_in_flight = 1;
     uint64_t a_seed = 0;
-    std::vector<cudaStream_t> streams;
+    std::vector<cudaStream_t> streams;     // per slot, lowest priority
+    std::vector<cudaStream_t> hi_streams;  // per slot, highest priority (small requests)
     std::vector<pcgb::Req*> slot_req;
     uint64_t* h_digest = nullptr;  // pinned, 2 words per slot
     std::mutex plans_mu;
@@ -133,9 +136,16 @@ void CUDART_CB on_done(void* p) {
     delete ctx;
 }
 
+// Requests with c^2 * N at most this run on their slot's high-priority
+// stream: when a large expansion fills every SM, the block scheduler starts
+// a small request's CTAs ahead of the large kernel's pending ones instead of
+// after them, which is what bounds the small requests' latency in a mix.
+constexpr uint64_t kSmallWork = uint64_t{1} << 20;
+
 // Enqueue one admitted request on its slot's stream (worker thread only).
 void launch(pcgb_server* s, Req* r) {
-    cudaStream_t st = s->streams[r->slot];
+    const uint64_t work = static_cast<uint64_t>(r->r.c) * r->r.c * static_cast<uint64_t>(r->r.N);
+    cudaStream_t st = work <= kSmallWork ? s->hi_streams[r->slot] : s->streams[r->slot];
     pcgb_expander* e = get_plan(s, r->r.N, r->r.c, r->r.t);
     int K = 0, levels = 0, nk = 0;
     size_t wsb = 0;
@@ -255,7 +265,13 @@ pcgb_server* server_create(int n_streams, size_t budget, int max_in_flight, uint
     s->budget = budget;
     s->streams.resize(n_streams);
     s->slot_req.assign(n_streams, nullptr);
-    for (auto& st : s->streams) PCGB_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    int prio_low = 0, prio_high = 0;
+    PCGB_CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    s->hi_streams.resize(n_streams);
+    for (auto& st : s->streams)
+        PCGB_CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_low));
+    for (auto& st : s->hi_streams)
+        PCGB_CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_high));
     PCGB_CK(cudaMallocHost(&s->h_digest, 16 * static_cast<size_t>(n_streams)));
     s->t0 = clk::now();
     s->worker = std::thread(worker_loop, s);
@@ -360,8 +376,10 @@ void server_destroy(pcgb_server* s, int timeout_ms) {
     }
     s->worker.join();
     for (auto& st : s->streams) cudaStreamSynchronize(st);
+    for (auto& st : s->hi_streams) cudaStreamSynchronize(st);
     for (auto& kv : s->plans) expander_destroy(kv.second);
     for (auto& st : s->streams) cudaStreamDestroy(st);
+    for (auto& st : s->hi_streams) cudaStreamDestroy(st);
     cudaFreeHost(s->h_digest);
     delete s;
 }
