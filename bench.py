@@ -127,6 +127,8 @@ def parse():
     ap.add_argument("--no-verify", action="store_true")
     ap.add_argument("--no-polymul", dest="polymul", action="store_false",
                     help="skip the batched 16 x 2^20 poly-mul measurement")
+    ap.add_argument("--no-graph", dest="graph", action="store_false",
+                    help="time direct launches instead of CUDA-graph replays")
     ap.add_argument("--polymul-only", action="store_true",
                     help="only the batched poly-mul measurement (profiler captures)")
     ap.add_argument("--serve-requests", type=int, default=200,
@@ -302,12 +304,28 @@ def run_ours(args, d):
     flush = L.DeviceBuffer(2 * L2_BYTES)
     args_dev = (d_r0.ptr, d_cws.ptr, d_cwo.ptr, d_pos.ptr, d_val.ptr, d_x.ptr, d_z.ptr)
 
+    leaf_tpb = e.autotune()     # leaf-kernel CTA size for this shape (untimed)
     for _ in range(args.warmup):
         e.expand_device(0, *args_dev)
     L.synchronize()
     gops_peak, _ = L.arx_peak()
 
+    # Per-stage device times: a profiled pass of the same steps (direct
+    # launches, events between the stages), not part of the timed region.
     e.set_profiling(args.steps)
+    for i in range(args.steps):
+        L.lib.pcgb_memset(flush.ptr, i & 0xFF, flush.nbytes, None)
+        e.expand_device(0, *args_dev)
+    stages = e.stage_times()
+    e.set_profiling(0)
+    if args.graph:
+        # Timed region replays the expansion as one CUDA graph per step
+        # (first call direct, second captures; both untimed).
+        e.set_graph(True)
+        for _ in range(2):
+            e.expand_device(0, *args_dev)
+    L.synchronize()
+
     evs = [(L.Event(), L.Event()) for _ in range(args.steps)]
     clocks = Clocks(d.local)
     d.barrier()
@@ -323,7 +341,7 @@ def run_ours(args, d):
     launches = L.launch_count() - launches0
     clk = clocks.stop()
     step_ms = [s.elapsed_ms(t) for s, t in evs]
-    stages = e.stage_times()
+    e.set_graph(False)
     total_ms = float(np.sum(step_ms))
     total_ms_max = d.max(total_ms)
     d.barrier()
@@ -432,6 +450,7 @@ def run_ours(args, d):
                        "N": N, "c": C_, "t": T_, "w": W_, "keys": K, "leaves": K * D,
                        "parallelism": f"replicas x{d.world}",
                        "l2": "flushed between timed steps (256 MiB write)",
+                       "cuda_graph": bool(args.graph), "leaf_cta_threads": leaf_tpb,
                        "vs_baseline_ref": "1x L40S serial arm 5.46M corr/s "
                                           "(GPU_baseline/final_l40s/e2e_arms.csv:32)"},
             "stage_ms": dict(zip(["tops", "leaf_gather", "x", "ntt"], stage_means))

@@ -208,8 +208,21 @@ int pcgb_expand_g_device(pcgb_expander* e, int party, const pcgb_blk* d_roots,
  * starts a new recording. */
 int pcgb_expander_set_profiling(pcgb_expander* e, int slots);
 int pcgb_expander_stage_times(pcgb_expander* e, float* ms, int max_expansions);
+/* CUDA graph replay of pcgb_expand_device (no reference counterpart): with
+ * enable != 0 the first expansion runs directly, the next is captured, and
+ * repeated calls with the same pointers, party and stream replay the graph
+ * with one launch; other pointers re-capture and update it.  The stream
+ * must be capturable (not the legacy default stream).  Off by default. */
+int pcgb_expander_set_graph(pcgb_expander* e, int enable);
+/* Times the fused leaf kernel at each CTA size that fits the shape (on zero
+ * keys: its work does not depend on key values), keeps the fastest for this
+ * expander and caches it per device and shape; *tpb_out gets the choice.
+ * Synchronises the library stream.  Server plans are tuned on creation. */
+int pcgb_expander_autotune(pcgb_expander* e, int* tpb_out);
 
-/* Seeded synthetic material (own deterministic generator). */
+/* Seeded synthetic material: a counter-based generator of this library
+ * (SplitMix64 finaliser over seed, domain and index; csrc/synth.h), since the
+ * reference draws noise and public a_i from unseeded emp PRGs. */
 int pcgb_noise(int N, int c, int t, uint64_t seed, int party, uint64_t* pos, uint64_t* val);
 int pcgb_public_a(int N, int c, uint64_t a_seed, uint64_t* a);
 /* Dealer on the GPU: keys for both parties of one expansion. */

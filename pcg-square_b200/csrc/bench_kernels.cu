@@ -43,6 +43,7 @@ __global__ void __launch_bounds__(256) arx_probe_kernel(uint32_t seed, int iters
 }  // namespace
 
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void note_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 

@@ -544,6 +544,21 @@ int pcgb_expander_set_profiling(pcgb_expander* e, int slots) {
     });
 }
 
+int pcgb_expander_set_graph(pcgb_expander* e, int enable) {
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander");
+        pcgb::expander_set_graph(e, enable != 0);
+    });
+}
+
+int pcgb_expander_autotune(pcgb_expander* e, int* tpb_out) {
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander");
+        const int tpb = pcgb::expander_autotune(e);
+        if (tpb_out) *tpb_out = tpb;
+    });
+}
+
 int pcgb_expander_stage_times(pcgb_expander* e, float* ms, int max_expansions) {
     int r = 0;
     const int rc = guarded([&] {

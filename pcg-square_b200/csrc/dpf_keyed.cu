@@ -107,7 +107,7 @@ void keyed_leaf_gather(const GatherPlan& gp, int party, int prg, const Blk* F, c
     LeafLaunch L;
     L.levels = gp.n / gp.w;
     L.bin = static_cast<size_t>(gp.N) / gp.t;
-    int tpb = 256;
+    int tpb = gp.tpb > 0 ? gp.tpb : 256;
     while (tpb > 1 && static_cast<size_t>(tpb) * gp.S > L.bin) tpb >>= 1;
     if (static_cast<size_t>(tpb) * gp.S > L.bin) fail(PCGB_EINVAL, "bin smaller than one tile");
     L.tpb = tpb;

@@ -13,6 +13,11 @@
 // produced (a_i a_j = a_j a_i), so only c(c+1)/2 forward transforms run.
 #include "pcgb_internal.h"
 
+#include <array>
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -127,6 +132,14 @@ struct pcgb_expander {
     size_t scratch_bytes = 0;
     std::vector<cudaEvent_t> prof_ev;  // 5 per slot
     int prof_slots = 0, prof_used = 0;
+    // CUDA graph of expand_device on the expander's own workspace.
+    bool use_graph = false;
+    bool graph_warm = false;
+    cudaGraphExec_t graph_exec = nullptr;
+    unsigned long long graph_kernels = 0;
+    std::array<const void*, 7> graph_key{};
+    int graph_party = -1;
+    cudaStream_t graph_stream = nullptr;
     // host staging for pcgb_expand_host
     void* h_stage = nullptr;
     size_t h_stage_bytes = 0;
@@ -211,6 +224,7 @@ void expander_destroy(pcgb_expander* e) {
     cudaFree(e->d_in);
     if (e->h_stage) cudaFreeHost(e->h_stage);
     for (auto& ev : e->prof_ev) cudaEventDestroy(ev);
+    if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
     cudaSetDevice(cur);
     delete e;
 }
@@ -265,6 +279,11 @@ void ensure_own_workspace(pcgb_expander* e) {
     e->d_g = ws.g;
 }
 
+// With graphs on, the first call runs directly (plans, tables and kernel
+// attributes are set up lazily there), the second captures the launch
+// sequence into a CUDA graph, and later calls with the same pointers, party
+// and stream replay it with one cudaGraphLaunch.  New pointers re-capture
+// and update the executable graph in place.  Profiling slots bypass graphs.
 void expand_device(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
                    const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val, uint64_t* x,
                    uint64_t* z, cudaStream_t st) {
@@ -273,7 +292,138 @@ void expand_device(pcgb_expander* e, int party, const Blk* roots, const Blk* cws
     ws.F = e->d_F;
     ws.tops = e->d_tops;
     ws.g = e->d_g;
-    expand_device_ws(e, ws, party, roots, cws, cw_out, pos, val, x, z, st);
+    const bool profiling = e->prof_slots > 0 && e->prof_used < e->prof_slots;
+    if (!e->use_graph || profiling || !e->graph_warm) {
+        expand_device_ws(e, ws, party, roots, cws, cw_out, pos, val, x, z, st);
+        e->graph_warm = true;
+        return;
+    }
+    const std::array<const void*, 7> key{roots, cws, cw_out, pos, val, x, z};
+    if (e->graph_exec && key == e->graph_key && party == e->graph_party && st == e->graph_stream) {
+        PCGB_CK(cudaGraphLaunch(e->graph_exec, st));
+        note_launches(e->graph_kernels);
+        return;
+    }
+    cudaGraph_t graph = nullptr;
+    PCGB_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+        expand_device_ws(e, ws, party, roots, cws, cw_out, pos, val, x, z, st);
+    } catch (...) {
+        cudaStreamEndCapture(st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        throw;
+    }
+    PCGB_CK(cudaStreamEndCapture(st, &graph));
+    size_t n_nodes = 0;
+    PCGB_CK(cudaGraphGetNodes(graph, nullptr, &n_nodes));
+    std::vector<cudaGraphNode_t> nodes(n_nodes);
+    PCGB_CK(cudaGraphGetNodes(graph, nodes.data(), &n_nodes));
+    unsigned long long kernels = 0;
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType ty;
+        PCGB_CK(cudaGraphNodeGetType(nd, &ty));
+        if (ty == cudaGraphNodeTypeKernel) ++kernels;
+    }
+    if (e->graph_exec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(e->graph_exec, graph, &info) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(e->graph_exec);
+            e->graph_exec = nullptr;
+        }
+    }
+    if (!e->graph_exec) {
+        const cudaError_t rc = cudaGraphInstantiate(&e->graph_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        PCGB_CK(rc);
+    } else {
+        cudaGraphDestroy(graph);
+    }
+    e->graph_key = key;
+    e->graph_party = party;
+    e->graph_stream = st;
+    e->graph_kernels = kernels;
+    // The captured launches were counted once as they were recorded; this
+    // launch is their one execution.
+    PCGB_CK(cudaGraphLaunch(e->graph_exec, st));
+}
+
+void expander_set_graph(pcgb_expander* e, bool on) {
+    if (!on && e->graph_exec) {
+        PCGB_CK(cudaStreamSynchronize(e->graph_stream ? e->graph_stream : default_stream()));
+        cudaGraphExecDestroy(e->graph_exec);
+        e->graph_exec = nullptr;
+    }
+    e->use_graph = on;
+}
+
+// Leaf-kernel CTA size: time each candidate on this shape (the kernel's work
+// does not depend on key values, so zero keys serve) and keep the fastest.
+// Results are cached per device and shape; later expanders of the shape
+// reuse them without timing.
+int expander_autotune(pcgb_expander* e) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, int, int, int>, int> cache;
+    const auto key = std::make_tuple(e->dev, e->N, e->c, e->t, e->w, e->prg);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            e->gp.tpb = it->second;
+            return it->second;
+        }
+    }
+    cudaStream_t st = default_stream();
+    const size_t K = e->K;
+    const size_t b_roots = K * sizeof(Blk), b_cws = K * e->levels * e->nk * sizeof(Blk);
+    const size_t b_keys = (b_roots + b_cws + 8 * K + 255) & ~static_cast<size_t>(255);
+    // A scratch workspace from the pool (server plans own none).
+    char* d = static_cast<char*>(pool_alloc(b_keys + e->scratch_bytes, st));
+    PCGB_CK(cudaMemsetAsync(d, 0, b_roots + b_cws + 8 * K, st));
+    const Workspace ws = workspace_carve(e, d + b_keys);
+    const Blk* roots = reinterpret_cast<const Blk*>(d);
+    const Blk* cws = reinterpret_cast<const Blk*>(d + b_roots);
+    const uint64_t* cwo = reinterpret_cast<const uint64_t*>(d + b_roots + b_cws);
+    keyed_expand_tops(e->K, e->n, e->w, e->prg, roots, cws, e->d_rk, e->gp.hl, ws.F, ws.tops, st);
+    const size_t bin = static_cast<size_t>(e->N) / e->t;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PCGB_CK(cudaEventCreate(&e0));
+    PCGB_CK(cudaEventCreate(&e1));
+    int best = 0;
+    float best_ms = 0;
+    try {
+        for (int tpb : {256, 128, 64, 32}) {
+            if (static_cast<size_t>(tpb) * e->gp.S > bin) continue;
+            e->gp.tpb = tpb;
+            keyed_leaf_gather(e->gp, 0, e->prg, ws.F, cws, cwo, e->d_rk, ws.g, st);  // warm
+            float ms = 0;
+            for (int rep = 0; rep < 3; ++rep) {
+                PCGB_CK(cudaEventRecord(e0, st));
+                keyed_leaf_gather(e->gp, 0, e->prg, ws.F, cws, cwo, e->d_rk, ws.g, st);
+                PCGB_CK(cudaEventRecord(e1, st));
+                PCGB_CK(cudaEventSynchronize(e1));
+                float t = 0;
+                PCGB_CK(cudaEventElapsedTime(&t, e0, e1));
+                ms = rep == 0 ? t : std::min(ms, t);
+            }
+            if (best == 0 || ms < best_ms) { best = tpb; best_ms = ms; }
+        }
+    } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaFreeAsync(d, st);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    PCGB_CK(cudaFreeAsync(d, st));
+    PCGB_CK(cudaStreamSynchronize(st));
+    if (best == 0) best = 32;
+    e->gp.tpb = best;
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = best;
+    return best;
 }
 
 void expand_host(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,

@@ -38,6 +38,7 @@ void check_cuda(cudaError_t e, const char* what);
 // Every kernel launch of the library is followed by PCGB_POST_LAUNCH(): it
 // checks the launch and counts it (pcgb_launch_count).
 void note_launch();
+void note_launches(unsigned long long n);   // kernels replayed from a CUDA graph
 #define PCGB_POST_LAUNCH()                                   \
     do {                                                     \
         ::pcgb::check_cuda(cudaGetLastError(), "kernel launch"); \
@@ -81,6 +82,7 @@ struct GatherPlan {
     int sl = 0;          // levels expanded per thread in the leaf kernel
     int S = 0;           // leaves per thread = m^sl
     int hl = 0;          // frontier level = levels - sl
+    int tpb = 0;         // leaf-kernel threads per CTA (0 = 256, halved to fit a bin)
     uint32_t* d_off = nullptr;      // [Q*t + 1]
     uint32_t* d_entries = nullptr;  // key_id << 2 | half << 1 | fold_negate
     uint16_t* d_qorder = nullptr;   // launch order of the pairs (heavy first)
@@ -141,6 +143,8 @@ pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64
                                const uint8_t* master_key);
 void expander_destroy(pcgb_expander* e);
 void expander_info(const pcgb_expander* e, int* K, int* levels, int* nk, size_t* scratch);
+int expander_autotune(pcgb_expander* e);          // leaf CTA size, cached per shape
+void expander_set_graph(pcgb_expander* e, bool on);
 size_t workspace_bytes(const pcgb_expander* e);
 Workspace workspace_carve(const pcgb_expander* e, void* base);
 void expand_device_ws(pcgb_expander* e, const Workspace& ws, int party, const Blk* roots,

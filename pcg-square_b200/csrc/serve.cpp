@@ -108,6 +108,12 @@ pcgb_expander* get_plan(pcgb_server* s, int N, int c, int t) {
     std::vector<uint64_t> a(static_cast<size_t>(c > 1 ? c - 1 : 1) * N);
     public_a_host(N, c, s->a_seed, a.data());
     pcgb_expander* e = expander_create(N, c, t, 1, PCGB_PRG_CHACHA8, a.data(), nullptr);
+    try {
+        expander_autotune(e);
+    } catch (...) {
+        expander_destroy(e);
+        throw;
+    }
     s->plans[key] = e;
     return e;
 }

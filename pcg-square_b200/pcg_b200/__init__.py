@@ -101,6 +101,8 @@ def _load():
         "pcgb_expand_host": ([_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
         "pcgb_expand_g_device": ([_vp, C.c_int, _vp, _vp, _vp, _vp, _vp], C.c_int),
         "pcgb_expander_set_profiling": ([_vp, C.c_int], C.c_int),
+        "pcgb_expander_set_graph": ([_vp, C.c_int], C.c_int),
+        "pcgb_expander_autotune": ([_vp, C.POINTER(C.c_int)], C.c_int),
         "pcgb_expander_stage_times": ([_vp, C.POINTER(C.c_float), C.c_int], C.c_int),
         "pcgb_launch_count": ([], C.c_ulonglong),
         "pcgb_arx_peak": ([C.POINTER(C.c_double), C.POINTER(C.c_float)], C.c_int),
@@ -475,6 +477,16 @@ class Expander:
     def deal_keys_device(self, seed, d_roots0, d_roots1, d_cws, d_cw_out, stream=None):
         _check(lib.pcgb_deal_keys_device(self.h, seed, d_roots0, d_roots1, d_cws, d_cw_out,
                                          stream))
+
+    def set_graph(self, enable=True):
+        """Replay expand_device as a CUDA graph (see pcgb_expander_set_graph)."""
+        _check(lib.pcgb_expander_set_graph(self.h, 1 if enable else 0))
+
+    def autotune(self):
+        """Pick the fused leaf kernel's CTA size for this shape; returns it."""
+        v = C.c_int()
+        _check(lib.pcgb_expander_autotune(self.h, C.byref(v)))
+        return v.value
 
     def set_profiling(self, slots):
         """Record per-stage events for the next `slots` expansions (0 = off)."""
