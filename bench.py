@@ -492,6 +492,40 @@ def run_polymul(L, batch=16, logN=20, steps=10, warmup=3, seed=11):
            "roofline": {"bound": "hbm", "achieved": nbytes / (med * 1e-3) / 1e9,
                         "peak": hbm_peak(), "unit": "GB/s", "bytes": nbytes}}
     out["roofline"]["frac"] = out["roofline"]["achieved"] / out["roofline"]["peak"]
+
+    # Mixed lengths in one call (five launches for the batch): 6 x 2^20,
+    # 5 x 2^18, 5 x 2^16, interleaved, through pcgb_poly_mul_device_multi.
+    import ctypes as C
+    sizes = [1 << 20, 1 << 16, 1 << 18] * 5 + [1 << 20]
+    bufs = [(L.to_device(rng.integers(0, L.P, n, dtype=np.uint64)),
+             L.to_device(rng.integers(0, L.P, n, dtype=np.uint64)), L.DeviceBuffer(8 * n))
+            for n in sizes]
+    arr = lambda k: (C.c_void_p * len(sizes))(*[bb[k].ptr for bb in bufs])
+    pa, pb, pc, pn = arr(0), arr(1), arr(2), (C.c_int * len(sizes))(*sizes)
+
+    def multi():
+        rc = L.lib.pcgb_poly_mul_device_multi(len(sizes), pc, pa, pb, pn, None)
+        if rc:
+            raise RuntimeError(L.lib.pcgb_last_error().decode())
+
+    for _ in range(warmup):
+        multi()
+    L.synchronize()
+    l0 = L.launch_count()
+    multi()
+    L.synchronize()
+    launches = L.launch_count() - l0
+    for s0, s1 in evs:
+        s0.record()
+        multi()
+        s1.record()
+    L.synchronize()
+    mm = float(np.median([s0.elapsed_ms(s1) for s0, s1 in evs]))
+    mbytes = 24 * sum(sizes)
+    out["mixed"] = {"workload": "16 products: 6 x 2^20, 5 x 2^18, 5 x 2^16 in one call",
+                    "ms_median": mm, "launches_per_call": int(launches),
+                    "achieved_gbs": mbytes / (mm * 1e-3) / 1e9,
+                    "frac_hbm": mbytes / (mm * 1e-3) / 1e9 / hbm_peak()}
     return out
 
 

@@ -169,7 +169,10 @@ int pcgb_dpf_keyed_full_eval(int K, int n, int w, int prg, const pcgb_blk* d_roo
 int pcgb_poly_mul_device(uint64_t* d_c, const uint64_t* d_a, const uint64_t* d_b, int batch,
                          int N, void* stream);
 /* Uneven batch: polys of different lengths in one call; d_a[i], d_b[i],
- * d_c[i] each of length N[i]. */
+ * d_c[i] each of length N[i]; d_c[i] may alias d_a[i] or d_b[i].  When every
+ * N[i] is in 2^16 .. 2^20 the whole batch runs as five launches (one per
+ * pass, each CTA reading its polynomial and tile from a job table); other
+ * lengths run one product at a time. */
 int pcgb_poly_mul_device_multi(int count, uint64_t* const* d_c, const uint64_t* const* d_a,
                                const uint64_t* const* d_b, const int* N, void* stream);
 

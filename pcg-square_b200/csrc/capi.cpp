@@ -467,18 +467,28 @@ int pcgb_poly_mul_device(uint64_t* d_c, const uint64_t* d_a, const uint64_t* d_b
 int pcgb_poly_mul_device_multi(int count, uint64_t* const* d_c, const uint64_t* const* d_a,
                                const uint64_t* const* d_b, const int* N, void* stream) {
     return guarded([&] {
+        if (count < 0 || (count > 0 && (!d_c || !d_a || !d_b || !N)))
+            pcgb::fail(PCGB_EINVAL, "multi poly-mul: bad arguments");
         cudaStream_t st = pcgb::as_stream(stream);
-        // Group equal lengths that sit back to back so each group is one launch set.
-        int i = 0;
-        while (i < count) {
+        std::vector<int> logN(count);
+        bool mixed = count > 0;
+        for (int i = 0; i < count; ++i) {
             if (!pcgb::pow2(N[i]) || N[i] < 2 || N[i] > (1 << pcgb::kMaxLogN))
                 pcgb::fail(PCGB_EINVAL, "N must be a power of two in [2, 2^24]");
-            const pcgb::NttPlan& pl = pcgb::ntt_plan(pcgb::ilog2i(N[i]));
-            uint64_t* scratch = nullptr;
-            scratch = static_cast<uint64_t*>(pcgb::pool_alloc(static_cast<size_t>(N[i]) * sizeof(uint64_t), st));
+            logN[i] = pcgb::ilog2i(N[i]);
+            mixed = mixed && pcgb::poly_mul_mixed_ok(logN[i]);
+        }
+        if (mixed) {
+            // Lengths 2^16 .. 2^20 in any mix: one launch per pass for the batch.
+            pcgb::poly_mul_device_mixed(count, d_c, d_a, d_b, logN.data(), st);
+            return;
+        }
+        for (int i = 0; i < count; ++i) {
+            const pcgb::NttPlan& pl = pcgb::ntt_plan(logN[i]);
+            uint64_t* scratch = static_cast<uint64_t*>(
+                pcgb::pool_alloc(static_cast<size_t>(N[i]) * sizeof(uint64_t), st));
             pcgb::poly_mul_device(pl, d_c[i], d_a[i], d_b[i], 1, scratch, st);
             PCGB_CK(cudaFreeAsync(scratch, st));
-            ++i;
         }
     });
 }

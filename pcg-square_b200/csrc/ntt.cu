@@ -47,6 +47,7 @@
 // 20-kernel four-step (poly_mul_gpuntt_square.cu:171-613).
 #include "pcgb_internal.h"
 
+#include <algorithm>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -241,63 +242,63 @@ __host__ __device__ constexpr int row_V() {
 template <int L>
 __host__ __device__ constexpr int row_threads() { return Geo<L>::T * row_V<L>(); }
 
-// Column pass, forward, then the four-step twiddle.  grid = (n2 / C, batch).
-// src may equal dst (every CTA loads its columns before its first store).
-// REDUCE maps arbitrary 64-bit inputs into [0, p) first; otherwise inputs
-// must be below 4p.  Outputs in [0, p).
-template <int L, bool REDUCE>
-__global__ void __launch_bounds__(col_threads<L>(), 2) col_fwd_kernel(
-    const uint64_t* src, uint64_t* dst, int l2, const ulonglong2* __restrict__ tw,
-    const uint64_t* __restrict__ W) {
-    constexpr int C = col_C(L), E = Geo<L>::E, LP = last_phase(L);
-    extern __shared__ uint64_t sm[];
+// ---- pass bodies ---------------------------------------------------------------
+// Shared by the per-length kernels (one length, batch in gridDim.y) and the
+// mixed-length kernels (a job table names each CTA's polynomial and tile).
+// Pointers arrive already offset to the polynomial's first word.
+
+// Column pass, forward, then the four-step twiddle, for columns
+// [tile*C, tile*C + C).  src may equal dst (every CTA loads its columns
+// before its first store).  REDUCE maps arbitrary 64-bit inputs into [0, p)
+// first; otherwise inputs must be below 4p.  Outputs in [0, p).
+template <int L, int C, bool REDUCE>
+__device__ __forceinline__ void col_fwd_body(const uint64_t* src, uint64_t* dst, int l2,
+                                             size_t tile, const ulonglong2* __restrict__ tw,
+                                             const uint64_t* __restrict__ W, uint64_t* sm) {
+    constexpr int E = Geo<L>::E, LP = last_phase(L);
     const int t = threadIdx.x / C, c = threadIdx.x % C;
     const size_t n2 = size_t{1} << l2;
-    const size_t col = static_cast<size_t>(blockIdx.x) * C + c;
-    const size_t off = static_cast<size_t>(blockIdx.y) * (n2 << L) + col;
+    const size_t col = tile * C + c;
     uint64_t x[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-        const uint64_t v = src[off + eidx<L, 0>(t, e) * n2];
+        const uint64_t v = src[col + eidx<L, 0>(t, e) * n2];
         x[e] = REDUCE ? reduce_p(v) : v;
     }
     forward_all<L>(x, t, tw, SmemLay<C>{sm + c});
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const size_t i = eidx<L, LP>(t, e);
-        dst[off + i * n2] = csub(mont_lazy(x[e], __ldg(W + i * n2 + col)), kPm);
+        dst[col + i * n2] = csub(mont_lazy(x[e], __ldg(W + i * n2 + col)), kPm);
     }
 }
 
 // Column pass, inverse, in place (output in natural coefficient order, in
 // [0, p)).
-template <int L>
-__global__ void __launch_bounds__(col_threads<L>(), 2) col_inv_kernel(
-    uint64_t* d, int l2, const ulonglong2* __restrict__ twi) {
-    constexpr int C = col_C(L), E = Geo<L>::E, LP = last_phase(L);
-    extern __shared__ uint64_t sm[];
+template <int L, int C>
+__device__ __forceinline__ void col_inv_body(uint64_t* d, int l2, size_t tile,
+                                             const ulonglong2* __restrict__ twi, uint64_t* sm) {
+    constexpr int E = Geo<L>::E, LP = last_phase(L);
     const int t = threadIdx.x / C, c = threadIdx.x % C;
     const size_t n2 = size_t{1} << l2;
-    const size_t off = static_cast<size_t>(blockIdx.y) * (n2 << L) +
-                       static_cast<size_t>(blockIdx.x) * C + c;
+    const size_t col = tile * C + c;
     uint64_t x[E];
 #pragma unroll
-    for (int e = 0; e < E; ++e) x[e] = d[off + eidx<L, LP>(t, e) * n2];
+    for (int e = 0; e < E; ++e) x[e] = d[col + eidx<L, LP>(t, e) * n2];
     inverse_all<L>(x, t, twi, SmemLay<C>{sm + c});
 #pragma unroll
-    for (int e = 0; e < E; ++e) d[off + eidx<L, 0>(t, e) * n2] = csub(x[e], kPm);
+    for (int e = 0; e < E; ++e) d[col + eidx<L, 0>(t, e) * n2] = csub(x[e], kPm);
 }
 
-// Row pass, forward, in place (each thread reads and writes the same set of
-// positions); outputs in [0, p) in the permuted order.  grid = (n1 / V, batch).
-template <int L>
-__global__ void __launch_bounds__(row_threads<L>()) row_fwd_kernel(
-    uint64_t* d, int l1, const ulonglong2* __restrict__ tw) {
-    constexpr int E = Geo<L>::E, T = Geo<L>::T, V = row_V<L>(), LP = last_phase(L);
-    extern __shared__ uint64_t sm[];
+// Row pass, forward, in place on rows [tile*V, tile*V + V) (each thread
+// reads and writes the same set of positions); outputs in [0, p) in the
+// permuted order.
+template <int L, int V>
+__device__ __forceinline__ void row_fwd_body(uint64_t* d, size_t tile,
+                                             const ulonglong2* __restrict__ tw, uint64_t* sm) {
+    constexpr int E = Geo<L>::E, T = Geo<L>::T, LP = last_phase(L);
     const int t = threadIdx.x % T, v = threadIdx.x / T;
-    uint64_t* row = d + static_cast<size_t>(blockIdx.y) * (size_t{1} << (L + l1)) +
-                    (static_cast<size_t>(blockIdx.x) * V + v) * Geo<L>::n;
+    uint64_t* row = d + (tile * V + v) * Geo<L>::n;
     uint64_t x[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) x[e] = row[eidx<L, 0>(t, e)];
@@ -307,26 +308,22 @@ __global__ void __launch_bounds__(row_threads<L>()) row_fwd_kernel(
         row[perm_pos<L>(eidx<L, LP>(t, e))] = csub(csub(x[e], k2P), kPm);
 }
 
-// Multiply-accumulate row pass:
+// Multiply-accumulate row pass on rows [tile*V, tile*V + V):
 //   out row = Wi (.) INTT( sum_q NTT(g_q row) (.) img_q row ),
-// img_q in the permuted evaluation order, Montgomery-scaled so that the
-// Montgomery product gives the plain one.  g rows come from the column pass;
-// out is in [0, p) and may alias g (a CTA reads all its rows before its first
-// store).  grid = (n1 / V, batch): instance b reads g and img at b*Q*N and
-// writes out at b*N.
-template <int L>
-__global__ void __launch_bounds__(row_threads<L>()) row_mac_inv_kernel(
-    const uint64_t* g, const uint64_t* __restrict__ img, int Q, int l1,
-    const ulonglong2* __restrict__ tw, const ulonglong2* __restrict__ twi,
-    const uint64_t* __restrict__ Wi, uint64_t* out) {
-    constexpr int E = Geo<L>::E, T = Geo<L>::T, V = row_V<L>(), LP = last_phase(L);
-    extern __shared__ uint64_t sm[];
+// g_q = g + q*N, img_q = img + q*N; img_q in the permuted evaluation order,
+// Montgomery-scaled so that the Montgomery product gives the plain one.
+// g rows come from the column pass; out is in [0, p) and may alias g (a CTA
+// reads all its rows before its first store).
+template <int L, int V>
+__device__ __forceinline__ void row_mac_body(const uint64_t* g, const uint64_t* __restrict__ img,
+                                             int Q, size_t N, size_t tile,
+                                             const ulonglong2* __restrict__ tw,
+                                             const ulonglong2* __restrict__ twi,
+                                             const uint64_t* __restrict__ Wi, uint64_t* out,
+                                             uint64_t* sm) {
+    constexpr int E = Geo<L>::E, T = Geo<L>::T, LP = last_phase(L);
     const int t = threadIdx.x % T, v = threadIdx.x / T;
-    const size_t N = size_t{1} << (L + l1);
-    const size_t base = (static_cast<size_t>(blockIdx.x) * V + v) * Geo<L>::n;
-    g += static_cast<size_t>(blockIdx.y) * Q * N;
-    img += static_cast<size_t>(blockIdx.y) * Q * N;
-    out += static_cast<size_t>(blockIdx.y) * N;
+    const size_t base = (tile * V + v) * Geo<L>::n;
     const SmemLay<1> lay{sm + v * Geo<L>::PAD};
     uint64_t acc[E];
 #pragma unroll
@@ -351,6 +348,138 @@ __global__ void __launch_bounds__(row_threads<L>()) row_mac_inv_kernel(
         out[i] = csub(mont_lazy(acc[e], __ldg(Wi + i)), kPm);
     }
 }
+
+// ---- per-length kernels: grid = (tiles, batch) ---------------------------------
+
+template <int L, bool REDUCE>
+__global__ void __launch_bounds__(col_threads<L>(), 2) col_fwd_kernel(
+    const uint64_t* src, uint64_t* dst, int l2, const ulonglong2* __restrict__ tw,
+    const uint64_t* __restrict__ W) {
+    extern __shared__ uint64_t sm[];
+    const size_t off = static_cast<size_t>(blockIdx.y) << (L + l2);
+    col_fwd_body<L, col_C(L), REDUCE>(src + off, dst + off, l2, blockIdx.x, tw, W, sm);
+}
+
+template <int L>
+__global__ void __launch_bounds__(col_threads<L>(), 2) col_inv_kernel(
+    uint64_t* d, int l2, const ulonglong2* __restrict__ twi) {
+    extern __shared__ uint64_t sm[];
+    col_inv_body<L, col_C(L)>(d + (static_cast<size_t>(blockIdx.y) << (L + l2)), l2, blockIdx.x,
+                              twi, sm);
+}
+
+template <int L>
+__global__ void __launch_bounds__(row_threads<L>()) row_fwd_kernel(
+    uint64_t* d, int l1, const ulonglong2* __restrict__ tw) {
+    extern __shared__ uint64_t sm[];
+    row_fwd_body<L, row_V<L>()>(d + (static_cast<size_t>(blockIdx.y) << (L + l1)), blockIdx.x,
+                                tw, sm);
+}
+
+// Instance b reads g and img at b*Q*N and writes out at b*N.
+template <int L>
+__global__ void __launch_bounds__(row_threads<L>()) row_mac_inv_kernel(
+    const uint64_t* g, const uint64_t* __restrict__ img, int Q, int l1,
+    const ulonglong2* __restrict__ tw, const ulonglong2* __restrict__ twi,
+    const uint64_t* __restrict__ Wi, uint64_t* out) {
+    extern __shared__ uint64_t sm[];
+    const size_t N = size_t{1} << (L + l1);
+    const size_t b = blockIdx.y;
+    row_mac_body<L, row_V<L>()>(g + b * Q * N, img + b * Q * N, Q, N, blockIdx.x, tw, twi, Wi,
+                                out + b * N, sm);
+}
+
+// ---- mixed-length kernels --------------------------------------------------------
+// One launch per pass over a batch of products whose lengths range over
+// 2^16 .. 2^20 (sub-lengths 2^8 .. 2^10 in both passes).  At these lengths
+// every column CTA holds 512 threads x 16 elements (C = 32, 16, 8 columns)
+// and every row CTA 64 threads (V = 4, 2, 1 rows), with the same shared
+// memory, so one launch shape serves every length; each CTA reads its
+// polynomial and tile from a job table and runs that length's body.
+
+struct MixedPoly {
+    const uint64_t* a;
+    const uint64_t* b;
+    uint64_t* c;
+    uint64_t* A;                 // NTT(a), scratch
+    const ulonglong2* tw1;
+    const ulonglong2* tw1i;
+    const ulonglong2* tw2;
+    const ulonglong2* tw2i;
+    const uint64_t* W;
+    const uint64_t* WiR;
+    int l1, l2;
+};
+struct MixedCta {
+    uint32_t poly, tile;
+};
+constexpr int kMixedColThreads = 512, kMixedRowThreads = 64;
+constexpr int kMixedLmin = 8, kMixedLmax = 10;
+template <int L>
+__host__ __device__ constexpr int mixed_C() { return kMixedColThreads / Geo<L>::T; }
+template <int L>
+__host__ __device__ constexpr int mixed_V() { return kMixedRowThreads / Geo<L>::T; }
+static_assert(mixed_V<8>() == row_V<8>() && mixed_V<9>() == row_V<9>() &&
+              mixed_V<10>() == row_V<10>(), "row CTA shapes agree");
+constexpr size_t kMixedColSmem = sizeof(uint64_t) * Geo<10>::PAD * mixed_C<10>();
+constexpr size_t kMixedRowSmem = sizeof(uint64_t) * Geo<10>::PAD * mixed_V<10>();
+static_assert(sizeof(uint64_t) * Geo<8>::PAD * mixed_C<8>() == kMixedColSmem &&
+              sizeof(uint64_t) * Geo<9>::PAD * mixed_C<9>() == kMixedColSmem, "col smem");
+
+#define PCGB_MIXED_SWITCH(LEN, CALL) \
+    switch (LEN) {                    \
+        case 8: CALL(8); break;       \
+        case 9: CALL(9); break;       \
+        case 10: CALL(10); break;     \
+        default: break;               \
+    }
+
+// which = 0: column pass of a into A; which = 1: column pass of b into c.
+__global__ void __launch_bounds__(kMixedColThreads, 2) mixed_col_fwd_kernel(
+    const MixedPoly* __restrict__ polys, const MixedCta* __restrict__ ctas, int which) {
+    extern __shared__ uint64_t sm[];
+    const MixedCta j = ctas[blockIdx.x];
+    const MixedPoly& p = polys[j.poly];
+    const uint64_t* src = which ? p.b : p.a;
+    uint64_t* dst = which ? p.c : p.A;
+#define PCGB_CALL(LL) col_fwd_body<LL, mixed_C<LL>(), true>(src, dst, p.l2, j.tile, p.tw1, p.W, sm)
+    PCGB_MIXED_SWITCH(p.l1, PCGB_CALL)
+#undef PCGB_CALL
+}
+
+__global__ void __launch_bounds__(kMixedRowThreads) mixed_row_fwd_kernel(
+    const MixedPoly* __restrict__ polys, const MixedCta* __restrict__ ctas) {
+    extern __shared__ uint64_t sm[];
+    const MixedCta j = ctas[blockIdx.x];
+    const MixedPoly& p = polys[j.poly];
+#define PCGB_CALL(LL) row_fwd_body<LL, mixed_V<LL>()>(p.A, j.tile, p.tw2, sm)
+    PCGB_MIXED_SWITCH(p.l2, PCGB_CALL)
+#undef PCGB_CALL
+}
+
+// c = Wi*R (.) INTT( NTT_rows(c) (.) A ), in place on c.
+__global__ void __launch_bounds__(kMixedRowThreads) mixed_row_mac_kernel(
+    const MixedPoly* __restrict__ polys, const MixedCta* __restrict__ ctas) {
+    extern __shared__ uint64_t sm[];
+    const MixedCta j = ctas[blockIdx.x];
+    const MixedPoly& p = polys[j.poly];
+    const size_t N = size_t{1} << (p.l1 + p.l2);
+#define PCGB_CALL(LL) \
+    row_mac_body<LL, mixed_V<LL>()>(p.c, p.A, 1, N, j.tile, p.tw2, p.tw2i, p.WiR, p.c, sm)
+    PCGB_MIXED_SWITCH(p.l2, PCGB_CALL)
+#undef PCGB_CALL
+}
+
+__global__ void __launch_bounds__(kMixedColThreads, 2) mixed_col_inv_kernel(
+    const MixedPoly* __restrict__ polys, const MixedCta* __restrict__ ctas) {
+    extern __shared__ uint64_t sm[];
+    const MixedCta j = ctas[blockIdx.x];
+    const MixedPoly& p = polys[j.poly];
+#define PCGB_CALL(LL) col_inv_body<LL, mixed_C<LL>()>(p.c, p.l2, j.tile, p.tw1i, sm)
+    PCGB_MIXED_SWITCH(p.l1, PCGB_CALL)
+#undef PCGB_CALL
+}
+#undef PCGB_MIXED_SWITCH
 
 // Twiddle tables: W[k*n2 + j2] = psi^(j2*(2*brev(k)+1-n1)) (times R), and
 // Wi = psi^-(...) * N^-1 (times R).  powR[b] = psi^(2^b) * R mod p.
@@ -621,6 +750,75 @@ void poly_mul_device(const NttPlan& pl, uint64_t* c, const uint64_t* a, const ui
     col_fwd(pl, b, c, batch, true, st);
     row_mac(pl, c, scratch, 1, batch, wir, c, st);
     col_inv(pl, c, batch, st);
+}
+
+bool poly_mul_mixed_ok(int logN) { return logN >= 2 * kMixedLmin && logN <= 2 * kMixedLmax; }
+
+void poly_mul_device_mixed(int count, uint64_t* const* c, const uint64_t* const* a,
+                           const uint64_t* const* b, const int* logN, cudaStream_t st) {
+    if (count <= 0) return;
+    std::vector<int> order(count);
+    size_t scratch_words = 0;
+    for (int i = 0; i < count; ++i) {
+        if (!poly_mul_mixed_ok(logN[i])) fail(PCGB_EINVAL, "mixed poly-mul: N must be 2^16 .. 2^20");
+        order[i] = i;
+        scratch_words += size_t{1} << logN[i];
+    }
+    // Longest products first, so the last CTAs of each pass are short ones.
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return logN[x] > logN[y]; });
+    std::vector<MixedPoly> polys(count);
+    std::vector<MixedCta> col, row;
+    uint64_t* scratch = static_cast<uint64_t*>(pool_alloc(8 * scratch_words, st));
+    size_t off = 0;
+    for (int k = 0; k < count; ++k) {
+        const int i = order[k];
+        NttPlan& pl = const_cast<NttPlan&>(ntt_plan(logN[i]));
+        MixedPoly& m = polys[k];
+        m.a = a[i]; m.b = b[i]; m.c = c[i]; m.A = scratch + off;
+        m.tw1 = pl.tw1; m.tw1i = pl.tw1i; m.tw2 = pl.tw2; m.tw2i = pl.tw2i;
+        m.W = pl.W; m.WiR = wi_times_r(pl, st);
+        m.l1 = pl.l1; m.l2 = pl.l2;
+        off += pl.N;
+        int C = 0, V = 0;
+        by_len(pl.l1, [&](auto L) {
+            if constexpr (decltype(L)::value >= kMixedLmin && decltype(L)::value <= kMixedLmax)
+                C = mixed_C<decltype(L)::value>();
+        });
+        by_len(pl.l2, [&](auto L) {
+            if constexpr (decltype(L)::value >= kMixedLmin && decltype(L)::value <= kMixedLmax)
+                V = mixed_V<decltype(L)::value>();
+        });
+        for (uint32_t tl = 0; tl < static_cast<uint32_t>(pl.n2 / C); ++tl) col.push_back({uint32_t(k), tl});
+        for (uint32_t tl = 0; tl < static_cast<uint32_t>(pl.n1 / V); ++tl) row.push_back({uint32_t(k), tl});
+    }
+    const size_t b_polys = sizeof(MixedPoly) * polys.size();
+    const size_t b_col = sizeof(MixedCta) * col.size(), b_row = sizeof(MixedCta) * row.size();
+    const size_t o_col = (b_polys + 255) & ~size_t{255};
+    const size_t o_row = (o_col + b_col + 255) & ~size_t{255};
+    char* tab = static_cast<char*>(pool_alloc(o_row + b_row, st));
+    PCGB_CK(cudaMemcpyAsync(tab, polys.data(), b_polys, cudaMemcpyHostToDevice, st));
+    PCGB_CK(cudaMemcpyAsync(tab + o_col, col.data(), b_col, cudaMemcpyHostToDevice, st));
+    PCGB_CK(cudaMemcpyAsync(tab + o_row, row.data(), b_row, cudaMemcpyHostToDevice, st));
+    const MixedPoly* d_polys = reinterpret_cast<const MixedPoly*>(tab);
+    const MixedCta* d_col = reinterpret_cast<const MixedCta*>(tab + o_col);
+    const MixedCta* d_row = reinterpret_cast<const MixedCta*>(tab + o_row);
+    const unsigned n_col = static_cast<unsigned>(col.size()), n_row = static_cast<unsigned>(row.size());
+    g_optin(mixed_col_fwd_kernel, kMixedColSmem);
+    g_optin(mixed_col_inv_kernel, kMixedColSmem);
+    g_optin(mixed_row_fwd_kernel, kMixedRowSmem);
+    g_optin(mixed_row_mac_kernel, kMixedRowSmem);
+    mixed_col_fwd_kernel<<<n_col, kMixedColThreads, kMixedColSmem, st>>>(d_polys, d_col, 0);
+    PCGB_POST_LAUNCH();
+    mixed_row_fwd_kernel<<<n_row, kMixedRowThreads, kMixedRowSmem, st>>>(d_polys, d_row);
+    PCGB_POST_LAUNCH();
+    mixed_col_fwd_kernel<<<n_col, kMixedColThreads, kMixedColSmem, st>>>(d_polys, d_col, 1);
+    PCGB_POST_LAUNCH();
+    mixed_row_mac_kernel<<<n_row, kMixedRowThreads, kMixedRowSmem, st>>>(d_polys, d_row);
+    PCGB_POST_LAUNCH();
+    mixed_col_inv_kernel<<<n_col, kMixedColThreads, kMixedColSmem, st>>>(d_polys, d_col);
+    PCGB_POST_LAUNCH();
+    PCGB_CK(cudaFreeAsync(tab, st));
+    PCGB_CK(cudaFreeAsync(scratch, st));
 }
 
 void ntt_mac_inverse(const NttPlan& pl, uint64_t* g, const uint64_t* img, int Q, uint64_t* acc,

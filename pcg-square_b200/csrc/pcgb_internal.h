@@ -175,6 +175,12 @@ void ntt_forward(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st);
 // uint64 (reduced mod p first).  scratch: batch*N words.
 void poly_mul_device(const NttPlan& pl, uint64_t* c, const uint64_t* a, const uint64_t* b,
                      int batch, uint64_t* scratch, cudaStream_t st);
+// c[i] = a[i] * b[i] mod (X^N_i + 1) for polynomials of different lengths
+// N_i = 2^logN[i] in 2^16 .. 2^20, five launches for the whole batch; c[i]
+// may alias a[i] or b[i]; inputs any uint64.
+bool poly_mul_mixed_ok(int logN);
+void poly_mul_device_mixed(int count, uint64_t* const* c, const uint64_t* const* a,
+                           const uint64_t* const* b, const int* logN, cudaStream_t st);
 // acc = INTT( sum_q img[q] (.) NTT(g[q]) ); g is consumed (transformed in
 // place); img in Montgomery-scaled evaluation layout.
 void ntt_mac_inverse(const NttPlan& pl, uint64_t* g, const uint64_t* img, int Q, uint64_t* acc,

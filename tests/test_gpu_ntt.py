@@ -139,3 +139,51 @@ def test_device_batch_api_uneven(pcg):
     assert rc == 0, pcg.lib.pcgb_last_error()
     for (a, b), (_, _, dc), N in zip(polys, bufs, sizes):
         assert (dc.download(np.uint64, N) == O.poly_mul(a, b, N)).all()
+
+
+def _multi(pcg, outs, As, Bs, sizes):
+    arr = lambda bufs: (C.c_void_p * len(sizes))(*[x.ptr for x in bufs])
+    Ns = (C.c_int * len(sizes))(*sizes)
+    rc = pcg.lib.pcgb_poly_mul_device_multi(len(sizes), arr(outs), arr(As), arr(Bs), Ns, None)
+    assert rc == 0, pcg.lib.pcgb_last_error()
+    pcg.synchronize()
+
+
+def test_mixed_lengths_one_launch_per_pass(pcg):
+    """Lengths 2^16..2^20 in any order and multiplicity, unreduced inputs, one
+    output aliasing its first operand: five launches for the whole batch and
+    every product equal to the single-length path's."""
+    rng = np.random.default_rng(17)
+    sizes = [1 << 17, 1 << 20, 1 << 16, 1 << 19, 1 << 17, 1 << 18]
+    A = [rng.integers(0, 2**64 - 1, N, dtype=np.uint64) for N in sizes]
+    B = [rng.integers(0, 2**64 - 1, N, dtype=np.uint64) for N in sizes]
+    dA, dB = [dev(pcg, a) for a in A], [dev(pcg, b) for b in B]
+    want = []
+    for a, b, N in zip(dA, dB, sizes):
+        out = pcg.DeviceBuffer(8 * N)
+        pcg.poly_mul_device(out.ptr, a.ptr, b.ptr, 1, N)
+        pcg.synchronize()
+        want.append(out.download(np.uint64, N))
+    outs = [pcg.DeviceBuffer(8 * N) for N in sizes]
+    outs[3] = dA[3]                                  # c aliases a
+    _multi(pcg, outs, dA, dB, sizes)                 # plans warm
+    dA[3] = dev(pcg, A[3])
+    outs[3] = dA[3]
+    before = pcg.launch_count()
+    _multi(pcg, outs, dA, dB, sizes)
+    assert pcg.launch_count() - before == 5
+    for o, w, N in zip(outs, want, sizes):
+        assert (o.download(np.uint64, N) == w).all()
+
+
+def test_multi_outside_mixed_range_falls_back(pcg):
+    rng = np.random.default_rng(18)
+    sizes = [1 << 12, 1 << 16, 1 << 21]
+    polys = [(rng.integers(0, P, N, dtype=np.uint64), rng.integers(0, P, N, dtype=np.uint64))
+             for N in sizes]
+    dA = [dev(pcg, a) for a, _ in polys]
+    dB = [dev(pcg, b) for _, b in polys]
+    outs = [pcg.DeviceBuffer(8 * N) for N in sizes]
+    _multi(pcg, outs, dA, dB, sizes)
+    for (a, b), o, N in zip(polys, outs, sizes):
+        assert (o.download(np.uint64, N) == O.poly_mul(a, b, N)).all()
