@@ -347,18 +347,25 @@ def run_ours(args, d):
     d.barrier()
     value = N * args.steps * d.world / (total_ms_max / 1e3)
 
-    # Bit-exactness spot check (untimed): party 1 on the same keys, then the
-    # OLE relation z0 + z1 = x0 * x1 over the whole ring.
+    # Correctness check (untimed): party 1 on the same keys, then the OLE
+    # relation z0 + z1 = x0 * x1 over the whole ring, checked slot by slot on
+    # the device (pcgb_verify_ole_device) and, independently, on the host
+    # through the library's product of x0 and x1.
     verified = None
     if not args.no_verify:
-        x0, z0 = d_x.download(np.uint64, N), d_z.download(np.uint64, N)
         d_pos1, d_val1 = L.to_device(pos1), L.to_device(val1)
-        e.expand_device(1, d_r1.ptr, d_cws.ptr, d_cwo.ptr, d_pos1.ptr, d_val1.ptr, d_x.ptr, d_z.ptr)
-        x1, z1 = d_x.download(np.uint64, N), d_z.download(np.uint64, N)
+        d_x1, d_z1 = L.DeviceBuffer(8 * N), L.DeviceBuffer(8 * N)
+        e.expand_device(1, d_r1.ptr, d_cws.ptr, d_cwo.ptr, d_pos1.ptr, d_val1.ptr, d_x1.ptr,
+                        d_z1.ptr)
+        d_bad = L.DeviceBuffer(8)
+        L.verify_ole_device(N, d_x.ptr, d_z.ptr, d_x1.ptr, d_z1.ptr, d_bad.ptr)
+        bad_slots = int(d_bad.download(np.uint64, 1)[0])
+        x0, z0 = d_x.download(np.uint64, N), d_z.download(np.uint64, N)
+        x1, z1 = d_x1.download(np.uint64, N), d_z1.download(np.uint64, N)
         prod, _ = L.poly_mul_u64_gpuntt(x0, x1, 1, N)
         zs = z0 + z1
         zs = np.where(zs >= np.uint64(L.P), zs - np.uint64(L.P), zs)
-        verified = bool((prod == zs).all())
+        verified = bool((prod == zs).all()) and bad_slots == 0
 
     # e2e through the public host API with pinned buffers.
     e2e = None

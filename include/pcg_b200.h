@@ -223,6 +223,28 @@ int pcgb_expander_set_graph(pcgb_expander* e, int enable);
  * Synchronises the library stream.  Server plans are tuned on creation. */
 int pcgb_expander_autotune(pcgb_expander* e, int* tpb_out);
 
+/* ---- native: consumers of the expansion -------------------------------- */
+/* One party's N Beaver-triple slot shares from its two ring OLEs (x1, z1)
+ * and (x2, z2) of length N (CPU_baseline/pcg_ole_2pc/triple.h:45-110):
+ * party 0 uses a = x1, b = x2, party 1 a = x2, b = x1, c = a*b + z1 + z2 in
+ * Z_p[X]/(X^N+1); d_a, d_b, d_c receive the forward NTTs in the reference's
+ * slot order (slot k = evaluation at psi^(2k+1), CPU_baseline/ntt.h), so
+ * (a0+a1)(b0+b1) = c0+c1 holds slot by slot.  Inputs any uint64. */
+int pcgb_triples_device(int N, int party, const uint64_t* d_x1, const uint64_t* d_z1,
+                        const uint64_t* d_x2, const uint64_t* d_z2, uint64_t* d_a, uint64_t* d_b,
+                        uint64_t* d_c, void* stream);
+/* *d_mismatches (device) = number of NTT slots where x0*x1 != z0+z1, i.e.
+ * 0 iff the two parties' outputs satisfy the OLE relation in R_p
+ * (CPU_baseline/test/pcg_ole_2pc.cpp:199-214).  No host synchronisation. */
+int pcgb_verify_ole_device(int N, const uint64_t* d_x0, const uint64_t* d_z0,
+                           const uint64_t* d_x1, const uint64_t* d_z1,
+                           unsigned long long* d_mismatches, void* stream);
+/* *d_mismatches (device) = number of slots k where (a0+a1)(b0+b1) != c0+c1. */
+int pcgb_verify_triples_device(int N, const uint64_t* d_a0, const uint64_t* d_b0,
+                               const uint64_t* d_c0, const uint64_t* d_a1,
+                               const uint64_t* d_b1, const uint64_t* d_c1,
+                               unsigned long long* d_mismatches, void* stream);
+
 /* Seeded synthetic material: a counter-based generator of this library
  * (SplitMix64 finaliser over seed, domain and index; csrc/synth.h), since the
  * reference draws noise and public a_i from unseeded emp PRGs. */

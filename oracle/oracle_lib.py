@@ -65,6 +65,8 @@ def lib():
                                         u64p, C.c_int]
         L.orc_poly_mul.argtypes = [u64p, u64p, u64p, C.c_int, C.c_int]
         L.orc_poly_mul_schoolbook.argtypes = [u64p, u64p, u64p, C.c_int]
+        L.orc_ntt_forward.argtypes = [u64p, C.c_int, C.c_int]
+        L.orc_triples.argtypes = [C.c_int, C.c_int, u64p, u64p, u64p, u64p, u64p, u64p, u64p]
         L.orc_mulmod.argtypes = [C.c_uint64, C.c_uint64]
         L.orc_mulmod.restype = C.c_uint64
         L.orc_rnd.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64]
@@ -201,6 +203,21 @@ def poly_mul(a, b, N):
     return c
 
 
+def ntt_forward(a, N):
+    """Negacyclic forward NTT (slot k = A(psi^(2k+1))) of each length-N row."""
+    x = np.array(a, dtype=np.uint64).reshape(-1).copy()
+    lib().orc_ntt_forward(x, x.size // N, N)
+    return x
+
+
+def triples(N, party, x1, z1, x2, z2):
+    """One party's (a, b, c) Beaver-triple slot shares from two ring OLEs."""
+    arrs = [np.ascontiguousarray(v, np.uint64) for v in (x1, z1, x2, z2)]
+    a, b, c = (np.zeros(N, np.uint64) for _ in range(3))
+    lib().orc_triples(N, party, *arrs, a, b, c)
+    return a, b, c
+
+
 def poly_mul_schoolbook(a, b, N):
     c = np.zeros(N, np.uint64)
     lib().orc_poly_mul_schoolbook(c, np.ascontiguousarray(a, np.uint64),
@@ -267,6 +284,7 @@ def ref_cpu():
         L = C.CDLL(path)
         L.ref_chacha8_keystream.argtypes = [u8p, C.c_uint64, C.c_uint64, u8p, C.c_size_t]
         L.ref_ntt_poly_mul.argtypes = [u64p, u64p, u64p, C.c_int, C.c_int]
+        L.ref_ntt_forward.argtypes = [u64p, C.c_int, C.c_int]
         L.ref_negacyclic_psi.argtypes = [C.c_int]
         L.ref_negacyclic_psi.restype = C.c_uint64
         _ref_cpu = L

@@ -597,6 +597,29 @@ void orc_poly_mul(uint64_t* c, const uint64_t* a, const uint64_t* b, int batch, 
                   b + static_cast<size_t>(k) * N, N);
 }
 
+void orc_ntt_forward(uint64_t* a, int batch, int N) {
+    const NttPlan& pl = plan_for(N);
+    for (int k = 0; k < batch; ++k) {
+        uint64_t* x = a + static_cast<size_t>(k) * N;
+        for (int i = 0; i < N; ++i) x[i] %= P;
+        pl.forward(x);
+    }
+}
+
+// triple.h:72-107: ring triple shares, then NTT slot extraction.
+void orc_triples(int N, int party, const uint64_t* x1, const uint64_t* z1, const uint64_t* x2,
+                 const uint64_t* z2, uint64_t* a, uint64_t* b, uint64_t* c) {
+    const uint64_t* as = party == 0 ? x1 : x2;
+    const uint64_t* bs = party == 0 ? x2 : x1;
+    for (int i = 0; i < N; ++i) { a[i] = as[i] % P; b[i] = bs[i] % P; }
+    poly_mul1(c, a, b, N);                               // poly_mul_backend
+    for (int i = 0; i < N; ++i) c[i] = addm(addm(c[i], z1[i] % P), z2[i] % P);   // poly_add
+    const NttPlan& pl = plan_for(N);
+    pl.forward(a);
+    pl.forward(b);
+    pl.forward(c);
+}
+
 // pcg_ole.h:92-106.
 void orc_poly_mul_schoolbook(uint64_t* c, const uint64_t* a, const uint64_t* b, int N) {
     std::vector<uint64_t> r(N, 0);

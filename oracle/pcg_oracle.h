@@ -99,6 +99,16 @@ void orc_out_scatter_g(const orc_blk* leaves, int B, size_t D, int t, int party,
 void orc_poly_mul(uint64_t* c, const uint64_t* a, const uint64_t* b, int batch, int N);
 /* Schoolbook negacyclic product (pcg_ole.h:92-106), small N only. */
 void orc_poly_mul_schoolbook(uint64_t* c, const uint64_t* a, const uint64_t* b, int N);
+/* In-place negacyclic forward NTT of `batch` polys (inputs reduced mod P):
+ * output k = A(psi^(2k+1)), the order of NTT<P>::forward (ntt.h:140-144). */
+void orc_ntt_forward(uint64_t* a, int batch, int N);
+
+/* ---- Beaver triples from two ring OLEs -----------------------------------
+ * One party's N Z_p triple shares (CPU_baseline/pcg_ole_2pc/triple.h:45-110):
+ * party 0 takes a = x1, b = x2, party 1 a = x2, b = x1; c = a*b + z1 + z2 in
+ * R_p; a, b, c are then forward-NTT'd slot by slot. */
+void orc_triples(int N, int party, const uint64_t* x1, const uint64_t* z1, const uint64_t* x2,
+                 const uint64_t* z2, uint64_t* a, uint64_t* b, uint64_t* c);
 uint64_t orc_mulmod(uint64_t a, uint64_t b);
 
 /* ---- seeded synthetic material + expansion ----------------------------- */

@@ -2,7 +2,7 @@
 // place from the reference tree (see oracle/Makefile).  TEST INFRASTRUCTURE:
 // used only to validate the oracle restatement (tests/) byte for byte.
 //   chacha8.h : CPU_baseline/chacha8.h      (ChaCha8PRG)
-//   ntt.h     : CPU_baseline/ntt.h          (NTT<P>::poly_mul)
+//   ntt.h     : CPU_baseline/ntt.h          (NTT<P>::poly_mul, forward)
 //   ntt_roots : GPU_baseline/common/ntt_roots.h (negacyclic_psi)
 #include <cstdint>
 #include <cstring>
@@ -37,6 +37,18 @@ void ref_ntt_poly_mul(uint64_t* c, const uint64_t* a, const uint64_t* b, int bat
         }
         ntt.poly_mul(fc.data(), fa.data(), fb.data());
         for (int i = 0; i < N; ++i) c[static_cast<size_t>(k) * N + i] = fc[i].val();
+    }
+}
+
+// NTT<P>::forward of `batch` polys in place (inputs reduced by FFp's
+// constructor): the slot order the reference's triple extraction uses.
+void ref_ntt_forward(uint64_t* a, int batch, int N) {
+    NTT<kP> ntt(N);
+    std::vector<FFp<kP>> fa(N);
+    for (int k = 0; k < batch; ++k) {
+        for (int i = 0; i < N; ++i) fa[i] = FFp<kP>(a[static_cast<size_t>(k) * N + i]);
+        ntt.forward(fa.data());
+        for (int i = 0; i < N; ++i) a[static_cast<size_t>(k) * N + i] = fa[i].val();
     }
 }
 

@@ -493,6 +493,34 @@ int pcgb_poly_mul_device_multi(int count, uint64_t* const* d_c, const uint64_t* 
     });
 }
 
+// ---- consumers: triples, relation checks -------------------------------------
+int pcgb_triples_device(int N, int party, const uint64_t* d_x1, const uint64_t* d_z1,
+                        const uint64_t* d_x2, const uint64_t* d_z2, uint64_t* d_a, uint64_t* d_b,
+                        uint64_t* d_c, void* stream) {
+    return guarded([&] {
+        pcgb::triples_device(N, party, d_x1, d_z1, d_x2, d_z2, d_a, d_b, d_c,
+                             pcgb::as_stream(stream));
+    });
+}
+
+int pcgb_verify_ole_device(int N, const uint64_t* d_x0, const uint64_t* d_z0,
+                           const uint64_t* d_x1, const uint64_t* d_z1,
+                           unsigned long long* d_mismatches, void* stream) {
+    return guarded([&] {
+        pcgb::verify_ole_device(N, d_x0, d_z0, d_x1, d_z1, d_mismatches, pcgb::as_stream(stream));
+    });
+}
+
+int pcgb_verify_triples_device(int N, const uint64_t* d_a0, const uint64_t* d_b0,
+                               const uint64_t* d_c0, const uint64_t* d_a1,
+                               const uint64_t* d_b1, const uint64_t* d_c1,
+                               unsigned long long* d_mismatches, void* stream) {
+    return guarded([&] {
+        pcgb::verify_triples_device(N, d_a0, d_b0, d_c0, d_a1, d_b1, d_c1, d_mismatches,
+                                    pcgb::as_stream(stream));
+    });
+}
+
 // ---- expansion --------------------------------------------------------------
 int pcgb_expander_create(pcgb_expander** e, int N, int c, int t, int w, int prg,
                          const uint64_t* public_a, const uint8_t* master_key) {

@@ -536,11 +536,18 @@ uint32_t brev_host(uint32_t x, int bits) {
     return r;
 }
 
+// Smallest primitive root of F_p, as the reference's NTT picks it
+// (CPU_baseline/ntt.h:200-222): p - 1 = 2^25 * 47189 * 2912521, and g is
+// primitive iff g^((p-1)/q) != 1 for each prime q | p - 1.  (It is 3.)  The
+// slot values of a transform, which triples expose, depend on this choice.
 uint64_t primitive_root_host() {
-    // p - 1 = 2^25 * (2^37 - 3); smallest g with g^((p-1)/q) != 1 for q in {2, 2^37-3}.
-    const uint64_t q2 = (kPm - 1) >> 25;
-    for (uint64_t g = 2;; ++g)
-        if (pow_p_host(g, (kPm - 1) / 2) != 1 && pow_p_host(g, (kPm - 1) / q2) != 1) return g;
+    constexpr uint64_t kQ[3] = {2, 47189, 2912521};
+    static_assert((kPm - 1) == (uint64_t{1} << 25) * 47189ULL * 2912521ULL, "p - 1 factors");
+    for (uint64_t g = 2;; ++g) {
+        bool ok = true;
+        for (uint64_t q : kQ) ok = ok && pow_p_host(g, (kPm - 1) / q) != 1;
+        if (ok) return g;
+    }
 }
 
 // Roots of a length-2^logn negacyclic transform with psi_n a primitive
@@ -733,6 +740,17 @@ const NttPlan& ntt_plan(int logN) {
     auto& slot = cache[{dev, logN}];
     if (!slot) slot.reset(build_plan(logN));
     return *slot;
+}
+
+void ntt_forward_from(const NttPlan& pl, const uint64_t* src, uint64_t* dst, int batch,
+                      bool reduce, cudaStream_t st) {
+    col_fwd(pl, src, dst, batch, reduce, st);
+    row_fwd(pl, dst, batch, st);
+}
+
+void ntt_log_sizes(const NttPlan& pl, int* l1, int* l2) {
+    *l1 = pl.l1;
+    *l2 = pl.l2;
 }
 
 void ntt_forward(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {

@@ -171,6 +171,11 @@ const NttPlan& ntt_plan(int logN);   // resident per (device, logN)
 // In-place forward transform of `batch` length-N polys into the internal
 // evaluation layout (coefficients must be < p).
 void ntt_forward(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st);
+// dst = forward transform of src (batch polys, contiguous); reduce maps any
+// uint64 input into [0, p) first, else inputs must be below 4p.
+void ntt_forward_from(const NttPlan& pl, const uint64_t* src, uint64_t* dst, int batch,
+                      bool reduce, cudaStream_t st);
+void ntt_log_sizes(const NttPlan& pl, int* l1, int* l2);   // see ntt_layout.cuh
 // c = a * b mod (X^N+1) for `batch` polys; c may alias a or b; inputs any
 // uint64 (reduced mod p first).  scratch: batch*N words.
 void poly_mul_device(const NttPlan& pl, uint64_t* c, const uint64_t* a, const uint64_t* b,
@@ -190,6 +195,15 @@ void ntt_mac_inverse(const NttPlan& pl, uint64_t* g, const uint64_t* img, int Q,
 void pointwise_mul(uint64_t* c, const uint64_t* a, const uint64_t* b, size_t count, int mode,
                    cudaStream_t st);
 void reduce_mod_p(uint64_t* d, const uint64_t* s, size_t count, cudaStream_t st);
+
+// ---- triples and relation checks (triples.cu) ----------------------------
+void triples_device(int N, int party, const uint64_t* x1, const uint64_t* z1, const uint64_t* x2,
+                    const uint64_t* z2, uint64_t* a, uint64_t* b, uint64_t* c, cudaStream_t st);
+void verify_ole_device(int N, const uint64_t* x0, const uint64_t* z0, const uint64_t* x1,
+                       const uint64_t* z1, unsigned long long* bad, cudaStream_t st);
+void verify_triples_device(int N, const uint64_t* a0, const uint64_t* b0, const uint64_t* c0,
+                           const uint64_t* a1, const uint64_t* b1, const uint64_t* c1,
+                           unsigned long long* bad, cudaStream_t st);
 
 }  // namespace pcgb
 

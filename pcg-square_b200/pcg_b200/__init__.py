@@ -71,6 +71,9 @@ def _load():
         "pcgb_stream_synchronize": ([_vp], C.c_int),
         "pcgb_device_synchronize": ([], C.c_int),
         "pcgb_trim_pool": ([], C.c_int),
+        "pcgb_triples_device": ([C.c_int, C.c_int] + [_vp] * 7 + [_vp], C.c_int),
+        "pcgb_verify_ole_device": ([C.c_int] + [_vp] * 5 + [_vp], C.c_int),
+        "pcgb_verify_triples_device": ([C.c_int] + [_vp] * 7 + [_vp], C.c_int),
         "pcgb_default_stream": ([], _vp),
         "pcgb_dpf_batch_full_eval": ([C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, C.c_int, _vp, _vp,
                                       _vp, C.c_int], C.c_int),
@@ -220,6 +223,21 @@ def to_device(arr):
 
 def synchronize():
     _check(lib.pcgb_device_synchronize())
+
+
+def triples_device(N, party, d_x1, d_z1, d_x2, d_z2, d_a, d_b, d_c, stream=None):
+    """One party's Beaver-triple slot shares from two ring OLEs (device)."""
+    _check(lib.pcgb_triples_device(N, party, d_x1, d_z1, d_x2, d_z2, d_a, d_b, d_c, stream))
+
+
+def verify_ole_device(N, d_x0, d_z0, d_x1, d_z1, d_bad, stream=None):
+    """d_bad (one u64 on the device) := slots where x0*x1 != z0+z1."""
+    _check(lib.pcgb_verify_ole_device(N, d_x0, d_z0, d_x1, d_z1, d_bad, stream))
+
+
+def verify_triples_device(N, d_a0, d_b0, d_c0, d_a1, d_b1, d_c1, d_bad, stream=None):
+    """d_bad (one u64 on the device) := slots where (a0+a1)(b0+b1) != c0+c1."""
+    _check(lib.pcgb_verify_triples_device(N, d_a0, d_b0, d_c0, d_a1, d_b1, d_c1, d_bad, stream))
 
 
 def trim_pool():

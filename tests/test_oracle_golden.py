@@ -123,3 +123,32 @@ def test_ntt_golden_checksums():
     assert int(np.bitwise_xor.reduce(c)) == 0x3969340B039F5D5D
     a, b = naive_inputs(N, batch)
     assert fnv64(O.poly_mul(a, b, N)) == 0x8599DD17BF241164
+
+
+def test_oracle_slot_order_is_the_references():
+    R = O.ref_cpu()
+    if R is None:
+        pytest.skip("oracle/_ref not built")
+    a = np.random.default_rng(3).integers(0, 2**64 - 1, 2 * 512, dtype=np.uint64)
+    want = a.copy()
+    R.ref_ntt_forward(want, 2, 512)
+    assert (O.ntt_forward(a, 512) == want).all()
+
+
+def test_oracle_triples_hold_on_oracle_oles():
+    """Two OLEs from the oracle's expansion at the CPU-runnable shape: the
+    triple.h restatement yields slot shares with (a0+a1)(b0+b1) = c0+c1."""
+    s = O.shape(4096, 2, 4)
+    a = O.public_a(s, 7)
+    oles = []
+    for seed in (11, 12):
+        r0, r1, cws, cwo = O.deal_keys(s, seed)
+        outs = []
+        for party, roots in ((0, r0), (1, r1)):
+            outs.append(O.expand(s, party, roots, cws, cwo, *O.noise(s, seed, party), a, None))
+        oles.append(outs)
+    N, P = 4096, O.P
+    sh = [O.triples(N, party, *oles[0][party], *oles[1][party]) for party in (0, 1)]
+    for k in range(0, N, 97):
+        lhs = (int(sh[0][0][k]) + int(sh[1][0][k])) * (int(sh[0][1][k]) + int(sh[1][1][k])) % P
+        assert lhs == (int(sh[0][2][k]) + int(sh[1][2][k])) % P
