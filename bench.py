@@ -438,6 +438,10 @@ def run_ours(args, d):
         v, sec, desc = cpu_sample(threads, shape=(N, C_, T_))
         cpu = {"value": v, "unit": "corr/s", "cores": threads, "kind": "port",
                "sample": desc, "sample_seconds": sec}
+        # The reference's CPU bench runs one thread per party (its OpenMP
+        # pragma is not compiled in): the same sample on one thread.
+        v1, sec1, desc1 = cpu_sample(1, keys=8, polymuls=2, shape=(N, C_, T_))
+        cpu["one_thread"] = {"value": v1, "cores": 1, "sample": desc1, "sample_seconds": sec1}
 
     serve = None
     if d.world == 1 and args.serve_requests > 0:

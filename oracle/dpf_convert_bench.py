@@ -11,18 +11,21 @@ host the current shares and takes the peer's back.  Here the exchange
 returns peer = my ^ CW, which makes the interactive evaluation equal to the
 keyed one, so three paths compute the same leaves:
 
-  ref      reference dpf_gpu_batch_full_eval_device + dpf_out_sums
-  drop_in  the library's dpf_gpu_batch_full_eval_device + dpf_out_sums,
-           same exchange callback
-  keyed    the library's pcgb_dpf_keyed_full_eval (no exchange) +
-           dpf_out_sums
+  ref      reference dpf_gpu_batch_full_eval_device + dpf_out_sums +
+           dpf_out_scatter_g
+  drop_in  the library's dpf_gpu_batch_full_eval_device + dpf_out_sums +
+           dpf_out_scatter_g, same exchange callback
+  keyed    the library's pcgb_dpf_keyed_full_eval (no exchange) + the same
+           convert calls
 
-Bit-exactness: per-instance sums (C mod p and T) of all B instances and the
-leaves of the first and last instance must agree across the three paths.
+The scatter uses the t = 64 geometry (B = t^2 = 4096 instances, N = t*D/2 =
+2^21), party 0, uniform F_p output CWs.  Bit-exactness: per-instance sums
+(C mod p and T), the whole scattered g, and the leaves of the first and last
+instance must agree across the three paths.
 Times are wall-clock per call with the device synchronised (the interactive
 paths include their per-level host round trips, as the reference's do).
 
-Usage: python oracle/dpf_convert_bench.py [--B 4096] [--n 16] [--iters 3]
+Usage: python oracle/dpf_convert_bench.py [--B 4096] [--n 16] [--w 1] [--iters 3]
 """
 import argparse
 import ctypes as C
@@ -44,6 +47,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--B", type=int, default=4096)
     ap.add_argument("--n", type=int, default=16)
+    ap.add_argument("--w", type=int, default=1)
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--seed", type=int, default=33)
     args = ap.parse_args()
@@ -52,17 +56,22 @@ def main():
     R = O.ref_gpu()
     if R is None:
         raise SystemExit("oracle/_ref/libref_gpu.so not built")
-    B, n, w = args.B, args.n, 1
+    B, n, w = args.B, args.n, args.w
     D, levels, nk = 1 << n, n // w, (1 << w) - 1
+    t = int(round(B ** 0.5))
+    assert t * t == B and n % w == 0
+    N = t * D // 2
     rng = np.random.default_rng(args.seed)
     roots = rng.integers(0, 2**64 - 1, (B, 2), dtype=np.uint64)
-    cws = rng.integers(0, 2**64 - 1, (B, levels * nk, 2), dtype=np.uint64)
+    cws = rng.integers(0, 2**64 - 1, (B, levels, nk, 2), dtype=np.uint64)
+    CW = rng.integers(0, O.P, B, dtype=np.uint64)
     zero_dlt = np.zeros((B * levels * nk, 2), np.uint64)
     d_roots, d_cws = L.to_device(roots), L.to_device(cws)
     d_keyed = L.DeviceBuffer(16 * B * D)
 
     EX = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p)
-    out = {"workload": f"{B} keys x 2^{n} leaves, w={w}, DPF full-domain eval + out_sums",
+    out = {"workload": f"{B} keys x 2^{n} leaves, w={w}, DPF full-domain eval + out_sums + "
+                       f"out_scatter_g (t={t}, N=2^{N.bit_length() - 1})",
            "device": L.device_name(), "iters": args.iters}
 
     for prg_name, prg in (("chacha8", L.PRG_CHACHA8), ("aes", L.PRG_AES)):
@@ -73,7 +82,7 @@ def main():
         def ex(my, peer, count, user):
             m = np.ctypeslib.as_array(C.cast(my, C.POINTER(C.c_uint64)), shape=(count, 2))
             p = np.ctypeslib.as_array(C.cast(peer, C.POINTER(C.c_uint64)), shape=(count, 2))
-            p[:] = m ^ cws[:, level[0]]
+            p[:] = m ^ cws[:, level[0]].reshape(-1, 2)
             level[0] += 1
 
         cb = EX(ex)
@@ -90,17 +99,22 @@ def main():
             t1 = time.perf_counter()
             sc, st = np.zeros(B, np.uint64), np.zeros(B, np.uint64)
             assert R.ref_dpf_out_sums(d.value, B, D, O.P, sc, st) == 0
-            return d.value, sc, st, t1
+            t2 = time.perf_counter()
+            g = np.zeros(N, np.uint64)
+            assert R.ref_dpf_out_scatter_g(d.value, B, D, t, 0, O.P, CW, g, N) == 0
+            return d.value, sc, st, g, t1, t2
 
         def run_drop_in():
             level[0] = 0
-            d = L.dpf_gpu_batch_full_eval_device(B, n, w, roots, zero_dlt, round_keys=rks,
-                                                 exchange=lambda my: my ^ cws[:, _next(level)],
-                                                 prg=prg)
+            d = L.dpf_gpu_batch_full_eval_device(
+                B, n, w, roots, zero_dlt, round_keys=rks,
+                exchange=lambda my: my ^ cws[:, _next(level)].reshape(-1, 2), prg=prg)
             L.synchronize()
             t1 = time.perf_counter()
             sc, st = L.dpf_out_sums(d, B, D)
-            return d, sc, st, t1
+            t2 = time.perf_counter()
+            g = L.dpf_out_scatter_g(d, B, D, t, 0, CW, N)
+            return d, sc, st, g, t1, t2
 
         def run_keyed():
             L.dpf_keyed_full_eval_device(B, n, w, prg, d_roots.ptr, d_cws.ptr, d_keyed.ptr,
@@ -108,29 +122,34 @@ def main():
             L.synchronize()
             t1 = time.perf_counter()
             sc, st = L.dpf_out_sums(d_keyed.ptr, B, D)
-            return d_keyed.ptr, sc, st, t1
+            t2 = time.perf_counter()
+            g = L.dpf_out_scatter_g(d_keyed.ptr, B, D, t, 0, CW, N)
+            return d_keyed.ptr, sc, st, g, t1, t2
 
         res = {}
         for name, fn in (("ref", run_ref), ("drop_in", run_drop_in), ("keyed", run_keyed)):
             fn()                                   # warm-up
-            ev, cv = [], []
+            ev, cv, sv = [], [], []
             for _ in range(args.iters):
                 t0 = time.perf_counter()
-                d, sc, st, t1 = fn()
-                t2 = time.perf_counter()
+                d, sc, st, g, t1, t2 = fn()
+                t3 = time.perf_counter()
                 ev.append(t1 - t0)
                 cv.append(t2 - t1)
+                sv.append(t3 - t2)
             first = _download(L, d, 0, D)
             last = _download(L, d, (B - 1) * D, D)
             res[name] = {"eval_ms": 1e3 * float(np.median(ev)),
                          "convert_ms": 1e3 * float(np.median(cv)),
-                         "sums": (sc.copy(), st.copy()), "leaves": (first, last)}
+                         "scatter_ms": 1e3 * float(np.median(sv)),
+                         "sums": (sc.copy(), st.copy(), g.copy()), "leaves": (first, last)}
         base = res["ref"]
         entry = {}
         for name, r in res.items():
             same = all((a == b).all() for a, b in zip(r["sums"], base["sums"])) and \
                 all((a == b).all() for a, b in zip(r["leaves"], base["leaves"]))
             entry[name] = {"eval_ms": r["eval_ms"], "convert_ms": r["convert_ms"],
+                           "scatter_ms": r["scatter_ms"],
                            "total_ms": r["eval_ms"] + r["convert_ms"],
                            "leaves_per_s": B * D / ((r["eval_ms"] + r["convert_ms"]) * 1e-3),
                            "bit_exact_vs_ref": bool(same)}

@@ -1,12 +1,14 @@
 // Serving loop: continuous batching of PCG-OLE expansion requests on one GPU.
 //
-// A worker thread owns S CUDA streams ("slots").  Requests wait in a FIFO;
-// the head is admitted as soon as a slot is free and its HBM footprint
-// (keys, noise, outputs and the expansion workspace) fits the memory budget
-// next to everything already in flight, so requests that arrive while others
-// are on the GPU start immediately and their kernels overlap on the device;
-// small requests run on high-priority streams so that they are not queued
-// behind the CTAs of a large one.
+// A worker thread owns S slots, each with a low- and a high-priority CUDA
+// stream.  Requests wait in arrival order; one is admitted as soon as a slot
+// is free and its HBM footprint (keys, noise, outputs and the expansion
+// workspace) fits the memory budget next to everything already in flight, so
+// requests that arrive while others are on the GPU start immediately and
+// their kernels overlap on the device.  Large requests (c^2 * N > 2^20) run
+// one at a time on low-priority streams; small ones pass queued large ones
+// and run on high-priority streams, so they are never queued behind a large
+// request's work.
 // Each admitted request runs on its slot's stream: GPU dealer (fresh seeded
 // keys), noise, the fused expansion against the shape's resident plan (a_i
 // images, gather plan, NTT tables), and a device digest of x and z; a host
@@ -37,11 +39,21 @@ namespace {
 
 using clk = std::chrono::steady_clock;
 
+// Requests with c^2 * N above this are "large".  At most one large request
+// is in flight at a time (they run back to back, as one at a time would,
+// instead of slowing each other down by sharing the GPU); small requests
+// take any free slot ahead of queued large ones and run on their slot's
+// high-priority stream, so the block scheduler starts their CTAs ahead of a
+// large kernel's pending ones.  Small requests thus never wait behind a
+// large one, and large ones lose only the SM time the small ones use.
+constexpr uint64_t kSmallWork = uint64_t{1} << 20;
+
 struct Req {
     uint64_t ticket = 0;
     pcgb_request r{};
     int state = 0;  // 0 pending, 1 running, 2 done, 3 failed
     int slot = -1;
+    bool big = false;   // c^2 * N above kSmallWork
     size_t bytes = 0;
     double submit_s = 0, start_s = 0, done_s = 0;
     uint64_t dx = 0, dz = 0;
@@ -78,6 +90,7 @@ struct pcgb_server {
     std::unordered_map<uint64_t, std::unique_ptr<pcgb::Req>> reqs;
     size_t in_flight_bytes = 0;
     int in_flight = 0;
+    int big_in_flight = 0;
     uint64_t next_ticket = 1;
     bool stopping = false;
     std::thread worker;
@@ -142,16 +155,9 @@ void CUDART_CB on_done(void* p) {
     delete ctx;
 }
 
-// Requests with c^2 * N at most this run on their slot's high-priority
-// stream: when a large expansion fills every SM, the block scheduler starts
-// a small request's CTAs ahead of the large kernel's pending ones instead of
-// after them, which is what bounds the small requests' latency in a mix.
-constexpr uint64_t kSmallWork = uint64_t{1} << 20;
-
 // Enqueue one admitted request on its slot's stream (worker thread only).
 void launch(pcgb_server* s, Req* r) {
-    const uint64_t work = static_cast<uint64_t>(r->r.c) * r->r.c * static_cast<uint64_t>(r->r.N);
-    cudaStream_t st = work <= kSmallWork ? s->hi_streams[r->slot] : s->streams[r->slot];
+    cudaStream_t st = r->big ? s->streams[r->slot] : s->hi_streams[r->slot];
     pcgb_expander* e = get_plan(s, r->r.N, r->r.c, r->r.t);
     int K = 0, levels = 0, nk = 0;
     size_t wsb = 0;
@@ -185,6 +191,23 @@ void launch(pcgb_server* s, Req* r) {
     PCGB_CK(cudaLaunchHostFunc(st, on_done, new CallbackCtx{s, r}));
 }
 
+// The request to admit next, or pending.end(): the first pending request in
+// arrival order that may start now -- a large request is skipped while
+// another large one is in flight, and the candidate's footprint must fit
+// the budget next to what is in flight (one larger than the whole budget
+// still runs alone).  The admission loop and the worker's wait use this same
+// rule, so the wait never holds the lock while an admission is possible.
+std::deque<Req*>::iterator next_admissible(pcgb_server* s) {
+    if (s->in_flight >= s->max_in_flight || s->in_flight >= s->n_slots) return s->pending.end();
+    for (auto it = s->pending.begin(); it != s->pending.end(); ++it) {
+        Req* r = *it;
+        if (r->big && s->big_in_flight > 0) continue;
+        if (s->in_flight > 0 && s->in_flight_bytes + r->bytes > s->budget) return s->pending.end();
+        return it;
+    }
+    return s->pending.end();
+}
+
 void worker_loop(pcgb_server* s) {
     cudaSetDevice(s->dev);
     std::unique_lock<std::mutex> lk(s->mu);
@@ -197,28 +220,28 @@ void worker_loop(pcgb_server* s) {
             s->slot_req[r->slot] = nullptr;
             s->in_flight_bytes -= r->bytes;
             --s->in_flight;
+            s->big_in_flight -= r->big ? 1 : 0;
         }
         if (!s->finished.empty()) {
             s->finished.clear();
             s->cv_done.notify_all();
         }
         if (s->stopping && s->in_flight == 0 && s->pending.empty()) break;
-        // Admissions (FIFO head first; a request larger than the whole
-        // budget still runs when nothing else is in flight).
-        while (!s->pending.empty() && s->in_flight < s->max_in_flight) {
+        // Admissions (next_admissible's rule).
+        for (auto it = next_admissible(s); it != s->pending.end(); it = next_admissible(s)) {
             int slot = -1;
             for (int i = 0; i < s->n_slots; ++i)
                 if (!s->slot_req[i]) { slot = i; break; }
             if (slot < 0) break;
-            Req* r = s->pending.front();
-            if (s->in_flight > 0 && s->in_flight_bytes + r->bytes > s->budget) break;
-            s->pending.pop_front();
+            Req* r = *it;
+            s->pending.erase(it);
             r->slot = slot;
             r->state = 1;
             r->start_s = s->now();
             s->slot_req[slot] = r;
             s->in_flight_bytes += r->bytes;
             ++s->in_flight;
+            s->big_in_flight += r->big ? 1 : 0;
             lk.unlock();
             bool ok = true;
             std::string msg;
@@ -236,19 +259,15 @@ void worker_loop(pcgb_server* s) {
                 s->slot_req[slot] = nullptr;
                 s->in_flight_bytes -= r->bytes;
                 --s->in_flight;
+                s->big_in_flight -= r->big ? 1 : 0;
                 s->cv_done.notify_all();
             }
         }
         // Sleep until something can change: a completion, shutdown, or a
-        // head request that can actually be admitted now (the same rule as
-        // above, footprint included, so the wait never spins while holding
-        // the lock the completion callback needs).
+        // request that can actually be admitted now.
         s->cv_work.wait(lk, [s] {
             if (!s->finished.empty() || (s->stopping && s->in_flight == 0)) return true;
-            if (s->pending.empty() || s->in_flight >= s->max_in_flight ||
-                s->in_flight >= s->n_slots)
-                return false;
-            return s->in_flight == 0 || s->in_flight_bytes + s->pending.front()->bytes <= s->budget;
+            return next_admissible(s) != s->pending.end();
         });
     }
 }
@@ -296,6 +315,7 @@ uint64_t server_submit(pcgb_server* s, const pcgb_request& r) {
     pcgb_expander* e = get_plan(s, r.N, r.c, r.t);
     auto req = std::make_unique<Req>();
     req->r = r;
+    req->big = static_cast<uint64_t>(r.c) * r.c * static_cast<uint64_t>(r.N) > kSmallWork;
     req->bytes = footprint(e, r);
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stopping) fail(PCGB_ESTATE, "server: shutting down");

@@ -91,3 +91,20 @@ def test_failures_are_reported_on_the_host(pcg):
     assert e.value.code == -6
     assert srv.wait(tks[0], timeout_ms=60000).status == 0
     srv.close(timeout_ms=60000)               # cancels or drains the rest
+
+
+def test_large_requests_run_one_at_a_time_and_small_ones_pass(pcg):
+    """Two large requests (c^2 N > 2^20) never overlap; a small one submitted
+    after both starts while the first large one is still running."""
+    srv = pcg.Server(n_streams=4, a_seed=A_SEED)
+    big, small = (1 << 18, 4, 16), (1 << 12, 2, 8)
+    srv.prepare(*big)
+    srv.prepare(*small)
+    t_big = [srv.submit(*big, s) for s in (1, 2)]
+    t_small = srv.submit(*small, 3)
+    rb = [srv.wait(t, timeout_ms=60000) for t in t_big]
+    rs = srv.wait(t_small, timeout_ms=60000)
+    assert all(r.status == 0 for r in rb + [rs])
+    assert rb[1].start_s >= rb[0].done_s - 1e-6
+    assert rs.start_s < rb[0].done_s
+    srv.close()
