@@ -200,6 +200,12 @@ int pcgb_expand_host(pcgb_expander* e, int party, const pcgb_blk* roots, const p
 /* Only the DPF + output-layer stages: the folded, pair-merged g' buffers
  * (Q = c(c+1)/2 of N words, pair order (0,0),(0,1)..(0,c-1),(1,1),..),
  * g'_ij = g_ij + g_ji for i < j.  For parity checks and staged pipelines. */
+/* Step 4 of the expansion (pcg_ole_impl.h:453-484) from output layers a
+ * caller computed itself, e.g. through the interactive drop-ins in a real
+ * two-party run: d_g holds the c*c folded blocks g_ij (N words each, block
+ * i*c + j), d_pos/d_val this party's noise; writes x and z. */
+int pcgb_expand_from_g_device(pcgb_expander* e, const uint64_t* d_g, const uint64_t* d_pos,
+                              const uint64_t* d_val, uint64_t* d_x, uint64_t* d_z, void* stream);
 int pcgb_expand_g_device(pcgb_expander* e, int party, const pcgb_blk* d_roots,
                          const pcgb_blk* d_cws, const uint64_t* d_cw_out, uint64_t* d_g,
                          void* stream);

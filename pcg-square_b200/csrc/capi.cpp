@@ -582,6 +582,14 @@ int pcgb_expander_set_profiling(pcgb_expander* e, int slots) {
     });
 }
 
+int pcgb_expand_from_g_device(pcgb_expander* e, const uint64_t* d_g, const uint64_t* d_pos,
+                              const uint64_t* d_val, uint64_t* d_x, uint64_t* d_z, void* stream) {
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander");
+        pcgb::expand_from_g_device(e, d_g, d_pos, d_val, d_x, d_z, pcgb::as_stream(stream));
+    });
+}
+
 int pcgb_expander_set_graph(pcgb_expander* e, int enable) {
     return guarded([&] {
         if (!e) pcgb::fail(PCGB_EINVAL, "null expander");

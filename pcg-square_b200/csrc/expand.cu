@@ -65,6 +65,21 @@ __global__ void x_kernel(const uint64_t* __restrict__ pos, const uint64_t* __res
 }
 
 // d[i] = mont(s[i], k): multiply by a constant given in Montgomery form.
+// g'_q = g_ij (+ g_ji when i != j) mod p for the Q pairs i <= j, from the
+// c*c per-block output-layer vectors g[(i*c + j)*N ..] (each in [0, p)).
+__global__ void pair_merge_kernel(const uint64_t* __restrict__ g, int c, size_t N,
+                                  uint64_t* __restrict__ gq) {
+    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int q = blockIdx.y;
+    if (idx >= N) return;
+    int i = 0, j = 0, k = q;
+    while (k >= c - i) { k -= c - i; ++i; }
+    j = i + k;
+    uint64_t v = reduce_p(g[static_cast<size_t>(i * c + j) * N + idx]);
+    if (i != j) v = add_p(v, reduce_p(g[static_cast<size_t>(j * c + i) * N + idx]));
+    gq[static_cast<size_t>(q) * N + idx] = v;
+}
+
 __global__ void scale_kernel(uint64_t* d, const uint64_t* s, size_t n, uint64_t k) {
     const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i < n) d[i] = mont_mul(reduce_p(s[i]), k);
@@ -458,6 +473,22 @@ void expand_host(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
     PCGB_CK(cudaMemcpyAsync(x, d_x, b_out, cudaMemcpyDeviceToHost, st));
     PCGB_CK(cudaMemcpyAsync(z, d_z, b_out, cudaMemcpyDeviceToHost, st));
     PCGB_CK(cudaStreamSynchronize(st));
+}
+
+// Step 4 from externally computed output layers (the interactive two-party
+// path): g holds the c*c folded blocks g_ij (pcg_ole_impl.h:453-484 reads
+// them the same way), pos/val this party's noise.
+void expand_from_g_device(pcgb_expander* e, const uint64_t* g, const uint64_t* pos,
+                          const uint64_t* val, uint64_t* x, uint64_t* z, cudaStream_t st) {
+    if (!g || !pos || !val || !x || !z) fail(PCGB_EINVAL, "expand_from_g: null pointer");
+    ensure_own_workspace(e);
+    const size_t NN = static_cast<size_t>(e->N);
+    pair_merge_kernel<<<dim3(blocks_for(NN, 256), e->Q), 256, 0, st>>>(g, e->c, NN, e->d_g);
+    PCGB_POST_LAUNCH();
+    const size_t sm = sizeof(uint64_t) * 2 * static_cast<size_t>(e->c) * e->t;
+    x_kernel<<<blocks_for(NN, 256), 256, sm, st>>>(pos, val, e->d_aR, e->c, e->t, NN, x);
+    PCGB_POST_LAUNCH();
+    ntt_mac_inverse(*e->ntt, e->d_g, e->d_img, e->Q, z, st);
 }
 
 void expand_g_device(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,

@@ -144,6 +144,8 @@ pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64
 void expander_destroy(pcgb_expander* e);
 void expander_info(const pcgb_expander* e, int* K, int* levels, int* nk, size_t* scratch);
 int expander_autotune(pcgb_expander* e);          // leaf CTA size, cached per shape
+void expand_from_g_device(pcgb_expander* e, const uint64_t* g, const uint64_t* pos,
+                          const uint64_t* val, uint64_t* x, uint64_t* z, cudaStream_t st);
 void expander_set_graph(pcgb_expander* e, bool on);
 size_t workspace_bytes(const pcgb_expander* e);
 Workspace workspace_carve(const pcgb_expander* e, void* base);

@@ -105,6 +105,7 @@ def _load():
         "pcgb_expand_g_device": ([_vp, C.c_int, _vp, _vp, _vp, _vp, _vp], C.c_int),
         "pcgb_expander_set_profiling": ([_vp, C.c_int], C.c_int),
         "pcgb_expander_set_graph": ([_vp, C.c_int], C.c_int),
+        "pcgb_expand_from_g_device": ([_vp] * 6 + [_vp], C.c_int),
         "pcgb_expander_autotune": ([_vp, C.POINTER(C.c_int)], C.c_int),
         "pcgb_expander_stage_times": ([_vp, C.POINTER(C.c_float), C.c_int], C.c_int),
         "pcgb_launch_count": ([], C.c_ulonglong),
@@ -197,6 +198,13 @@ class DeviceBuffer:
         arr = np.ascontiguousarray(arr)
         assert arr.nbytes <= self.nbytes
         _check(lib.pcgb_memcpy_h2d(self.ptr, _p(arr), arr.nbytes, None))
+        return self
+
+    def upload_at(self, arr, offset):
+        """Copy a host array into the buffer at byte `offset`."""
+        arr = np.ascontiguousarray(arr)
+        assert offset + arr.nbytes <= self.nbytes
+        _check(lib.pcgb_memcpy_h2d(self.ptr + offset, _p(arr), arr.nbytes, None))
         return self
 
     def download(self, dtype, count):
@@ -495,6 +503,10 @@ class Expander:
     def deal_keys_device(self, seed, d_roots0, d_roots1, d_cws, d_cw_out, stream=None):
         _check(lib.pcgb_deal_keys_device(self.h, seed, d_roots0, d_roots1, d_cws, d_cw_out,
                                          stream))
+
+    def expand_from_g_device(self, d_g, d_pos, d_val, d_x, d_z, stream=None):
+        """Step 4 (x, z) from c*c caller-computed folded blocks g_ij."""
+        _check(lib.pcgb_expand_from_g_device(self.h, d_g, d_pos, d_val, d_x, d_z, stream))
 
     def set_graph(self, enable=True):
         """Replay expand_device as a CUDA graph (see pcgb_expander_set_graph)."""
