@@ -114,6 +114,12 @@ int pcgb_dpf_out_sums(const pcgb_blk* d_leaves, int B, size_t D, uint64_t prime,
 int pcgb_dpf_out_scatter_g(const pcgb_blk* d_leaves, int B, size_t D, int t, int party,
                            uint64_t prime, const uint64_t* CW_host, uint64_t* g_out_host,
                            int N);
+/* Device-pointer form of pcgb_dpf_out_scatter_g (no reference counterpart):
+ * d_cw (B words in [0, p)) already on the device, folded g written to d_g
+ * (N words, every one of them) on `stream`, no host synchronisation; the
+ * prime is this library's p. */
+int pcgb_dpf_out_scatter_g_device(const pcgb_blk* d_leaves, int B, size_t D, int t, int party,
+                                  const uint64_t* d_cw, uint64_t* d_g, int N, void* stream);
 
 /* Allocation-free variant of pcgb_dpf_out_sums, with no counterpart in the
  * reference.  It is for callers that must not allocate device memory

@@ -23,6 +23,8 @@ void dpf_out_sums_host(const Blk* d_leaves, int B, size_t D, uint64_t prime, uin
                        uint64_t* sumT);
 void dpf_out_scatter_host(const Blk* d_leaves, int B, size_t D, int t, int party, uint64_t prime,
                           const uint64_t* CW, uint64_t* g_out, int N);
+void dpf_out_scatter_device(const Blk* d_leaves, int B, size_t D, int t, int party,
+                            const uint64_t* d_cw, uint64_t* d_g, int N, cudaStream_t st);
 void aes_ecb_encrypt_device(const uint8_t* keys, const uint8_t* in, uint8_t* out, int count);
 void dpf_out_sums_noalloc(const Blk* d_leaves, int B, size_t D, uint64_t prime, uint64_t* d_sumC,
                           uint64_t* d_sumT, cudaStream_t st);
@@ -333,6 +335,15 @@ int pcgb_dpf_out_sums(const pcgb_blk* d_leaves, int B, size_t D, uint64_t prime,
     return guarded([&] {
         pcgb::dpf_out_sums_host(reinterpret_cast<const Blk*>(d_leaves), B, D, prime, sumC_host,
                                 sumT_host);
+    });
+}
+
+int pcgb_dpf_out_scatter_g_device(const pcgb_blk* d_leaves, int B, size_t D, int t, int party,
+                                  const uint64_t* d_cw, uint64_t* d_g, int N, void* stream) {
+    if (B <= 0) return PCGB_OK;
+    return guarded([&] {
+        pcgb::dpf_out_scatter_device(reinterpret_cast<const Blk*>(d_leaves), B, D, t, party, d_cw,
+                                     d_g, N, pcgb::as_stream(stream));
     });
 }
 

@@ -278,4 +278,19 @@ void dpf_out_scatter_host(const Blk* d_leaves, int B, size_t D, int t, int party
     PCGB_CK(cudaStreamSynchronize(st));
 }
 
+// Device-pointer form: CWs already on the device (values in [0, p)), g
+// written to the device (every position once, so it needs no clearing).
+void dpf_out_scatter_device(const Blk* d_leaves, int B, size_t D, int t, int party,
+                            const uint64_t* d_cw, uint64_t* d_g, int N, cudaStream_t st) {
+    if (B <= 0) return;
+    check_common(d_leaves, B, D, kP);
+    if (!d_cw || !d_g) fail(PCGB_EINVAL, "dpf_out_scatter_g_device: null pointer");
+    if (t <= 0 || N <= 0) fail(PCGB_EINVAL, "dpf_out_scatter_g_device: t and N must be positive");
+    const size_t bin = D >> 1;
+    const size_t s_max = static_cast<size_t>((B - 1) / t) + t - 1;
+    if ((s_max + 2) * bin > 2 * static_cast<size_t>(N))
+        fail(PCGB_EINVAL, "dpf_out_scatter_g_device: N smaller than the instances' span");
+    out_gather_launch(d_leaves, B, D, t, party, d_cw, d_g, static_cast<size_t>(N), st);
+}
+
 }  // namespace pcgb

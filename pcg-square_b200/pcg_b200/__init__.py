@@ -106,6 +106,8 @@ def _load():
         "pcgb_expander_set_profiling": ([_vp, C.c_int], C.c_int),
         "pcgb_expander_set_graph": ([_vp, C.c_int], C.c_int),
         "pcgb_expand_from_g_device": ([_vp] * 6 + [_vp], C.c_int),
+        "pcgb_dpf_out_scatter_g_device": ([_vp, C.c_int, C.c_size_t, C.c_int, C.c_int, _vp, _vp,
+                                           C.c_int, _vp], C.c_int),
         "pcgb_expander_autotune": ([_vp, C.POINTER(C.c_int)], C.c_int),
         "pcgb_expander_stage_times": ([_vp, C.POINTER(C.c_float), C.c_int], C.c_int),
         "pcgb_launch_count": ([], C.c_ulonglong),
@@ -348,6 +350,11 @@ def dpf_out_sums(d_leaves, B, D, prime=P):
     sc, st = np.zeros(B, np.uint64), np.zeros(B, np.uint64)
     _check(lib.pcgb_dpf_out_sums(d_leaves, B, D, prime, sc, st))
     return sc, st
+
+
+def dpf_out_scatter_g_device(d_leaves, B, D, t, party, d_cw, d_g, N, stream=None):
+    """Folded g of the B instances into device d_g; CWs on the device."""
+    _check(lib.pcgb_dpf_out_scatter_g_device(d_leaves, B, D, t, party, d_cw, d_g, N, stream))
 
 
 def dpf_out_scatter_g(d_leaves, B, D, t, party, CW, N, prime=P):

@@ -13,6 +13,9 @@ run by each party in its own process:
     g_ij = dpf_out_scatter_g(leaves, ..., CW)
   x, z = step 4 over the g_ij (pcgb_expand_from_g_device)
 
+By default all c*c blocks run as one batch (see gen_and_expand), which
+leaves levels + 2 message exchanges per expansion instead of c*c*(levels+2).
+
 The preprocessing the reference draws from OT and boolean circuits
 (DltSft shares, Delta shares, beta shares, Beaver triples; pcg_ole_impl.h:
 100-200) is an input here (`PartyMaterial`); the OT layer itself is outside
@@ -26,7 +29,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import (DeviceBuffer, P, PRG_CHACHA8, dpf_gpu_batch_full_eval_device, dpf_out_sums,
-               dpf_out_scatter_g, to_device)
+               dpf_out_scatter_g_device, synchronize, to_device)
 
 
 @dataclass
@@ -78,44 +81,59 @@ class Channel:
         return t_peer.numpy().view(np.uint64).reshape(mine.shape)
 
 
-def _add(a, b):
-    return [(int(x) + int(y)) % P for x, y in zip(a, b)]
+def _beaver_cw(party, chan, sumC, sumT, beta, r, s, rs):
+    """Output-layer correction words of a batch of instances: <A> =
+    (-1)^party sumT, <B> = (-1)^(1-party) sumC + <beta>, CW = A*B by one
+    Beaver triple per instance (two opens; pcg_ole_impl.h:222-290)."""
+    A = [(P - int(v) % P) % P if party == 1 else int(v) % P for v in sumT]
+    Bsh = [((P - int(v)) % P if party == 0 else int(v)) for v in sumC]
+    Bsh = [(b + int(x)) % P for b, x in zip(Bsh, beta)]
+    n = len(A)
+    de_my = np.array([(a - int(x)) % P for a, x in zip(A, r)] +
+                     [(b - int(x)) % P for b, x in zip(Bsh, s)], np.uint64)
+    de_peer = chan.exchange(de_my)
+    cw_my = np.empty(n, np.uint64)
+    for k in range(n):
+        d = (int(de_my[k]) + int(de_peer[k])) % P
+        e = (int(de_my[n + k]) + int(de_peer[n + k])) % P
+        v = (d * int(s[k]) + e * int(r[k]) + int(rs[k])) % P
+        if party == 0:
+            v = (v + d * e) % P
+        cw_my[k] = v
+    cw_peer = chan.exchange(cw_my)
+    return np.array([(int(a) + int(b)) % P for a, b in zip(cw_my, cw_peer)], np.uint64)
 
 
-def gen_and_expand(party, chan, expander, material, prg=PRG_CHACHA8):
+def gen_and_expand(party, chan, expander, material, prg=PRG_CHACHA8, batched=True):
     """One party's online expansion; returns device buffers (x, z) of N words.
 
     `expander` is this party's pcg_b200.Expander for (N, c, t), w = 1 (its
-    resident a_i images serve step 4)."""
+    resident a_i images serve step 4).  batched=True evaluates the c*c
+    blocks' t*t keys as one batch of c*c*t*t instances -- levels + 2 message
+    exchanges in all -- where the reference runs block by block
+    (c*c*(levels + 2) exchanges; batched=False does the same).  Both parties
+    must use the same mode.  The output layers stay on the device."""
     e = expander
     N, c, t = e.N, e.c, e.t
     B, n = t * t, e.levels
     D = 1 << n
     m = material
     d_g = DeviceBuffer(8 * c * c * N)
-    for blk in range(c * c):
-        ex = (lambda my: chan.exchange(my))
-        d_leaves = dpf_gpu_batch_full_eval_device(B, n, 1, m.roots[blk], m.dltsft[blk],
-                                                  party=party, exchange=ex, prg=prg)
-        sumC, sumT = dpf_out_sums(d_leaves, B, D)
-        A = [(P - int(v) % P) % P if party == 1 else int(v) % P for v in sumT]
-        Bsh = [(P - int(v)) % P if party == 0 else int(v) for v in sumC]
-        Bsh = _add(Bsh, m.beta[blk])
-        de_my = np.array([(a - int(x)) % P for a, x in zip(A, m.r[blk])] +
-                         [(b - int(x)) % P for b, x in zip(Bsh, m.s[blk])], np.uint64)
-        de_peer = chan.exchange(de_my)
-        d = _add(de_my[:B], de_peer[:B])
-        ev = _add(de_my[B:], de_peer[B:])
-        cw_my = []
-        for k in range(B):
-            v = (d[k] * int(m.s[blk][k]) + ev[k] * int(m.r[blk][k]) + int(m.rs[blk][k])) % P
-            if party == 0:
-                v = (v + d[k] * ev[k]) % P
-            cw_my.append(v)
-        cw_my = np.array(cw_my, np.uint64)
-        CW = np.array(_add(cw_my, chan.exchange(cw_my)), np.uint64)
-        g = dpf_out_scatter_g(d_leaves, B, D, t, party, CW, N)
-        d_g.upload_at(g, 8 * blk * N)
+    groups = [list(range(c * c))] if batched else [[blk] for blk in range(c * c)]
+    for blocks in groups:
+        nb = len(blocks)
+        roots = np.ascontiguousarray(np.concatenate([m.roots[b] for b in blocks]))
+        dlt = np.ascontiguousarray(np.concatenate([m.dltsft[b] for b in blocks]))
+        d_leaves = dpf_gpu_batch_full_eval_device(nb * B, n, 1, roots, dlt, party=party,
+                                                  exchange=chan.exchange, prg=prg)
+        sumC, sumT = dpf_out_sums(d_leaves, nb * B, D)
+        cat = lambda a: np.concatenate([a[b] for b in blocks])
+        CW = _beaver_cw(party, chan, sumC, sumT, cat(m.beta), cat(m.r), cat(m.s), cat(m.rs))
+        d_cw = to_device(CW)
+        for k, blk in enumerate(blocks):
+            dpf_out_scatter_g_device(d_leaves + 16 * k * B * D, B, D, t, party,
+                                     d_cw.ptr + 8 * k * B, d_g.ptr + 8 * blk * N, N)
+        synchronize()   # d_leaves is valid until the next DPF call
     d_pos, d_val = to_device(m.pos), to_device(m.val)
     d_x, d_z = DeviceBuffer(8 * N), DeviceBuffer(8 * N)
     e.expand_from_g_device(d_g.ptr, d_pos.ptr, d_val.ptr, d_x.ptr, d_z.ptr)

@@ -64,7 +64,7 @@ def dealer(N, c, t, seed):
                 rs=rs_, a=O.public_a(s, 7))
 
 
-def _party(party, port, N, c, t, mat, q):
+def _party(party, port, N, c, t, mat, q, batched):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     import datetime
     import torch.distributed as dist
@@ -79,7 +79,7 @@ def _party(party, port, N, c, t, mat, q):
             r=mat["r"][party], s=mat["s"][party], rs=mat["rs"][party],
             pos=mat["noise"][party][0], val=mat["noise"][party][1])
         chan = twoparty.Channel(party)
-        d_x, d_z = twoparty.gen_and_expand(party, chan, e, m)
+        d_x, d_z = twoparty.gen_and_expand(party, chan, e, m, batched=batched)
         L.synchronize()
         q.put((party, d_x.download(np.uint64, N), d_z.download(np.uint64, N), chan.messages))
         e.close()
@@ -88,13 +88,15 @@ def _party(party, port, N, c, t, mat, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("N,c,t", [(1 << 12, 2, 4), (1 << 13, 2, 8)])
-def test_two_processes_match_the_fused_expansion(pcg, N, c, t):
+@pytest.mark.parametrize("N,c,t,batched", [(1 << 12, 2, 4, False), (1 << 12, 2, 4, True),
+                                           (1 << 13, 2, 8, True)])
+def test_two_processes_match_the_fused_expansion(pcg, N, c, t, batched):
     mat = dealer(N, c, t, 5150 + N)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_party, args=(p, port, N, c, t, mat, q)) for p in (0, 1)]
+    procs = [ctx.Process(target=_party, args=(p, port, N, c, t, mat, q, batched))
+             for p in (0, 1)]
     for p in procs:
         p.start()
     out = {}
@@ -105,7 +107,8 @@ def test_two_processes_match_the_fused_expansion(pcg, N, c, t):
         p.join(timeout=120)
     assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
     levels = O.shape(N, c, t).n
-    assert out[0][2] == c * c * (levels + 2)          # per-level CW + two Beaver opens
+    # Per-level CW exchanges and two Beaver opens, per block or for all blocks.
+    assert out[0][2] == (levels + 2) * (1 if batched else c * c)
     e = pcg.Expander(N, c, t, 1, pcg.PRG_CHACHA8, public_a=mat["a"])
     K = e.K
     for party in (0, 1):
