@@ -193,6 +193,21 @@ int pcgb_expander_create(pcgb_expander** e, int N, int c, int t, int w, int prg,
 int pcgb_expander_destroy(pcgb_expander* e);
 /* Shape-derived sizes: K keys, levels, nk CWs per level. */
 int pcgb_expander_info(const pcgb_expander* e, int* K, int* levels, int* nk, size_t* scratch_bytes);
+/* A shard of one expansion for multi-GPU runs (no reference counterpart):
+ * the c(c+1)/2 pair blocks (i <= j) are split over `world` expanders,
+ * balanced by work (off-diagonal pairs carry two blocks), and this one
+ * (`rank`) evaluates, writes and transforms only its own, holding only their
+ * a_i a_j images.  Its z is the partial INTT(sum over its pairs); the sum of
+ * all shards' z mod p is the expansion's z (linearity), exact as a uint64
+ * all-reduce for world <= 4 (4(p-1) < 2^64) followed by pcgb_reduce_mod_p.
+ * Every shard's x is the full x.  rank 0 of world 1 is pcgb_expander_create. */
+int pcgb_expander_create_shard(pcgb_expander** e, int N, int c, int t, int w, int prg,
+                               const uint64_t* public_a, const uint8_t* master_key, int rank,
+                               int world);
+int pcgb_expander_shard(const pcgb_expander* e, int* rank, int* world, int* pairs_local,
+                        int* pairs_total);
+/* d[i] = s[i] mod p for any 64-bit words (d may equal s). */
+int pcgb_reduce_mod_p(uint64_t* d, const uint64_t* s, size_t count, void* stream);
 /* One party's expansion from device-resident inputs:
  *   d_roots[K], d_cws[K*levels*nk], d_cw_out[K], d_pos[c*t], d_val[c*t]
  *   -> d_x[N], d_z[N] (x = sum a_i e_i, z = sum_{i,j} a_i a_j g_ij). */

@@ -28,8 +28,6 @@ void dpf_out_scatter_device(const Blk* d_leaves, int B, size_t D, int t, int par
 void aes_ecb_encrypt_device(const uint8_t* keys, const uint8_t* in, uint8_t* out, int count);
 void dpf_out_sums_noalloc(const Blk* d_leaves, int B, size_t D, uint64_t prime, uint64_t* d_sumC,
                           uint64_t* d_sumT, cudaStream_t st);
-pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64_t* public_a,
-                               const uint8_t* master_key);
 void expander_destroy(pcgb_expander* e);
 void expand_device(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
                    const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val, uint64_t* x,
@@ -539,6 +537,31 @@ int pcgb_expander_create(pcgb_expander** e, int N, int c, int t, int w, int prg,
     return guarded([&] {
         if (!e) pcgb::fail(PCGB_EINVAL, "null expander handle");
         *e = pcgb::expander_create(N, c, t, w, prg, public_a, master_key);
+    });
+}
+
+int pcgb_expander_create_shard(pcgb_expander** e, int N, int c, int t, int w, int prg,
+                               const uint64_t* public_a, const uint8_t* master_key, int rank,
+                               int world) {
+    if (e) *e = nullptr;
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander handle");
+        *e = pcgb::expander_create(N, c, t, w, prg, public_a, master_key, rank, world);
+    });
+}
+
+int pcgb_expander_shard(const pcgb_expander* e, int* rank, int* world, int* pairs_local,
+                        int* pairs_total) {
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander");
+        pcgb::expander_shard(e, rank, world, pairs_local, pairs_total);
+    });
+}
+
+int pcgb_reduce_mod_p(uint64_t* d, const uint64_t* s, size_t count, void* stream) {
+    return guarded([&] {
+        if (count && (!d || !s)) pcgb::fail(PCGB_EINVAL, "reduce_mod_p: null pointer");
+        if (count) pcgb::reduce_mod_p(d, s, count, pcgb::as_stream(stream));
     });
 }
 

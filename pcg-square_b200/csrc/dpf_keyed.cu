@@ -35,9 +35,11 @@ void keyed_expand_tops(int K, int n, int w, int prg, const Blk* roots, const Blk
 // (kk+ll)*bin + [0, 2*bin) (pcg_ole_impl.h:435-444), so with s = kk+ll:
 //   s = r     -> first half,  kept;   s = r-1   -> second half, kept;
 //   s = r+t   -> first half,  negated; s = r+t-1 -> second half, negated.
-void gather_plan_build(GatherPlan& gp, int N, int c, int t, int n, int w) {
+void gather_plan_build(GatherPlan& gp, int N, int c, int t, int n, int w, int rank, int world) {
     gather_plan_free(gp);
+    if (world < 1 || rank < 0 || rank >= world) fail(PCGB_EINVAL, "expander: bad shard rank/world");
     gp.N = N; gp.c = c; gp.t = t; gp.n = n; gp.w = w;
+    gp.rank = rank; gp.world = world;
     const int levels = n / w;
     // Leaves per thread: 16 for w in {1,2,4}, 8 for w = 3; fewer when the
     // half domain is smaller.
@@ -81,16 +83,39 @@ void gather_plan_build(GatherPlan& gp, int N, int c, int t, int n, int w) {
     gp.Q = Q;
     gp.n_entries = static_cast<int>(ent.size());
     // Heavy pairs (i != j carry two blocks) first so the tail is short.
-    std::vector<uint16_t> order;
-    for (int q = 0; q < Q; ++q) if ((pair_ij[q] / c) != (pair_ij[q] % c)) order.push_back(q);
-    for (int q = 0; q < Q; ++q) if ((pair_ij[q] / c) == (pair_ij[q] % c)) order.push_back(q);
+    std::vector<int> heavy_first;
+    for (int q = 0; q < Q; ++q) if ((pair_ij[q] / c) != (pair_ij[q] % c)) heavy_first.push_back(q);
+    for (int q = 0; q < Q; ++q) if ((pair_ij[q] / c) == (pair_ij[q] % c)) heavy_first.push_back(q);
+    // Shards: longest-first greedy by block count, ties to the lowest rank.
+    std::vector<int> owner(Q, 0), load(world, 0);
+    for (int q : heavy_first) {
+        const int wgt = (pair_ij[q] / c) != (pair_ij[q] % c) ? 2 : 1;
+        int best = 0;
+        for (int r = 1; r < world; ++r) if (load[r] < load[best]) best = r;
+        owner[q] = best;
+        load[best] += wgt;
+    }
+    gp.shard_pairs.clear();
+    for (int q = 0; q < Q; ++q) if (owner[q] == rank) gp.shard_pairs.push_back(q);
+    gp.Qs = static_cast<int>(gp.shard_pairs.size());
+    std::vector<uint16_t> order, slot;
+    for (int q : heavy_first) {
+        if (owner[q] != rank) continue;
+        order.push_back(static_cast<uint16_t>(q));
+        const auto it = std::find(gp.shard_pairs.begin(), gp.shard_pairs.end(), q);
+        slot.push_back(static_cast<uint16_t>(it - gp.shard_pairs.begin()));
+    }
     PCGB_CK(cudaMalloc(&gp.d_off, off.size() * sizeof(uint32_t)));
     PCGB_CK(cudaMalloc(&gp.d_entries, std::max<size_t>(ent.size(), 1) * sizeof(uint32_t)));
-    PCGB_CK(cudaMalloc(&gp.d_qorder, order.size() * sizeof(uint16_t)));
+    PCGB_CK(cudaMalloc(&gp.d_qorder, std::max<size_t>(order.size(), 1) * sizeof(uint16_t)));
+    PCGB_CK(cudaMalloc(&gp.d_qslot, std::max<size_t>(slot.size(), 1) * sizeof(uint16_t)));
     upload_blocking(gp.d_off, off.data(), off.size() * sizeof(uint32_t));
     if (!ent.empty())
         upload_blocking(gp.d_entries, ent.data(), ent.size() * sizeof(uint32_t));
-    upload_blocking(gp.d_qorder, order.data(), order.size() * sizeof(uint16_t));
+    if (!order.empty()) {
+        upload_blocking(gp.d_qorder, order.data(), order.size() * sizeof(uint16_t));
+        upload_blocking(gp.d_qslot, slot.data(), slot.size() * sizeof(uint16_t));
+    }
     gp.pair_ij = pair_ij;
 }
 
@@ -98,7 +123,8 @@ void gather_plan_free(GatherPlan& gp) {
     if (gp.d_off) cudaFree(gp.d_off);
     if (gp.d_entries) cudaFree(gp.d_entries);
     if (gp.d_qorder) cudaFree(gp.d_qorder);
-    gp.d_off = nullptr; gp.d_entries = nullptr; gp.d_qorder = nullptr;
+    if (gp.d_qslot) cudaFree(gp.d_qslot);
+    gp.d_off = nullptr; gp.d_entries = nullptr; gp.d_qorder = nullptr; gp.d_qslot = nullptr;
 }
 
 void keyed_leaf_gather(const GatherPlan& gp, int party, int prg, const Blk* F, const Blk* cws,
@@ -111,13 +137,14 @@ void keyed_leaf_gather(const GatherPlan& gp, int party, int prg, const Blk* F, c
     while (tpb > 1 && static_cast<size_t>(tpb) * gp.S > L.bin) tpb >>= 1;
     if (static_cast<size_t>(tpb) * gp.S > L.bin) fail(PCGB_EINVAL, "bin smaller than one tile");
     L.tpb = tpb;
+    if (gp.Qs == 0) return;   // a shard with no pairs
     L.grid = dim3(static_cast<unsigned>(L.bin / (static_cast<size_t>(tpb) * gp.S)),
-                  static_cast<unsigned>(gp.t), static_cast<unsigned>(gp.Q));
+                  static_cast<unsigned>(gp.t), static_cast<unsigned>(gp.Qs));
     L.smem = static_cast<size_t>(tpb) * (gp.S + 1) * sizeof(uint64_t) +
              (prg == PCGB_PRG_AES ? keyed_aes_smem_bytes_aes() : 0);
     L.st = st;
     L.F = F; L.cws = cws; L.cw_out = cw_out;
-    L.off = gp.d_off; L.entries = gp.d_entries; L.q_order = gp.d_qorder;
+    L.off = gp.d_off; L.entries = gp.d_entries; L.q_order = gp.d_qorder; L.q_slot = gp.d_qslot;
     L.t = gp.t; L.hl = gp.hl; L.N = gp.N; L.party = party;
     L.rk = d_aes_rk; L.gq = gq;
     if (prg == PCGB_PRG_AES) {

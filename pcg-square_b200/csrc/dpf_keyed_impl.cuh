@@ -257,7 +257,8 @@ template <int W, int SL, int PRG>
 __global__ void __launch_bounds__(256) leaf_gather_kernel(
     const Blk* __restrict__ F, const Blk* __restrict__ cws, const uint64_t* __restrict__ cw_out,
     const uint32_t* __restrict__ off, const uint32_t* __restrict__ entries,
-    const uint16_t* __restrict__ q_order, int t, int levels, int hl, size_t bin, int N,
+    const uint16_t* __restrict__ q_order, const uint16_t* __restrict__ q_slot, int t, int levels,
+    int hl, size_t bin, int N,
     int party, const uint32_t* __restrict__ aes_te, const uint32_t* __restrict__ aes_rk,
     uint64_t* __restrict__ gq) {
     constexpr int M = 1 << W, NK = M - 1;
@@ -269,6 +270,7 @@ __global__ void __launch_bounds__(256) leaf_gather_kernel(
 
     const int r = blockIdx.y;
     const int q = q_order[blockIdx.z];
+    const int slot = q_slot[blockIdx.z];
     const size_t tile = static_cast<size_t>(blockDim.x) * S;
     const size_t o = static_cast<size_t>(blockIdx.x) * tile + static_cast<size_t>(threadIdx.x) * S;
     uint64_t* acc = acc_s + threadIdx.x * STRIDE;
@@ -292,7 +294,7 @@ __global__ void __launch_bounds__(256) leaf_gather_kernel(
     }
     __syncthreads();
     // Coalesced write-out of the CTA's tile.
-    uint64_t* dst = gq + static_cast<size_t>(q) * N + static_cast<size_t>(r) * bin +
+    uint64_t* dst = gq + static_cast<size_t>(slot) * N + static_cast<size_t>(r) * bin +
                     static_cast<size_t>(blockIdx.x) * tile;
     for (size_t e = threadIdx.x; e < tile; e += blockDim.x)
         dst[e] = acc_s[(e / S) * STRIDE + (e % S)];
@@ -402,7 +404,8 @@ void leaf_one(const LeafLaunch& L) {
     if (L.smem > 48 * 1024)
         PCGB_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(L.smem)));
-    kern<<<L.grid, L.tpb, L.smem, L.st>>>(L.F, L.cws, L.cw_out, L.off, L.entries, L.q_order, L.t,
+    kern<<<L.grid, L.tpb, L.smem, L.st>>>(L.F, L.cws, L.cw_out, L.off, L.entries, L.q_order,
+                                         L.q_slot, L.t,
                                          L.levels, L.hl, L.bin, L.N, L.party, L.te, L.rk, L.gq);
     PCGB_POST_LAUNCH();
 }

@@ -165,7 +165,7 @@ struct pcgb_expander {
 namespace pcgb {
 
 pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64_t* public_a,
-                               const uint8_t* master_key) {
+                               const uint8_t* master_key, int rank, int world) {
     if (N < 4 || (N & (N - 1)) || N > (1 << kMaxLogN))
         fail(PCGB_EINVAL, "expander: N must be a power of two in [4, 2^24]");
     if (c < 1 || c > 8) fail(PCGB_EINVAL, "expander: c must be in [1, 8]");
@@ -182,9 +182,10 @@ pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64
         e->levels = n / w; e->nk = (1 << w) - 1; e->K = c * c * t * t; e->Q = c * (c + 1) / 2;
         cudaStream_t st = default_stream();
         e->ntt = &ntt_plan(ilog2(N));
-        gather_plan_build(e->gp, N, c, t, n, w);
+        gather_plan_build(e->gp, N, c, t, n, w, rank, world);
         const size_t NN = static_cast<size_t>(N);
-        PCGB_CK(cudaMalloc(&e->d_img, sizeof(uint64_t) * NN * e->Q));
+        const int Qs = e->gp.Qs;
+        PCGB_CK(cudaMalloc(&e->d_img, sizeof(uint64_t) * NN * std::max(Qs, 1)));
         if (c > 1) PCGB_CK(cudaMalloc(&e->d_aR, sizeof(uint64_t) * NN * (c - 1)));
         // a_i coefficients (Montgomery form) and evaluations.
         std::vector<uint64_t*> ahat(c, nullptr);
@@ -198,16 +199,18 @@ pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64
             PCGB_POST_LAUNCH();
             ntt_forward(*e->ntt, tmp, c - 1, st);
             for (int i = 1; i < c; ++i) ahat[i] = tmp + NN * (i - 1);
-            int q = 0;
-            for (int i = 0; i < c; ++i)
-                for (int j = i; j < c; ++j, ++q)
-                    image_kernel<<<blocks_for(NN, 256), 256, 0, st>>>(
-                        e->d_img + NN * q, i == 0 ? (j == 0 ? nullptr : ahat[j]) : ahat[i],
-                        i == 0 ? nullptr : ahat[j], NN, r2, r3);
-                    PCGB_POST_LAUNCH();
+            // Images of this shard's pairs, in slot order.
+            for (int k = 0; k < Qs; ++k) {
+                const int ij = static_cast<int>(e->gp.pair_ij[e->gp.shard_pairs[k]]);
+                const int i = ij / c, j = ij % c;
+                image_kernel<<<blocks_for(NN, 256), 256, 0, st>>>(
+                    e->d_img + NN * k, i == 0 ? (j == 0 ? nullptr : ahat[j]) : ahat[i],
+                    i == 0 ? nullptr : ahat[j], NN, r2, r3);
+                PCGB_POST_LAUNCH();
+            }
             PCGB_CK(cudaStreamSynchronize(st));
             cudaFree(tmp);
-        } else {
+        } else if (Qs > 0) {
             image_kernel<<<blocks_for(NN, 256), 256, 0, st>>>(e->d_img, nullptr, nullptr, NN, r2, r3);
             PCGB_POST_LAUNCH();
         }
@@ -250,7 +253,8 @@ void expander_destroy(pcgb_expander* e) {
 size_t workspace_bytes(const pcgb_expander* e) {
     const size_t fnodes = static_cast<size_t>(e->K) << (e->w * e->gp.hl);
     const size_t tnodes = keyed_tops_scratch_nodes(e->K, e->w, e->gp.hl);
-    return sizeof(Blk) * (fnodes + tnodes) + sizeof(uint64_t) * static_cast<size_t>(e->N) * e->Q;
+    return sizeof(Blk) * (fnodes + tnodes) +
+           sizeof(uint64_t) * static_cast<size_t>(e->N) * std::max(e->gp.Qs, 1);
 }
 
 Workspace workspace_carve(const pcgb_expander* e, void* base) {
@@ -280,7 +284,8 @@ void expand_device_ws(pcgb_expander* e, const Workspace& ws, int party, const Bl
     x_kernel<<<blocks_for(NN, 256), 256, sm, st>>>(pos, val, e->d_aR, e->c, e->t, NN, x);
     PCGB_POST_LAUNCH();
     if (ev) PCGB_CK(cudaEventRecord(ev[3], st));
-    ntt_mac_inverse(*e->ntt, ws.g, e->d_img, e->Q, z, st);
+    if (e->gp.Qs > 0) ntt_mac_inverse(*e->ntt, ws.g, e->d_img, e->gp.Qs, z, st);
+    else PCGB_CK(cudaMemsetAsync(z, 0, sizeof(uint64_t) * NN, st));   // a shard with no pairs
     if (ev) PCGB_CK(cudaEventRecord(ev[4], st));
 }
 
@@ -379,8 +384,9 @@ void expander_set_graph(pcgb_expander* e, bool on) {
 // reuse them without timing.
 int expander_autotune(pcgb_expander* e) {
     static std::mutex mu;
-    static std::map<std::tuple<int, int, int, int, int, int>, int> cache;
-    const auto key = std::make_tuple(e->dev, e->N, e->c, e->t, e->w, e->prg);
+    static std::map<std::tuple<int, int, int, int, int, int, int>, int> cache;
+    const auto key = std::make_tuple(e->dev, e->N, e->c, e->t, e->w, e->prg,
+                                     e->gp.world * 64 + e->gp.rank);
     {
         std::lock_guard<std::mutex> lk(mu);
         auto it = cache.find(key);
@@ -481,6 +487,7 @@ void expand_host(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
 void expand_from_g_device(pcgb_expander* e, const uint64_t* g, const uint64_t* pos,
                           const uint64_t* val, uint64_t* x, uint64_t* z, cudaStream_t st) {
     if (!g || !pos || !val || !x || !z) fail(PCGB_EINVAL, "expand_from_g: null pointer");
+    if (e->gp.world != 1) fail(PCGB_EINVAL, "expand_from_g: needs an unsharded expander");
     ensure_own_workspace(e);
     const size_t NN = static_cast<size_t>(e->N);
     pair_merge_kernel<<<dim3(blocks_for(NN, 256), e->Q), 256, 0, st>>>(g, e->c, NN, e->d_g);
@@ -537,6 +544,13 @@ void deal_keys_device(pcgb_expander* e, uint64_t seed, Blk* r0, Blk* r1, Blk* cw
 }  // namespace pcgb
 
 namespace pcgb {
+
+void expander_shard(const pcgb_expander* e, int* rank, int* world, int* q_local, int* q_total) {
+    if (rank) *rank = e->gp.rank;
+    if (world) *world = e->gp.world;
+    if (q_local) *q_local = e->gp.Qs;
+    if (q_total) *q_total = e->Q;
+}
 
 void expander_info(const pcgb_expander* e, int* K, int* levels, int* nk, size_t* scratch) {
     if (K) *K = e->K;

@@ -85,11 +85,19 @@ struct GatherPlan {
     int tpb = 0;         // leaf-kernel threads per CTA (0 = 256, halved to fit a bin)
     uint32_t* d_off = nullptr;      // [Q*t + 1]
     uint32_t* d_entries = nullptr;  // key_id << 2 | half << 1 | fold_negate
-    uint16_t* d_qorder = nullptr;   // launch order of the pairs (heavy first)
+    uint16_t* d_qorder = nullptr;   // launch order of this shard's pairs (heavy first)
+    uint16_t* d_qslot = nullptr;    // output slot of each launched pair
     std::vector<uint32_t> pair_ij;  // pair q -> block index i*c + j (i <= j)
+    std::vector<int> shard_pairs;   // pairs of this shard, ascending; slot = index
+    int rank = 0, world = 1;
+    int Qs = 0;                     // pairs of this shard (Q when world = 1)
     int n_entries = 0;
 };
-void gather_plan_build(GatherPlan& gp, int N, int c, int t, int n, int w);
+// A shard (rank of world) owns a subset of the Q pairs, balanced by work
+// (off-diagonal pairs weigh 2 blocks, diagonal 1), and writes and
+// transforms only those, in slot order.  world = 1 owns all, slot = q.
+void gather_plan_build(GatherPlan& gp, int N, int c, int t, int n, int w, int rank = 0,
+                       int world = 1);
 void gather_plan_free(GatherPlan& gp);
 
 // Launch parameters of the fused leaf kernel (dpf_keyed_impl.cuh).
@@ -104,6 +112,7 @@ struct LeafLaunch {
     const uint32_t* off = nullptr;
     const uint32_t* entries = nullptr;
     const uint16_t* q_order = nullptr;
+    const uint16_t* q_slot = nullptr;
     int t = 0, levels = 0, hl = 0;
     size_t bin = 0;
     int N = 0, party = 0;
@@ -139,8 +148,10 @@ struct Workspace {
     Blk* tops = nullptr;
     uint64_t* g = nullptr;
 };
+// rank/world: this expander's shard of the pair blocks (see GatherPlan).
 pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64_t* public_a,
-                               const uint8_t* master_key);
+                               const uint8_t* master_key, int rank = 0, int world = 1);
+void expander_shard(const pcgb_expander* e, int* rank, int* world, int* q_local, int* q_total);
 void expander_destroy(pcgb_expander* e);
 void expander_info(const pcgb_expander* e, int* K, int* levels, int* nk, size_t* scratch);
 int expander_autotune(pcgb_expander* e);          // leaf CTA size, cached per shape

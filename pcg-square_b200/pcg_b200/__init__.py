@@ -105,6 +105,10 @@ def _load():
         "pcgb_expand_g_device": ([_vp, C.c_int, _vp, _vp, _vp, _vp, _vp], C.c_int),
         "pcgb_expander_set_profiling": ([_vp, C.c_int], C.c_int),
         "pcgb_expander_set_graph": ([_vp, C.c_int], C.c_int),
+        "pcgb_expander_create_shard": ([_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp,
+                                        _vp, C.c_int, C.c_int], C.c_int),
+        "pcgb_expander_shard": ([_vp] * 5, C.c_int),
+        "pcgb_reduce_mod_p": ([_vp, _vp, C.c_size_t, _vp], C.c_int),
         "pcgb_expand_from_g_device": ([_vp] * 6 + [_vp], C.c_int),
         "pcgb_dpf_out_scatter_g_device": ([_vp, C.c_int, C.c_size_t, C.c_int, C.c_int, _vp, _vp,
                                            C.c_int, _vp], C.c_int),
@@ -248,6 +252,11 @@ def verify_ole_device(N, d_x0, d_z0, d_x1, d_z1, d_bad, stream=None):
 def verify_triples_device(N, d_a0, d_b0, d_c0, d_a1, d_b1, d_c1, d_bad, stream=None):
     """d_bad (one u64 on the device) := slots where (a0+a1)(b0+b1) != c0+c1."""
     _check(lib.pcgb_verify_triples_device(N, d_a0, d_b0, d_c0, d_a1, d_b1, d_c1, d_bad, stream))
+
+
+def reduce_mod_p(d_dst, d_src, count, stream=None):
+    """d_dst[i] = d_src[i] mod p for any 64-bit words (device)."""
+    _check(lib.pcgb_reduce_mod_p(d_dst, d_src, count, stream))
 
 
 def trim_pool():
@@ -466,17 +475,23 @@ def public_a(N, c, a_seed):
 class Expander:
     """Resident per-shape state of the fused PCG-OLE expansion (one device)."""
 
-    def __init__(self, N, c, t, w=1, prg=PRG_CHACHA8, public_a=None, master_key=None):
+    def __init__(self, N, c, t, w=1, prg=PRG_CHACHA8, public_a=None, master_key=None,
+                 rank=0, world=1):
+        """rank/world: this expander's shard of the pair blocks (see
+        pcgb_expander_create_shard); Q is then the shard's own pair count."""
         self.N, self.c, self.t, self.w, self.prg = N, c, t, w, prg
         pa = None if public_a is None else np.ascontiguousarray(public_a, np.uint64)
         mk = None if master_key is None else _u8(master_key)
         h = C.c_void_p()
-        _check(lib.pcgb_expander_create(C.byref(h), N, c, t, w, prg, _p(pa), _p(mk)))
+        _check(lib.pcgb_expander_create_shard(C.byref(h), N, c, t, w, prg, _p(pa), _p(mk),
+                                              rank, world))
         self.h = h.value
         K, L, nk, sb = C.c_int(), C.c_int(), C.c_int(), C.c_size_t()
         _check(lib.pcgb_expander_info(self.h, C.byref(K), C.byref(L), C.byref(nk), C.byref(sb)))
         self.K, self.levels, self.nk, self.scratch_bytes = K.value, L.value, nk.value, sb.value
-        self.Q = c * (c + 1) // 2
+        r, wd, ql, qt = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(lib.pcgb_expander_shard(self.h, C.byref(r), C.byref(wd), C.byref(ql), C.byref(qt)))
+        self.rank, self.world, self.Q, self.Q_total = r.value, wd.value, ql.value, qt.value
 
     def close(self):
         if getattr(self, "h", None):
