@@ -49,6 +49,70 @@ __device__ __forceinline__ void aes128_encrypt_words(const uint32_t* __restrict_
 #undef PCGB_SB
 }
 
+// Bank-conflict-free form.  The state bytes index the tables at random, so
+// the 32 lanes of a warp reading one 256-word table collide in several banks
+// per lookup.  Here a single table Te0 is stored 32 times interleaved,
+// te_rep[x * 32 + c] = Te0[x], and lane L reads copy L: every lookup of a
+// warp hits 32 different banks.  Te1..Te3 are Te0 rotated left by 8, 16 and
+// 24 bits, applied with byte permutes.
+constexpr int kAesRepWords = 256 * 32;
+
+__device__ __forceinline__ uint32_t rotl8_u32(uint32_t x) { return __byte_perm(x, 0, 0x2103); }
+__device__ __forceinline__ uint32_t rotl16_u32(uint32_t x) { return __byte_perm(x, 0, 0x1032); }
+__device__ __forceinline__ uint32_t rotl24_u32(uint32_t x) { return __byte_perm(x, 0, 0x0321); }
+
+// Fills te_rep (kAesRepWords words of shared memory) from Te0 (256 words in
+// global memory); all threads of the CTA take part, no barrier inside.
+__device__ __forceinline__ void aes_fill_rep(uint32_t* te_rep, const uint32_t* __restrict__ te0) {
+    for (int i = threadIdx.x; i < kAesRepWords; i += blockDim.x) te_rep[i] = __ldg(te0 + (i >> 5));
+}
+
+__device__ __forceinline__ void aes128_encrypt_words_rep(const uint32_t* __restrict__ te_rep,
+                                                         const uint32_t* __restrict__ rk,
+                                                         uint32_t& w0, uint32_t& w1, uint32_t& w2,
+                                                         uint32_t& w3) {
+    const uint32_t* T = te_rep + (threadIdx.x & 31);
+#define PCGB_TE(x) T[static_cast<uint32_t>(x) << 5]
+    uint32_t s0 = w0 ^ rk[0], s1 = w1 ^ rk[1], s2 = w2 ^ rk[2], s3 = w3 ^ rk[3];
+#pragma unroll
+    for (int r = 1; r < 10; ++r) {
+        const uint32_t t0 = PCGB_TE(s0 & 0xff) ^ rotl8_u32(PCGB_TE((s1 >> 8) & 0xff)) ^
+                            rotl16_u32(PCGB_TE((s2 >> 16) & 0xff)) ^ rotl24_u32(PCGB_TE(s3 >> 24)) ^
+                            rk[4 * r + 0];
+        const uint32_t t1 = PCGB_TE(s1 & 0xff) ^ rotl8_u32(PCGB_TE((s2 >> 8) & 0xff)) ^
+                            rotl16_u32(PCGB_TE((s3 >> 16) & 0xff)) ^ rotl24_u32(PCGB_TE(s0 >> 24)) ^
+                            rk[4 * r + 1];
+        const uint32_t t2 = PCGB_TE(s2 & 0xff) ^ rotl8_u32(PCGB_TE((s3 >> 8) & 0xff)) ^
+                            rotl16_u32(PCGB_TE((s0 >> 16) & 0xff)) ^ rotl24_u32(PCGB_TE(s1 >> 24)) ^
+                            rk[4 * r + 2];
+        const uint32_t t3 = PCGB_TE(s3 & 0xff) ^ rotl8_u32(PCGB_TE((s0 >> 8) & 0xff)) ^
+                            rotl16_u32(PCGB_TE((s1 >> 16) & 0xff)) ^ rotl24_u32(PCGB_TE(s2 >> 24)) ^
+                            rk[4 * r + 3];
+        s0 = t0; s1 = t1; s2 = t2; s3 = t3;
+    }
+#define PCGB_SB(x) ((PCGB_TE(x) >> 8) & 0xffu)
+    w0 = (PCGB_SB(s0 & 0xff) | (PCGB_SB((s1 >> 8) & 0xff) << 8) |
+          (PCGB_SB((s2 >> 16) & 0xff) << 16) | (PCGB_SB(s3 >> 24) << 24)) ^ rk[40];
+    w1 = (PCGB_SB(s1 & 0xff) | (PCGB_SB((s2 >> 8) & 0xff) << 8) |
+          (PCGB_SB((s3 >> 16) & 0xff) << 16) | (PCGB_SB(s0 >> 24) << 24)) ^ rk[41];
+    w2 = (PCGB_SB(s2 & 0xff) | (PCGB_SB((s3 >> 8) & 0xff) << 8) |
+          (PCGB_SB((s0 >> 16) & 0xff) << 16) | (PCGB_SB(s1 >> 24) << 24)) ^ rk[42];
+    w3 = (PCGB_SB(s3 & 0xff) | (PCGB_SB((s0 >> 8) & 0xff) << 8) |
+          (PCGB_SB((s1 >> 16) & 0xff) << 16) | (PCGB_SB(s2 >> 24) << 24)) ^ rk[43];
+#undef PCGB_SB
+#undef PCGB_TE
+}
+
+__device__ __forceinline__ void aes_ccr_rep(const uint32_t* te_rep, const uint32_t* rk,
+                                            uint64_t lo, uint64_t hi, uint64_t& olo,
+                                            uint64_t& ohi) {
+    uint32_t w0 = static_cast<uint32_t>(lo), w1 = static_cast<uint32_t>(lo >> 32);
+    uint32_t w2 = static_cast<uint32_t>(hi), w3 = static_cast<uint32_t>(hi >> 32);
+    aes128_encrypt_words_rep(te_rep, rk, w0, w1, w2, w3);
+    olo = (w0 | (static_cast<uint64_t>(w1) << 32)) ^ lo;
+    ohi = (w2 | (static_cast<uint64_t>(w3) << 32)) ^ hi;
+}
+
 // Correlation-robust hash H(x) = AES_k(x) ^ x on a node held as (lo, hi).
 __device__ __forceinline__ void aes_ccr(const uint32_t* te, const uint32_t* rk, uint64_t lo,
                                         uint64_t hi, uint64_t& olo, uint64_t& ohi) {

@@ -31,6 +31,9 @@ namespace {
 
 constexpr int kTPB = 128;
 
+// The compact four-table AES: these kernels run one short pass per node, so
+// staging the per-lane replicated table (32 KB per CTA) would cost as much
+// as the bank conflicts it removes.
 struct AesSm {
     uint32_t te[1024];
     uint32_t rk[15 * 44];

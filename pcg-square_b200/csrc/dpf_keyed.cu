@@ -13,7 +13,7 @@ namespace pcgb {
 
 size_t keyed_tops_scratch_nodes(int K, int w, int to_level) {
     int l1 = 0;
-    while (l1 < to_level && (static_cast<size_t>(K) << (w * l1)) < 65536) ++l1;
+    while (l1 < to_level && (static_cast<size_t>(K) << (w * l1)) < kTopsStage2Threads) ++l1;
     if (l1 >= to_level || l1 == 0) return 0;
     return static_cast<size_t>(K) << (w * l1);
 }

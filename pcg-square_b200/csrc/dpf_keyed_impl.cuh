@@ -45,13 +45,13 @@ template <int W>
 __host__ __device__ constexpr int tops_max_depth() { return 30 / W + 1; }
 
 struct AesSmem {
-    uint32_t te[1024];
+    uint32_t te_rep[kAesRepWords];   // Te0 replicated per lane (aes128.cuh)
     uint32_t rk[15 * 44];
 };
 
 __device__ __forceinline__ void load_aes_smem(AesSmem& s, const uint32_t* te, const uint32_t* rk,
                                               int nk) {
-    for (int i = threadIdx.x; i < 1024; i += blockDim.x) s.te[i] = te[i];
+    aes_fill_rep(s.te_rep, te);
     for (int i = threadIdx.x; i < nk * 44; i += blockDim.x) s.rk[i] = rk[i];
     __syncthreads();
 }
@@ -94,7 +94,7 @@ __device__ __forceinline__ void children(const Blk& p, const Blk* __restrict__ c
 #pragma unroll 1
         for (int k = 0; k < NK; ++k) {
             uint64_t hl, hh;
-            aes_ccr(aes->te, aes->rk + 44 * k, p.lo, p.hi, hl, hh);
+            aes_ccr_rep(aes->te_rep, aes->rk + 44 * k, p.lo, p.hi, hl, hh);
             const Blk cv = ldblk(cw + k);
             cfl ^= cv.lo; cfh ^= cv.hi;
             hxl ^= hl; hxh ^= hh;
@@ -123,7 +123,8 @@ __device__ __forceinline__ void hash_raw(const Blk& p, const AesSmem* aes, Blk (
         }
     } else {
 #pragma unroll 1
-        for (int k = 0; k < NK; ++k) aes_ccr(aes->te, aes->rk + 44 * k, p.lo, p.hi, h[k].lo, h[k].hi);
+        for (int k = 0; k < NK; ++k)
+            aes_ccr_rep(aes->te_rep, aes->rk + 44 * k, p.lo, p.hi, h[k].lo, h[k].hi);
     }
 }
 
@@ -317,7 +318,7 @@ void tops_dispatch(int K, int levels, const Blk* roots, const Blk* cws, const ui
                    const uint32_t* rk, int to_level, Blk* out, Blk* scratch, cudaStream_t st) {
     // Stage 1 gives every key m^l1 subtrees so stage 2 has enough threads.
     int l1 = 0;
-    while (l1 < to_level && (static_cast<size_t>(K) << (W * l1)) < 65536) ++l1;
+    while (l1 < to_level && (static_cast<size_t>(K) << (W * l1)) < kTopsStage2Threads) ++l1;
     if (l1 >= to_level || l1 == 0) {
         launch_tops<W, PRG>(roots, K, 0, to_level, levels, cws, te, rk, out, st);
         return;

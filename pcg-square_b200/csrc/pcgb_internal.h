@@ -77,6 +77,12 @@ void keyed_expand_tops(int K, int n, int w, int prg, const Blk* roots, const Blk
 // Contribution list of the gather form of the output-layer scatter: for
 // every merged (i<=j) pair q and output bin r, the key halves that land in
 // [r*bin, (r+1)*bin) of the folded g (see gather_plan in dpf_keyed.cu).
+// Keyed top-level expansion runs in two stages: stage 1 expands every key to
+// the level where K * m^l1 reaches this many subtrees, stage 2 gives each
+// subtree a thread that walks it depth first.  2^19 threads keep every SM
+// busy (a few thousand threads each) and keep the walks shallow.
+constexpr size_t kTopsStage2Threads = size_t{1} << 19;
+
 struct GatherPlan {
     int N = 0, c = 0, t = 0, n = 0, w = 0, Q = 0;
     int sl = 0;          // levels expanded per thread in the leaf kernel
