@@ -11,11 +11,29 @@
 
 namespace pcgb {
 
+std::vector<int> tops_stages(int K, int w, int to_level) {
+    std::vector<int> b{0};
+    int l = 0;
+    while (l < to_level) {
+        if ((static_cast<size_t>(K) << (w * l)) >= kTopsStage2Threads) {
+            b.push_back(to_level);
+            break;
+        }
+        int s = 1;
+        while (l + s < to_level && (static_cast<size_t>(K) << (w * (l + s))) < kTopsStage2Threads &&
+               (1 << (w * (s + 1))) <= 32)
+            ++s;
+        l += s;
+        b.push_back(l);
+    }
+    return b;
+}
+
+// Two ping-pong halves, each holding the largest intermediate level.
 size_t keyed_tops_scratch_nodes(int K, int w, int to_level) {
-    int l1 = 0;
-    while (l1 < to_level && (static_cast<size_t>(K) << (w * l1)) < kTopsStage2Threads) ++l1;
-    if (l1 >= to_level || l1 == 0) return 0;
-    return static_cast<size_t>(K) << (w * l1);
+    const std::vector<int> b = tops_stages(K, w, to_level);
+    if (b.size() <= 2) return 0;
+    return 2 * (static_cast<size_t>(K) << (w * b[b.size() - 2]));
 }
 
 void keyed_expand_tops(int K, int n, int w, int prg, const Blk* roots, const Blk* cws,

@@ -316,15 +316,16 @@ void launch_tops(const Blk* src, int K, int src_lvl, int nlev, int levels, const
 template <int W, int PRG>
 void tops_dispatch(int K, int levels, const Blk* roots, const Blk* cws, const uint32_t* te,
                    const uint32_t* rk, int to_level, Blk* out, Blk* scratch, cudaStream_t st) {
-    // Stage 1 gives every key m^l1 subtrees so stage 2 has enough threads.
-    int l1 = 0;
-    while (l1 < to_level && (static_cast<size_t>(K) << (W * l1)) < kTopsStage2Threads) ++l1;
-    if (l1 >= to_level || l1 == 0) {
-        launch_tops<W, PRG>(roots, K, 0, to_level, levels, cws, te, rk, out, st);
-        return;
+    // Stages (tops_stages): intermediate levels alternate between the two
+    // halves of the scratch, the last stage writes `out`.
+    const std::vector<int> b = tops_stages(K, W, to_level);
+    const size_t half = b.size() > 2 ? (static_cast<size_t>(K) << (W * b[b.size() - 2])) : 0;
+    const Blk* src = roots;
+    for (size_t k = 0; k + 1 < b.size(); ++k) {
+        Blk* dst = (k + 2 == b.size()) ? out : scratch + (k % 2) * half;
+        launch_tops<W, PRG>(src, K, b[k], b[k + 1] - b[k], levels, cws, te, rk, dst, st);
+        src = dst;
     }
-    launch_tops<W, PRG>(roots, K, 0, l1, levels, cws, te, rk, scratch, st);
-    launch_tops<W, PRG>(scratch, K, l1, to_level - l1, levels, cws, te, rk, out, st);
 }
 
 template <int W, int PRG>

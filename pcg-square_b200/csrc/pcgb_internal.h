@@ -77,11 +77,15 @@ void keyed_expand_tops(int K, int n, int w, int prg, const Blk* roots, const Blk
 // Contribution list of the gather form of the output-layer scatter: for
 // every merged (i<=j) pair q and output bin r, the key halves that land in
 // [r*bin, (r+1)*bin) of the folded g (see gather_plan in dpf_keyed.cu).
-// Keyed top-level expansion runs in two stages: stage 1 expands every key to
-// the level where K * m^l1 reaches this many subtrees, stage 2 gives each
-// subtree a thread that walks it depth first.  2^19 threads keep every SM
-// busy (a few thousand threads each) and keep the walks shallow.
+// Keyed top-level expansion runs in stages.  Each stage gives every node of
+// its start level a thread that walks its subtree depth first down to the
+// next boundary; the thread count grows at most 32-fold per stage (so the
+// early, narrow stages do short walks) until K * m^l reaches this many
+// subtrees, and the final stage walks from there to the target level.
+// 2^19 threads keep every SM busy and the final walks shallow.
 constexpr size_t kTopsStage2Threads = size_t{1} << 19;
+// Stage boundaries 0 = l_0 < l_1 < ... < l_s = to_level.
+std::vector<int> tops_stages(int K, int w, int to_level);
 
 struct GatherPlan {
     int N = 0, c = 0, t = 0, n = 0, w = 0, Q = 0;
