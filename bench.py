@@ -304,7 +304,8 @@ def run_ours(args, d):
     flush = L.DeviceBuffer(2 * L2_BYTES)
     args_dev = (d_r0.ptr, d_cws.ptr, d_cwo.ptr, d_pos.ptr, d_val.ptr, d_x.ptr, d_z.ptr)
 
-    leaf_tpb = e.autotune()     # leaf-kernel CTA size for this shape (untimed)
+    e.autotune()                # leaf-kernel shape for this expansion shape (untimed)
+    leaf_tpb, leaf_lpt = e.leaf_shape()
     for _ in range(args.warmup):
         e.expand_device(0, *args_dev)
     L.synchronize()
@@ -407,13 +408,14 @@ def run_ours(args, d):
     # Roofline of the dominant kernel (fused leaf gather), ALU bound.
     leaf_ms = float(np.mean([s[1] for s in stages])) if stages else None
     D = 1 << e.levels
-    S = 16
+    S = leaf_lpt                # leaves per thread of the leaf kernel
     # Per leaf: one output hash; per internal node below the frontier (S - 1
     # of them per S leaves): one tree block.
     ops = K * D * (OPS_OUT_HASH + OPS_TREE_W1 * (S - 1) / S)
     achieved = ops / (leaf_ms * 1e-3) / 1e12 if leaf_ms else None
     peak = gops_peak / 1e3
-    roofline = {"bound": "int_alu", "kernel": "leaf_gather_kernel<1,4,chacha8>",
+    roofline = {"bound": "int_alu",
+                "kernel": f"leaf_gather_kernel<1,{S.bit_length() - 1},chacha8>",
                 "achieved": achieved, "peak": peak, "unit": "Tops/s",
                 "frac": achieved / peak if achieved else None,
                 "traffic": LEAF_DRAM_BYTES_PER_LEAF * K * D,
@@ -462,6 +464,7 @@ def run_ours(args, d):
                        "parallelism": f"replicas x{d.world}",
                        "l2": "flushed between timed steps (256 MiB write)",
                        "cuda_graph": bool(args.graph), "leaf_cta_threads": leaf_tpb,
+                       "leaf_leaves_per_thread": leaf_lpt,
                        "vs_baseline_ref": "1x L40S serial arm 5.46M corr/s "
                                           "(GPU_baseline/final_l40s/e2e_arms.csv:32)"},
             "stage_ms": dict(zip(["tops", "leaf_gather", "x", "ntt"], stage_means))

@@ -244,11 +244,16 @@ int pcgb_expander_stage_times(pcgb_expander* e, float* ms, int max_expansions);
  * with one launch; other pointers re-capture and update it.  The stream
  * must be capturable (not the legacy default stream).  Off by default. */
 int pcgb_expander_set_graph(pcgb_expander* e, int enable);
-/* Times the fused leaf kernel at each CTA size that fits the shape (on zero
- * keys: its work does not depend on key values), keeps the fastest for this
- * expander and caches it per device and shape; *tpb_out gets the choice.
- * Synchronises the library stream.  Server plans are tuned on creation. */
+/* Times the top-level walk plus the fused leaf kernel for each leaf shape
+ * that fits the shape -- leaves per thread (the default and two smaller
+ * powers of m; fewer leaves per thread means more threads and a deeper
+ * frontier, which pays at small N) times CTA size -- on zero keys (their
+ * work does not depend on key values), keeps the fastest for this expander
+ * and caches it per device, shape and shard; *tpb_out gets the CTA size.
+ * The workspace size (pcgb_expander_info) may change.  Synchronises the
+ * library stream.  Server plans are tuned on creation. */
 int pcgb_expander_autotune(pcgb_expander* e, int* tpb_out);
+int pcgb_expander_leaf_shape(const pcgb_expander* e, int* tpb, int* leaves_per_thread);
 
 /* ---- native: consumers of the expansion -------------------------------- */
 /* One party's N Beaver-triple slot shares from its two ring OLEs (x1, z1)

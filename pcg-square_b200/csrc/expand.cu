@@ -145,6 +145,7 @@ struct pcgb_expander {
     uint64_t* d_g = nullptr;     // Q*N
     uint32_t* d_rk = nullptr;    // AES sub-key schedules
     size_t scratch_bytes = 0;
+    size_t own_ws_bytes = 0;     // size of d_F when allocated
     std::vector<cudaEvent_t> prof_ev;  // 5 per slot
     int prof_slots = 0, prof_used = 0;
     // CUDA graph of expand_device on the expander's own workspace.
@@ -292,8 +293,19 @@ void expand_device_ws(pcgb_expander* e, const Workspace& ws, int party, const Bl
 // The expander's own workspace, allocated on first use (plans held by the
 // server never need it: requests bring their own).
 void ensure_own_workspace(pcgb_expander* e) {
-    if (e->d_F) return;
+    if (e->d_F && e->own_ws_bytes >= e->scratch_bytes) return;
+    if (e->d_F) {
+        // Regrow (the leaf shape changed): drain uses of the old one first;
+        // a captured graph refers to it, so drop the graph too.
+        PCGB_CK(cudaDeviceSynchronize());
+        cudaFree(e->d_F);
+        e->d_F = nullptr;
+        if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+        e->graph_exec = nullptr;
+        e->graph_warm = false;
+    }
     PCGB_CK(cudaMalloc(&e->d_F, e->scratch_bytes));
+    e->own_ws_bytes = e->scratch_bytes;
     const Workspace ws = workspace_carve(e, e->d_F);
     e->d_tops = ws.tops;
     e->d_g = ws.g;
@@ -378,73 +390,111 @@ void expander_set_graph(pcgb_expander* e, bool on) {
     e->use_graph = on;
 }
 
-// Leaf-kernel CTA size: time each candidate on this shape (the kernel's work
-// does not depend on key values, so zero keys serve) and keep the fastest.
-// Results are cached per device and shape; later expanders of the shape
-// reuse them without timing.
+// Leaf-kernel shape for this expander: leaves per thread (S = m^sl; fewer
+// means more threads, shorter serial walks and a deeper frontier, which
+// pays at small shapes) and CTA size.  Each candidate runs the top-level
+// walk and the leaf kernel on zero keys (their work does not depend on key
+// values); the fastest is kept and cached per device, shape and shard.
+// Changing sl changes the frontier level, so the workspace size is
+// recomputed (and an expander's own workspace regrown on next use).
+namespace {
+void set_leaf_sl(pcgb_expander* e, int sl) {
+    e->gp.sl = sl;
+    e->gp.S = 1 << (e->w * sl);
+    e->gp.hl = e->levels - sl;
+}
+}  // namespace
+
 int expander_autotune(pcgb_expander* e) {
     static std::mutex mu;
-    static std::map<std::tuple<int, int, int, int, int, int, int>, int> cache;
+    static std::map<std::tuple<int, int, int, int, int, int, int>, std::pair<int, int>> cache;
     const auto key = std::make_tuple(e->dev, e->N, e->c, e->t, e->w, e->prg,
                                      e->gp.world * 64 + e->gp.rank);
     {
         std::lock_guard<std::mutex> lk(mu);
         auto it = cache.find(key);
         if (it != cache.end()) {
-            e->gp.tpb = it->second;
-            return it->second;
+            set_leaf_sl(e, it->second.first);
+            e->gp.tpb = it->second.second;
+            e->scratch_bytes = workspace_bytes(e);
+            return e->gp.tpb;
         }
+    }
+    // Candidate leaves-per-thread exponents: the default and up to two
+    // smaller, as long as the walk below the frontier keeps >= 1 level.
+    const int sl0 = e->gp.sl;
+    std::vector<int> sls;
+    for (int sl = sl0; sl >= 1 && sl >= sl0 - 2; --sl) sls.push_back(sl);
+    size_t ws_max = 0;
+    for (int sl : sls) {
+        set_leaf_sl(e, sl);
+        ws_max = std::max(ws_max, workspace_bytes(e));
     }
     cudaStream_t st = default_stream();
     const size_t K = e->K;
     const size_t b_roots = K * sizeof(Blk), b_cws = K * e->levels * e->nk * sizeof(Blk);
     const size_t b_keys = (b_roots + b_cws + 8 * K + 255) & ~static_cast<size_t>(255);
     // A scratch workspace from the pool (server plans own none).
-    char* d = static_cast<char*>(pool_alloc(b_keys + e->scratch_bytes, st));
+    char* d = static_cast<char*>(pool_alloc(b_keys + ws_max, st));
     PCGB_CK(cudaMemsetAsync(d, 0, b_roots + b_cws + 8 * K, st));
-    const Workspace ws = workspace_carve(e, d + b_keys);
     const Blk* roots = reinterpret_cast<const Blk*>(d);
     const Blk* cws = reinterpret_cast<const Blk*>(d + b_roots);
     const uint64_t* cwo = reinterpret_cast<const uint64_t*>(d + b_roots + b_cws);
-    keyed_expand_tops(e->K, e->n, e->w, e->prg, roots, cws, e->d_rk, e->gp.hl, ws.F, ws.tops, st);
     const size_t bin = static_cast<size_t>(e->N) / e->t;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     PCGB_CK(cudaEventCreate(&e0));
     PCGB_CK(cudaEventCreate(&e1));
-    int best = 0;
+    int best_sl = sl0, best_tpb = 0;
     float best_ms = 0;
     try {
-        for (int tpb : {256, 128, 64, 32}) {
-            if (static_cast<size_t>(tpb) * e->gp.S > bin) continue;
-            e->gp.tpb = tpb;
-            keyed_leaf_gather(e->gp, 0, e->prg, ws.F, cws, cwo, e->d_rk, ws.g, st);  // warm
-            float ms = 0;
-            for (int rep = 0; rep < 3; ++rep) {
-                PCGB_CK(cudaEventRecord(e0, st));
-                keyed_leaf_gather(e->gp, 0, e->prg, ws.F, cws, cwo, e->d_rk, ws.g, st);
-                PCGB_CK(cudaEventRecord(e1, st));
-                PCGB_CK(cudaEventSynchronize(e1));
-                float t = 0;
-                PCGB_CK(cudaEventElapsedTime(&t, e0, e1));
-                ms = rep == 0 ? t : std::min(ms, t);
+        for (int sl : sls) {
+            set_leaf_sl(e, sl);
+            const Workspace ws = workspace_carve(e, d + b_keys);
+            for (int tpb : {256, 128, 64, 32}) {
+                if (static_cast<size_t>(tpb) * e->gp.S > bin) continue;
+                e->gp.tpb = tpb;
+                auto run = [&] {
+                    keyed_expand_tops(e->K, e->n, e->w, e->prg, roots, cws, e->d_rk, e->gp.hl,
+                                      ws.F, ws.tops, st);
+                    keyed_leaf_gather(e->gp, 0, e->prg, ws.F, cws, cwo, e->d_rk, ws.g, st);
+                };
+                run();   // warm
+                float ms = 0;
+                for (int rep = 0; rep < 3; ++rep) {
+                    PCGB_CK(cudaEventRecord(e0, st));
+                    run();
+                    PCGB_CK(cudaEventRecord(e1, st));
+                    PCGB_CK(cudaEventSynchronize(e1));
+                    float t = 0;
+                    PCGB_CK(cudaEventElapsedTime(&t, e0, e1));
+                    ms = rep == 0 ? t : std::min(ms, t);
+                }
+                if (best_tpb == 0 || ms < best_ms) { best_sl = sl; best_tpb = tpb; best_ms = ms; }
             }
-            if (best == 0 || ms < best_ms) { best = tpb; best_ms = ms; }
         }
     } catch (...) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         cudaFreeAsync(d, st);
+        set_leaf_sl(e, sl0);
         throw;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     PCGB_CK(cudaFreeAsync(d, st));
     PCGB_CK(cudaStreamSynchronize(st));
-    if (best == 0) best = 32;
-    e->gp.tpb = best;
+    if (best_tpb == 0) best_tpb = 32;
+    set_leaf_sl(e, best_sl);
+    e->gp.tpb = best_tpb;
+    e->scratch_bytes = workspace_bytes(e);
     std::lock_guard<std::mutex> lk(mu);
-    cache[key] = best;
-    return best;
+    cache[key] = {best_sl, best_tpb};
+    return best_tpb;
+}
+
+void expander_leaf_shape(const pcgb_expander* e, int* tpb, int* leaves_per_thread) {
+    if (tpb) *tpb = e->gp.tpb > 0 ? e->gp.tpb : 256;
+    if (leaves_per_thread) *leaves_per_thread = e->gp.S;
 }
 
 void expand_host(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,

@@ -113,6 +113,7 @@ def _load():
         "pcgb_dpf_out_scatter_g_device": ([_vp, C.c_int, C.c_size_t, C.c_int, C.c_int, _vp, _vp,
                                            C.c_int, _vp], C.c_int),
         "pcgb_expander_autotune": ([_vp, C.POINTER(C.c_int)], C.c_int),
+        "pcgb_expander_leaf_shape": ([_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
         "pcgb_expander_stage_times": ([_vp, C.POINTER(C.c_float), C.c_int], C.c_int),
         "pcgb_launch_count": ([], C.c_ulonglong),
         "pcgb_arx_peak": ([C.POINTER(C.c_double), C.POINTER(C.c_float)], C.c_int),
@@ -535,10 +536,20 @@ class Expander:
         _check(lib.pcgb_expander_set_graph(self.h, 1 if enable else 0))
 
     def autotune(self):
-        """Pick the fused leaf kernel's CTA size for this shape; returns it."""
+        """Pick the fused leaf kernel's shape (leaves per thread, CTA size)
+        for this expansion shape; returns the CTA size."""
         v = C.c_int()
         _check(lib.pcgb_expander_autotune(self.h, C.byref(v)))
+        K, L, nk, sb = C.c_int(), C.c_int(), C.c_int(), C.c_size_t()
+        _check(lib.pcgb_expander_info(self.h, C.byref(K), C.byref(L), C.byref(nk), C.byref(sb)))
+        self.scratch_bytes = sb.value
         return v.value
+
+    def leaf_shape(self):
+        """(CTA threads, leaves per thread) of the fused leaf kernel."""
+        tpb, lpt = C.c_int(), C.c_int()
+        _check(lib.pcgb_expander_leaf_shape(self.h, C.byref(tpb), C.byref(lpt)))
+        return tpb.value, lpt.value
 
     def set_profiling(self, slots):
         """Record per-stage events for the next `slots` expansions (0 = off)."""
