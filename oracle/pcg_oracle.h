@@ -113,7 +113,9 @@ uint64_t orc_mulmod(uint64_t a, uint64_t b);
 
 /* ---- seeded synthetic material + expansion ----------------------------- */
 /* Counter-based generator shared with the library's dealer (own definition,
- * documented in DESIGN.md): rnd(seed, dom, idx). */
+ * since the reference draws from unseeded emp PRGs): with the SplitMix64
+ * finaliser mix, rnd(seed, dom, idx) = mix(mix(seed ^ dom * phi) + (idx + 1)
+ * * 0xd1b54a32d192ed03), phi = 0x9e3779b97f4a7c15. */
 uint64_t orc_rnd(uint64_t seed, uint64_t dom, uint64_t idx);
 
 typedef struct {
