@@ -218,6 +218,17 @@ int pcgb_expand_device(pcgb_expander* e, int party, const pcgb_blk* d_roots,
 int pcgb_expand_host(pcgb_expander* e, int party, const pcgb_blk* roots, const pcgb_blk* cws,
                      const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val,
                      uint64_t* x, uint64_t* z);
+/* pcgb_expand_host without waiting (no reference counterpart): the copies
+ * and kernels are queued on one of two internal streams, alternating, with
+ * the expansions themselves kept in order (they share the workspace), so one
+ * expansion's host copies overlap the next one's kernels.  Host buffers must
+ * stay valid until pcgb_expander_wait (pin them for real overlap).  Other
+ * calls on the same expander first wait for pending asynchronous ones only
+ * in pcgb_expand_host; call pcgb_expander_wait before pcgb_expand_device. */
+int pcgb_expand_host_async(pcgb_expander* e, int party, const pcgb_blk* roots,
+                           const pcgb_blk* cws, const uint64_t* cw_out, const uint64_t* pos,
+                           const uint64_t* val, uint64_t* x, uint64_t* z);
+int pcgb_expander_wait(pcgb_expander* e);
 /* Only the DPF + output-layer stages: the folded, pair-merged g' buffers
  * (Q = c(c+1)/2 of N words, pair order (0,0),(0,1)..(0,c-1),(1,1),..),
  * g'_ij = g_ij + g_ji for i < j.  For parity checks and staged pipelines. */

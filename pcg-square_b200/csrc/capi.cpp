@@ -587,6 +587,23 @@ int pcgb_expand_device(pcgb_expander* e, int party, const pcgb_blk* d_roots, con
     });
 }
 
+int pcgb_expand_host_async(pcgb_expander* e, int party, const pcgb_blk* roots,
+                           const pcgb_blk* cws, const uint64_t* cw_out, const uint64_t* pos,
+                           const uint64_t* val, uint64_t* x, uint64_t* z) {
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander");
+        pcgb::expand_host_async(e, party, reinterpret_cast<const Blk*>(roots),
+                                reinterpret_cast<const Blk*>(cws), cw_out, pos, val, x, z);
+    });
+}
+
+int pcgb_expander_wait(pcgb_expander* e) {
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander");
+        pcgb::expander_wait(e);
+    });
+}
+
 int pcgb_expand_host(pcgb_expander* e, int party, const pcgb_blk* roots, const pcgb_blk* cws,
                      const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val, uint64_t* x,
                      uint64_t* z) {

@@ -161,6 +161,17 @@ struct pcgb_expander {
     size_t h_stage_bytes = 0;
     void* d_in = nullptr;
     size_t d_in_bytes = 0;
+    // pcgb_expand_host_async: two I/O slots, each with its own stream and
+    // device buffers; the computes (which share the workspace) are chained
+    // by `async_compute` so slot i's copies overlap slot i+1's kernels.
+    struct AsyncSlot {
+        cudaStream_t st = nullptr;
+        void* d_io = nullptr;
+        size_t bytes = 0;
+    } aslot[2];
+    int aturn = 0;
+    cudaEvent_t async_compute = nullptr;
+    bool async_pending = false;
 };
 
 namespace pcgb {
@@ -242,6 +253,12 @@ void expander_destroy(pcgb_expander* e) {
     cudaFree(e->d_img); cudaFree(e->d_aR); cudaFree(e->d_F); cudaFree(e->d_rk);
     cudaFree(e->d_in);
     if (e->h_stage) cudaFreeHost(e->h_stage);
+    for (auto& a : e->aslot) {
+        if (a.st) cudaStreamSynchronize(a.st);
+        cudaFree(a.d_io);
+        if (a.st) cudaStreamDestroy(a.st);
+    }
+    if (e->async_compute) cudaEventDestroy(e->async_compute);
     for (auto& ev : e->prof_ev) cudaEventDestroy(ev);
     if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
     cudaSetDevice(cur);
@@ -497,9 +514,67 @@ void expander_leaf_shape(const pcgb_expander* e, int* tpb, int* leaves_per_threa
     if (leaves_per_thread) *leaves_per_thread = e->gp.S;
 }
 
+void expander_wait(pcgb_expander* e) {
+    for (auto& a : e->aslot)
+        if (a.st) PCGB_CK(cudaStreamSynchronize(a.st));
+    e->async_pending = false;
+}
+
+// One expansion from host inputs to host outputs without waiting for it.
+// Host buffers must stay valid (and, for overlap, be pinned) until
+// expander_wait.  Slot k's stream runs H2D -> (wait for the previous
+// compute) -> kernels -> D2H, alternating k = 0, 1.
+void expand_host_async(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
+                       const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val,
+                       uint64_t* x, uint64_t* z) {
+    if (!roots || !cws || !cw_out || !pos || !val || !x || !z)
+        fail(PCGB_EINVAL, "expand_host_async: null pointer");
+    const size_t K = e->K, ct = static_cast<size_t>(e->c) * e->t, NN = e->N;
+    const size_t b_roots = K * sizeof(Blk), b_cws = K * e->levels * e->nk * sizeof(Blk);
+    const size_t b_cwo = K * 8, b_noise = ct * 8, b_out = NN * 8;
+    const size_t in_bytes = b_roots + b_cws + b_cwo + 2 * b_noise;
+    const size_t dev_bytes = in_bytes + 2 * b_out;
+    if (!e->async_compute) PCGB_CK(cudaEventCreateWithFlags(&e->async_compute, cudaEventDisableTiming));
+    ensure_own_workspace(e);
+    auto& a = e->aslot[e->aturn];
+    e->aturn ^= 1;
+    if (!a.st) PCGB_CK(cudaStreamCreateWithFlags(&a.st, cudaStreamNonBlocking));
+    if (dev_bytes > a.bytes) {
+        PCGB_CK(cudaStreamSynchronize(a.st));
+        cudaFree(a.d_io);
+        a.d_io = nullptr;
+        PCGB_CK(cudaMalloc(&a.d_io, dev_bytes));
+        a.bytes = dev_bytes;
+    }
+    char* d = static_cast<char*>(a.d_io);
+    Blk* d_roots = reinterpret_cast<Blk*>(d);
+    Blk* d_cws = reinterpret_cast<Blk*>(d + b_roots);
+    uint64_t* d_cwo = reinterpret_cast<uint64_t*>(d + b_roots + b_cws);
+    uint64_t* d_pos = reinterpret_cast<uint64_t*>(d + b_roots + b_cws + b_cwo);
+    uint64_t* d_val = d_pos + ct;
+    uint64_t* d_x = reinterpret_cast<uint64_t*>(d + in_bytes);
+    uint64_t* d_z = d_x + NN;
+    PCGB_CK(cudaMemcpyAsync(d_roots, roots, b_roots, cudaMemcpyHostToDevice, a.st));
+    PCGB_CK(cudaMemcpyAsync(d_cws, cws, b_cws, cudaMemcpyHostToDevice, a.st));
+    PCGB_CK(cudaMemcpyAsync(d_cwo, cw_out, b_cwo, cudaMemcpyHostToDevice, a.st));
+    PCGB_CK(cudaMemcpyAsync(d_pos, pos, b_noise, cudaMemcpyHostToDevice, a.st));
+    PCGB_CK(cudaMemcpyAsync(d_val, val, b_noise, cudaMemcpyHostToDevice, a.st));
+    if (e->async_pending) PCGB_CK(cudaStreamWaitEvent(a.st, e->async_compute, 0));
+    Workspace ws;
+    ws.F = e->d_F;
+    ws.tops = e->d_tops;
+    ws.g = e->d_g;
+    expand_device_ws(e, ws, party, d_roots, d_cws, d_cwo, d_pos, d_val, d_x, d_z, a.st);
+    PCGB_CK(cudaEventRecord(e->async_compute, a.st));
+    e->async_pending = true;
+    PCGB_CK(cudaMemcpyAsync(x, d_x, b_out, cudaMemcpyDeviceToHost, a.st));
+    PCGB_CK(cudaMemcpyAsync(z, d_z, b_out, cudaMemcpyDeviceToHost, a.st));
+}
+
 void expand_host(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
                  const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val, uint64_t* x,
                  uint64_t* z) {
+    if (e->async_pending) expander_wait(e);
     cudaStream_t st = default_stream();
     const size_t K = e->K, ct = static_cast<size_t>(e->c) * e->t, NN = e->N;
     const size_t b_roots = K * sizeof(Blk), b_cws = K * e->levels * e->nk * sizeof(Blk);

@@ -166,6 +166,10 @@ void expander_destroy(pcgb_expander* e);
 void expander_info(const pcgb_expander* e, int* K, int* levels, int* nk, size_t* scratch);
 int expander_autotune(pcgb_expander* e);  // leaf shape (leaves/thread, CTA size), cached per shape
 void expander_leaf_shape(const pcgb_expander* e, int* tpb, int* leaves_per_thread);
+void expand_host_async(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
+                       const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val,
+                       uint64_t* x, uint64_t* z);
+void expander_wait(pcgb_expander* e);
 void expand_from_g_device(pcgb_expander* e, const uint64_t* g, const uint64_t* pos,
                           const uint64_t* val, uint64_t* x, uint64_t* z, cudaStream_t st);
 void expander_set_graph(pcgb_expander* e, bool on);

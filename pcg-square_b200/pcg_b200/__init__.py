@@ -114,6 +114,8 @@ def _load():
                                            C.c_int, _vp], C.c_int),
         "pcgb_expander_autotune": ([_vp, C.POINTER(C.c_int)], C.c_int),
         "pcgb_expander_leaf_shape": ([_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+        "pcgb_expand_host_async": ([_vp, C.c_int] + [_vp] * 7, C.c_int),
+        "pcgb_expander_wait": ([_vp], C.c_int),
         "pcgb_expander_stage_times": ([_vp, C.POINTER(C.c_float), C.c_int], C.c_int),
         "pcgb_launch_count": ([], C.c_ulonglong),
         "pcgb_arx_peak": ([C.POINTER(C.c_double), C.POINTER(C.c_float)], C.c_int),

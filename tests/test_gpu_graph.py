@@ -72,3 +72,27 @@ def test_autotune_keeps_outputs(pcg, N, c, t):
     got = _expand(pcg, e, d, x, z)
     assert (got[0] == want[0]).all() and (got[1] == want[1]).all()
     e.close()
+
+
+def test_async_host_expansions_match_sync(pcg):
+    """pcgb_expand_host_async over alternating parties and buffer sets equals
+    pcgb_expand_host, call for call."""
+    N, c, t = 1 << 14, 2, 8
+    s = O.shape(N, c, t)
+    a = O.public_a(s, 7)
+    e = pcg.Expander(N, c, t, 1, pcg.PRG_CHACHA8, public_a=a)
+    r0, r1, cws, cwo = O.deal_keys(s, 1234)
+    noise = [O.noise(s, 1234, p) for p in (0, 1)]
+    want = [e.expand_host(p, (r0, r1)[p], cws, cwo, *noise[p]) for p in (0, 1)]
+    bufs = []
+    for k in range(6):
+        p = k % 2
+        ins = [np.ascontiguousarray(v, np.uint64) for v in ((r0, r1)[p], cws, cwo, *noise[p])]
+        outs = [np.zeros(N, np.uint64), np.zeros(N, np.uint64)]
+        bufs.append((p, ins, outs))
+        rc = pcg.lib.pcgb_expand_host_async(e.h, p, *[v.ctypes.data for v in ins + outs])
+        assert rc == 0, pcg.lib.pcgb_last_error()
+    assert pcg.lib.pcgb_expander_wait(e.h) == 0
+    for p, _, (x, z) in bufs:
+        assert (x == want[p][0]).all() and (z == want[p][1]).all()
+    e.close()
