@@ -108,6 +108,40 @@ int pcgb_dpf_batch_full_eval_device(int B, int n, int w, const pcgb_blk* roots,
                                     pcgb_exchange_fn exchange, void* user, int prg,
                                     const pcgb_blk** d_leaves);
 
+/* ---- boolean preprocessing: two-party GMW ------------------------------
+ * The circuits in front of the interactive DPF, evaluated on the device
+ * for B instances at once: the Kogge-Stone position adder
+ * (CPU_baseline/pcg_ole_2pc/pcg_ole_impl.h:118-159 over
+ * CPU_baseline/bool_circuit/adder.h:22-63) and the DltSft circuit
+ * (HalfTreeDPF::batch_F_DeltaShiftShare, CPU_baseline/half_tree_dpf/
+ * dpf.cpp:171-283).  The reference's TripleGen (OT) is replaced by an
+ * input: boolean AND triples, bit-sliced over instances -- gates rows of
+ * W = ceil(B/32) uint32 words each (instance b = bit b%32 of word b/32),
+ * XOR shares a, b, c with (a0^a1) & (b0^b1) = c0^c1 -- consumed one row per
+ * AND gate.  Each AND depth costs one `exchange` call (party 0's message
+ * first in the reference's NetIO order is the callback's concern); messages
+ * are whole pcgb_blk, zero-padded.  The callback is required. */
+/* AND gates of the position adder (0 if off_bits is outside [1,63]). */
+size_t pcgb_gmw_position_add_gates(int off_bits);
+/* alpha = off0 + off1 as XOR shares (off_bits + 1 bits, LSB first, the top
+ * bit the carry): my_off[B] is this party's offsets (its private input),
+ * alpha_share[B] receives its share. */
+int pcgb_gmw_position_add(int party, int B, int off_bits, const uint64_t* my_off,
+                          const uint32_t* triple_a, const uint32_t* triple_b,
+                          const uint32_t* triple_c, pcgb_exchange_fn exchange, void* user,
+                          uint64_t* alpha_share);
+/* AND gates of the DltSft circuit for domain 2^n, branching 2^w (0 unless
+ * 1 <= w <= 8, w | n, n <= 64). */
+size_t pcgb_gmw_dltsft_gates(int n, int w);
+/* dltsft[B][n/w][2^w-1] shares of [digit_i(alpha) == k] * Delta, digit 0
+ * the top w bits of alpha; alpha_share[B] (n bits) and delta_share[B] are
+ * XOR shares.  delta_share is updated in place to force lsb(Delta) = 1
+ * (party 0 sets its bit 0, party 1 clears it), as the reference does. */
+int pcgb_gmw_dltsft(int party, int B, int n, int w, const uint64_t* alpha_share,
+                    pcgb_blk* delta_share, const uint32_t* triple_a, const uint32_t* triple_b,
+                    const uint32_t* triple_c, pcgb_exchange_fn exchange, void* user,
+                    pcgb_blk* dltsft);
+
 /* ---- drop-ins: output layer (GPU_baseline/common/leaf_convert_cuda.h:43-52) */
 int pcgb_dpf_out_sums(const pcgb_blk* d_leaves, int B, size_t D, uint64_t prime,
                       uint64_t* sumC_host, uint64_t* sumT_host);

@@ -327,6 +327,33 @@ int pcgb_dpf_batch_full_eval_device(int B, int n, int w, const pcgb_blk* roots,
     });
 }
 
+size_t pcgb_gmw_position_add_gates(int off_bits) { return pcgb::gmw_position_add_gates(off_bits); }
+
+int pcgb_gmw_position_add(int party, int B, int off_bits, const uint64_t* my_off,
+                          const uint32_t* triple_a, const uint32_t* triple_b,
+                          const uint32_t* triple_c, pcgb_exchange_fn exchange, void* user,
+                          uint64_t* alpha_share) {
+    if (B <= 0) return PCGB_OK;
+    return guarded([&] {
+        pcgb::gmw_position_add(party, B, off_bits, my_off, triple_a, triple_b, triple_c, exchange,
+                               user, alpha_share, pcgb::default_stream());
+    });
+}
+
+size_t pcgb_gmw_dltsft_gates(int n, int w) { return pcgb::gmw_dltsft_gates(n, w); }
+
+int pcgb_gmw_dltsft(int party, int B, int n, int w, const uint64_t* alpha_share,
+                    pcgb_blk* delta_share, const uint32_t* triple_a, const uint32_t* triple_b,
+                    const uint32_t* triple_c, pcgb_exchange_fn exchange, void* user,
+                    pcgb_blk* dltsft) {
+    if (B <= 0) return PCGB_OK;
+    return guarded([&] {
+        pcgb::gmw_dltsft(party, B, n, w, alpha_share, reinterpret_cast<Blk*>(delta_share),
+                         triple_a, triple_b, triple_c, exchange, user,
+                         reinterpret_cast<Blk*>(dltsft), pcgb::default_stream());
+    });
+}
+
 int pcgb_dpf_out_sums(const pcgb_blk* d_leaves, int B, size_t D, uint64_t prime,
                       uint64_t* sumC_host, uint64_t* sumT_host) {
     if (B <= 0) return PCGB_OK;

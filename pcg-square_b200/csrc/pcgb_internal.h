@@ -233,6 +233,16 @@ void verify_triples_device(int N, const uint64_t* a0, const uint64_t* b0, const 
                            const uint64_t* a1, const uint64_t* b1, const uint64_t* c1,
                            unsigned long long* bad, cudaStream_t st);
 
+// ---- boolean preprocessing, two-party GMW (gmw.cu) -------------------------
+size_t gmw_position_add_gates(int off_bits);
+size_t gmw_dltsft_gates(int n, int w);
+void gmw_position_add(int party, int B, int off_bits, const uint64_t* my_off, const uint32_t* ta,
+                      const uint32_t* tb, const uint32_t* tc, pcgb_exchange_fn ex, void* user,
+                      uint64_t* alpha_share, cudaStream_t st);
+void gmw_dltsft(int party, int B, int n, int w, const uint64_t* alpha_share, Blk* delta_share,
+                const uint32_t* ta, const uint32_t* tb, const uint32_t* tc, pcgb_exchange_fn ex,
+                void* user, Blk* dltsft, cudaStream_t st);
+
 }  // namespace pcgb
 
 #endif

@@ -79,6 +79,12 @@ def _load():
                                       _vp, C.c_int], C.c_int),
         "pcgb_dpf_batch_full_eval_device": ([C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, C.c_int,
                                              _vp, _vp, C.c_int, C.POINTER(_vp)], C.c_int),
+        "pcgb_gmw_position_add_gates": ([C.c_int], C.c_size_t),
+        "pcgb_gmw_position_add": ([C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+                                  C.c_int),
+        "pcgb_gmw_dltsft_gates": ([C.c_int, C.c_int], C.c_size_t),
+        "pcgb_gmw_dltsft": ([C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                             _vp], C.c_int),
         "pcgb_dpf_out_sums": ([_vp, C.c_int, C.c_size_t, C.c_uint64, _u64p, _u64p], C.c_int),
         "pcgb_dpf_out_scatter_g": ([_vp, C.c_int, C.c_size_t, C.c_int, C.c_int, C.c_uint64, _u64p,
                                     _u64p, C.c_int], C.c_int),
@@ -354,6 +360,56 @@ def dpf_gpu_batch_full_eval_device(B, n, w, roots, dltsft, round_keys=None, part
                                                C.cast(cb, C.c_void_p) if cb else None, None, prg,
                                                C.byref(d)))
     return d.value
+
+
+# ---- boolean preprocessing, two-party GMW (dpf.cpp:171-283, adder.h:22-63) --
+def gmw_position_add_gates(off_bits):
+    """AND gates (triple rows) of the Kogge-Stone position adder."""
+    return int(lib.pcgb_gmw_position_add_gates(off_bits))
+
+
+def gmw_dltsft_gates(n, w):
+    """AND gates (triple rows) of the DltSft circuit."""
+    return int(lib.pcgb_gmw_dltsft_gates(n, w))
+
+
+def _bool_triples(triples, rows, B):
+    words = rows * ((B + 31) // 32)
+    out = [np.ascontiguousarray(v, dtype=np.uint32).reshape(-1) for v in triples]
+    if len(out) != 3 or any(v.size < words for v in out):
+        raise ValueError(f"triples need 3 arrays of {words} uint32 words")
+    return out
+
+
+def gmw_position_add(party, my_off, off_bits, triples, exchange):
+    """XOR shares of alpha = off0 + off1 (off_bits + 1 bits) for B instances.
+
+    my_off: this party's B offsets; triples: (a, b, c) bit-sliced AND-triple
+    shares, gmw_position_add_gates(off_bits) rows of ceil(B/32) words;
+    exchange(my) -> peer message, as for the interactive DPF."""
+    my_off = np.ascontiguousarray(my_off, dtype=np.uint64).reshape(-1)
+    B = my_off.size
+    ta, tb, tc = _bool_triples(triples, gmw_position_add_gates(off_bits), B)
+    out = np.zeros(B, np.uint64)
+    cb = _exchange_cb(exchange)
+    _check(lib.pcgb_gmw_position_add(party, B, off_bits, _p(my_off), _p(ta), _p(tb), _p(tc),
+                                     C.cast(cb, C.c_void_p) if cb else None, None, _p(out)))
+    return out
+
+
+def gmw_dltsft(party, alpha_share, delta_share, n, w, triples, exchange):
+    """DltSft shares [B * n/w * (2^w-1), 2] of [digit_i(alpha) == k] * Delta.
+
+    Returns (delta_share with lsb(Delta) forced, dltsft)."""
+    alpha_share = np.ascontiguousarray(alpha_share, dtype=np.uint64).reshape(-1)
+    B = alpha_share.size
+    delta = _blocks(delta_share, B)[:B].copy()
+    ta, tb, tc = _bool_triples(triples, gmw_dltsft_gates(n, w), B)
+    out = np.zeros((B * (n // w) * ((1 << w) - 1), 2), np.uint64)
+    cb = _exchange_cb(exchange)
+    _check(lib.pcgb_gmw_dltsft(party, B, n, w, _p(alpha_share), _p(delta), _p(ta), _p(tb), _p(tc),
+                               C.cast(cb, C.c_void_p) if cb else None, None, _p(out)))
+    return delta, out
 
 
 # ---- output layer (leaf_convert_cuda.h:43-52) ------------------------------

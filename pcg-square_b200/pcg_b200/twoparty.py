@@ -16,10 +16,12 @@ run by each party in its own process:
 By default all c*c blocks run as one batch (see gen_and_expand), which
 leaves levels + 2 message exchanges per expansion instead of c*c*(levels+2).
 
-The preprocessing the reference draws from OT and boolean circuits
-(DltSft shares, Delta shares, beta shares, Beaver triples; pcg_ole_impl.h:
-100-200) is an input here (`PartyMaterial`); the OT layer itself is outside
-this library.  Messages travel over a `Channel`: party 0 sends first and
+The boolean part of the reference's preprocessing (pcg_ole_impl.h:118-199:
+Kogge-Stone position add, then the DltSft circuit) runs on the GPU by
+two-party GMW (`preprocess`, over pcgb_gmw_*), given AND triples.  What the
+reference draws from OT -- the AND triples, beta shares (Gilboa) and the F_p
+Beaver triples -- is an input (`PartyMaterial`, `bool_triples_dealer`); the
+OT layer itself is outside this library.  Messages travel over a `Channel`: party 0 sends first and
 party 1 receives first, as the reference's NetIO exchange does.  With
 torch.distributed the two parties may share one GPU: they exchange through
 the host between kernels and no kernel waits on the other party.
@@ -29,7 +31,12 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import (DeviceBuffer, P, PRG_CHACHA8, dpf_gpu_batch_full_eval_device, dpf_out_sums,
-               dpf_out_scatter_g_device, synchronize, to_device)
+               dpf_out_scatter_g_device, gmw_dltsft, gmw_position_add, synchronize, to_device)
+
+# The public block W both parties add to their Delta share to form the DPF
+# root (HalfTreeDPF::setup_params, dpf.cpp:289-296, draws it from a PRG with
+# a fixed seed): any constant known to both parties serves.  Hex digits of pi.
+PUBLIC_W = np.array([0x243F6A8885A308D3, 0x13198A2E03707344], np.uint64)
 
 
 @dataclass
@@ -138,3 +145,55 @@ def gen_and_expand(party, chan, expander, material, prg=PRG_CHACHA8, batched=Tru
     d_x, d_z = DeviceBuffer(8 * N), DeviceBuffer(8 * N)
     e.expand_from_g_device(d_g.ptr, d_pos.ptr, d_val.ptr, d_x.ptr, d_z.ptr)
     return d_x, d_z
+
+
+def bool_triples_dealer(rows, B, rng):
+    """Both parties' shares of `rows` bit-sliced AND triples for B instances,
+    ((a0, b0, c0), (a1, b1, c1)) with (a0^a1) & (b0^b1) == c0^c1 -- a trusted
+    dealer standing in for the reference's OT-based TripleGen in tests and
+    benchmarks (whoever runs it sees both shares)."""
+    W = (B + 31) // 32
+    a0, a1, b0, b1, c0 = (rng.integers(0, 1 << 32, rows * W, dtype=np.uint32) for _ in range(5))
+    return (a0, b0, c0), (a1, b1, ((a0 ^ a1) & (b0 ^ b1)) ^ c0)
+
+
+def instance_offsets(party, N, c, t, pos):
+    """This party's private adder input for every instance of the c*c blocks
+    (block (i, j) = i*c + j, instance k*t + l): the in-bin offset of its noise
+    position i*t + k (party 0) or j*t + l (party 1) (pcg_ole_impl.h:132-139)."""
+    bin_ = N // t
+    pos = np.asarray(pos, np.uint64)
+    blk = np.arange(c * c)[:, None]
+    idx = np.arange(t * t)[None, :]
+    sel = (blk // c) * t + idx // t if party == 0 else (blk % c) * t + idx % t
+    return (pos[sel] % np.uint64(bin_)).reshape(-1)
+
+
+def preprocess_gates(N, c, t):
+    """AND-triple rows the two circuits of `preprocess` consume:
+    (position adder, DltSft), each for c*c*t*t instances."""
+    from . import gmw_dltsft_gates, gmw_position_add_gates
+    bin_ = N // t
+    off_bits = max(1, bin_.bit_length() - 1)
+    return gmw_position_add_gates(off_bits), gmw_dltsft_gates(off_bits + 1, 1)
+
+
+def preprocess(party, chan, N, c, t, pos, delta_share, adder_triples, dltsft_triples):
+    """Boolean preprocessing of one expansion, all c*c blocks in one circuit
+    each (the reference runs both circuits per block, pcg_ole_impl.h:118-199):
+
+      alpha = off0 + off1   Kogge-Stone adder, log2(bin) + 1 bits
+      DltSft = [digit_i(alpha) == 0] * Delta   (w = 1)
+      root = Delta share ^ PUBLIC_W
+
+    delta_share: [c*c*t*t, 2] this party's random Delta shares.  Returns
+    (roots, dltsft) in PartyMaterial's layout plus the forced Delta shares and
+    the alpha shares.  Costs 1 + ceil(log2(off_bits)) + 1 exchanges."""
+    bin_ = N // t
+    off_bits = max(1, bin_.bit_length() - 1)
+    n = off_bits + 1
+    off = instance_offsets(party, N, c, t, pos)
+    alpha = gmw_position_add(party, off, off_bits, adder_triples, chan.exchange)
+    delta, dlt = gmw_dltsft(party, alpha, delta_share, n, 1, dltsft_triples, chan.exchange)
+    roots = delta ^ PUBLIC_W[None, :]
+    return (roots.reshape(c * c, t * t, 2), dlt.reshape(c * c, t * t * n, 2), delta, alpha)

@@ -65,3 +65,34 @@ def test_synthetic_material_matches_oracle():
         p_orc, v_orc = O.noise(s, 77, party)
         assert (p_lib == p_orc).all() and (v_lib == v_orc).all()
     assert (L.public_a(4096, 4, 5) == O.public_a(s, 5)).all()
+
+
+def test_gmw_gate_counts_follow_the_reference_circuits():
+    """AND gates of the two preprocessing circuits: the Kogge-Stone adder
+    (bool_circuit/adder.h:22-63: m initial generates, then 2(m - d) per
+    prefix step d = 1, 2, 4, ...) and DltSft (dpf.cpp:214-238: per level and
+    branch, a w-1 gate AND tree and 128 ANDs with Delta)."""
+    import numpy as np
+
+    import pcg_b200 as L
+    from pcg_b200 import twoparty as T
+    for m in (1, 2, 3, 5, 15, 16, 40, 63):
+        want = m + sum(2 * (m - (1 << k)) for k in range(6) if (1 << k) < m)
+        assert L.gmw_position_add_gates(m) == want, m
+    assert L.gmw_position_add_gates(0) == 0 and L.gmw_position_add_gates(64) == 0
+    for n, w in ((16, 1), (17, 1), (8, 4), (6, 2), (9, 3), (8, 8)):
+        assert L.gmw_dltsft_gates(n, w) == (n // w) * ((1 << w) - 1) * (w - 1 + 128), (n, w)
+    assert L.gmw_dltsft_gates(7, 2) == 0 and L.gmw_dltsft_gates(18, 9) == 0
+    assert T.preprocess_gates(1 << 20, 4, 16) == (114, 17 * 128)
+    # The dealer's triples hold, and the instance offsets follow the block order.
+    (a0, b0, c0), (a1, b1, c1) = T.bool_triples_dealer(7, 100, np.random.default_rng(1))
+    assert a0.size == 7 * 4 and (((a0 ^ a1) & (b0 ^ b1)) == (c0 ^ c1)).all()
+    N, c, t = 1 << 10, 2, 4
+    pos = np.array([k * (N // t) + 3 * k + i for i in range(c) for k in range(t)], np.uint64)
+    off0, off1 = T.instance_offsets(0, N, c, t, pos), T.instance_offsets(1, N, c, t, pos)
+    for blk in range(c * c):
+        ii, jj = divmod(blk, c)
+        for idx in range(t * t):
+            kk, ll = divmod(idx, t)
+            assert off0[blk * t * t + idx] == 3 * kk + ii
+            assert off1[blk * t * t + idx] == 3 * ll + jj
