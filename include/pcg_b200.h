@@ -155,6 +155,36 @@ int pcgb_dpf_out_scatter_g(const pcgb_blk* d_leaves, int B, size_t D, int t, int
 int pcgb_dpf_out_scatter_g_device(const pcgb_blk* d_leaves, int B, size_t D, int t, int party,
                                   const uint64_t* d_cw, uint64_t* d_g, int N, void* stream);
 
+/* Output layer hashing each leaf once (no reference counterpart; the pair
+ * replaces dpf_out_sums + dpf_out_scatter_g, leaf_convert_cuda.h:43-52, for
+ * callers that run both on the same leaves).  The sums pass also stores each
+ * leaf's converted word C | tau << 63 in d_conv[B][D] (8 bytes per leaf),
+ * and the scatter reads those words instead of hashing the leaves again.
+ * Sums and g are as the drop-ins give them, bit for bit.  Device pointers,
+ * ordered on `stream`. */
+int pcgb_dpf_out_convert_device(const pcgb_blk* d_leaves, int B, size_t D, uint64_t* d_conv,
+                                uint64_t* d_sumC, uint64_t* d_sumT, void* stream);
+int pcgb_dpf_out_scatter_g_conv_device(const uint64_t* d_conv, int B, size_t D, int t, int party,
+                                       const uint64_t* d_cw, uint64_t* d_g, int N, void* stream);
+
+/* The output-layer Beaver multiplication of the two-party expansion
+ * (CPU_baseline/pcg_ole_2pc/pcg_ole_impl.h:222-290) on device arrays of B
+ * words.  Open: <A> = (-1)^party sumT, <B> = (-1)^(1-party) sumC + <beta>;
+ * d_de[0..B) = <A> - r, d_de[B..2B) = <B> - s (mod p), the message to send.
+ * Close, with the peer's message: d = d0 + d1, e = e0 + e1, the CW share is
+ * d*s + e*r + rs, plus d*e for party 0.  CW = the sum of the two shares
+ * (pcgb_add_mod_p_device). */
+int pcgb_out_beaver_open_device(int B, int party, const uint64_t* d_sumC, const uint64_t* d_sumT,
+                                const uint64_t* d_beta, const uint64_t* d_r, const uint64_t* d_s,
+                                uint64_t* d_de, void* stream);
+int pcgb_out_beaver_close_device(int B, int party, const uint64_t* d_de_my,
+                                 const uint64_t* d_de_peer, const uint64_t* d_r,
+                                 const uint64_t* d_s, const uint64_t* d_rs, uint64_t* d_cw_share,
+                                 void* stream);
+/* d[i] = (u[i] + v[i]) mod p for any 64-bit u, v (d may alias either). */
+int pcgb_add_mod_p_device(uint64_t* d, const uint64_t* u, const uint64_t* v, size_t count,
+                          void* stream);
+
 /* Allocation-free variant of pcgb_dpf_out_sums, with no counterpart in the
  * reference.  It is for callers that must not allocate device memory
  * themselves or through the library: code whose device memory is owned by a

@@ -44,8 +44,11 @@ def _party(party, port, N, c, t, mat, iters, q, batched, gmw):
             r=mat["r"][party], s=mat["s"][party], rs=mat["rs"][party],
             pos=mat["noise"][party][0], val=mat["noise"][party][1])
         times, pre = [], []
+        d_x = d_z = None
         for it in range(iters + 1):
             chan = twoparty.Channel(party)
+            del d_x, d_z              # the previous outputs, freed before the clock starts
+            L.synchronize()
             dist.barrier()
             t0 = time.perf_counter()
             if gmw:

@@ -28,6 +28,16 @@ void dpf_out_scatter_device(const Blk* d_leaves, int B, size_t D, int t, int par
 void aes_ecb_encrypt_device(const uint8_t* keys, const uint8_t* in, uint8_t* out, int count);
 void dpf_out_sums_noalloc(const Blk* d_leaves, int B, size_t D, uint64_t prime, uint64_t* d_sumC,
                           uint64_t* d_sumT, cudaStream_t st);
+void dpf_out_convert_device(const Blk* d_leaves, int B, size_t D, uint64_t* d_conv,
+                            uint64_t* d_sumC, uint64_t* d_sumT, cudaStream_t st);
+void dpf_out_scatter_conv_device(const uint64_t* d_conv, int B, size_t D, int t, int party,
+                                 const uint64_t* d_cw, uint64_t* d_g, int N, cudaStream_t st);
+void out_beaver_open_device(int B, int party, const uint64_t* d_sumC, const uint64_t* d_sumT,
+                            const uint64_t* d_beta, const uint64_t* d_r, const uint64_t* d_s,
+                            uint64_t* d_de, cudaStream_t st);
+void out_beaver_close_device(int B, int party, const uint64_t* d_de_my, const uint64_t* d_de_peer,
+                             const uint64_t* d_r, const uint64_t* d_s, const uint64_t* d_rs,
+                             uint64_t* d_cw, cudaStream_t st);
 void expander_destroy(pcgb_expander* e);
 void expand_device(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
                    const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val, uint64_t* x,
@@ -390,6 +400,43 @@ int pcgb_dpf_out_sums_noalloc(const pcgb_blk* d_leaves, int B, size_t D, uint64_
     });
 }
 
+int pcgb_dpf_out_convert_device(const pcgb_blk* d_leaves, int B, size_t D, uint64_t* d_conv,
+                                uint64_t* d_sumC, uint64_t* d_sumT, void* stream) {
+    if (B <= 0) return PCGB_OK;
+    return guarded([&] {
+        pcgb::dpf_out_convert_device(reinterpret_cast<const Blk*>(d_leaves), B, D, d_conv, d_sumC,
+                                     d_sumT, pcgb::as_stream(stream));
+    });
+}
+
+int pcgb_dpf_out_scatter_g_conv_device(const uint64_t* d_conv, int B, size_t D, int t, int party,
+                                       const uint64_t* d_cw, uint64_t* d_g, int N, void* stream) {
+    if (B <= 0) return PCGB_OK;
+    return guarded([&] {
+        pcgb::dpf_out_scatter_conv_device(d_conv, B, D, t, party, d_cw, d_g, N,
+                                          pcgb::as_stream(stream));
+    });
+}
+
+int pcgb_out_beaver_open_device(int B, int party, const uint64_t* d_sumC, const uint64_t* d_sumT,
+                                const uint64_t* d_beta, const uint64_t* d_r, const uint64_t* d_s,
+                                uint64_t* d_de, void* stream) {
+    return guarded([&] {
+        pcgb::out_beaver_open_device(B, party, d_sumC, d_sumT, d_beta, d_r, d_s, d_de,
+                                     pcgb::as_stream(stream));
+    });
+}
+
+int pcgb_out_beaver_close_device(int B, int party, const uint64_t* d_de_my,
+                                 const uint64_t* d_de_peer, const uint64_t* d_r,
+                                 const uint64_t* d_s, const uint64_t* d_rs, uint64_t* d_cw_share,
+                                 void* stream) {
+    return guarded([&] {
+        pcgb::out_beaver_close_device(B, party, d_de_my, d_de_peer, d_r, d_s, d_rs, d_cw_share,
+                                      pcgb::as_stream(stream));
+    });
+}
+
 // ---- poly-mul drop-ins --------------------------------------------------
 int pcgb_poly_mul_supported(int variant, uint64_t prime, int N, char* reason, size_t len) {
     std::string r;
@@ -589,6 +636,14 @@ int pcgb_reduce_mod_p(uint64_t* d, const uint64_t* s, size_t count, void* stream
     return guarded([&] {
         if (count && (!d || !s)) pcgb::fail(PCGB_EINVAL, "reduce_mod_p: null pointer");
         if (count) pcgb::reduce_mod_p(d, s, count, pcgb::as_stream(stream));
+    });
+}
+
+int pcgb_add_mod_p_device(uint64_t* d, const uint64_t* u, const uint64_t* v, size_t count,
+                          void* stream) {
+    return guarded([&] {
+        if (count && (!d || !u || !v)) pcgb::fail(PCGB_EINVAL, "add_mod_p: null pointer");
+        if (count) pcgb::add_mod_p_device(d, u, v, count, pcgb::as_stream(stream));
     });
 }
 

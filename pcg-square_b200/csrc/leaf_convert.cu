@@ -11,6 +11,18 @@
 // most 2t) instances whose shifted leaf ranges cover it, so every word is
 // produced once without atomics (the reference resolves overlaps with a
 // CAS-loop modular atomic, leaf_convert_cuda.cu:68-77,207-234).
+//
+// The drop-ins hash every leaf in both passes, as the reference does
+// (leaf_convert_cuda.h:47-49 judges that cheaper than keeping B*D values).
+// On B200 the hash is the bound (341 integer ops per 16-byte leaf) and HBM
+// is not, so the convert/scatter-conv pair keeps each leaf's converted word
+// C | tau << 63 (C < p < 2^62) from the sums pass, and the scatter reads 8
+// bytes per leaf instead of hashing 16 again.
+//
+// The two-party expansion's output-layer Beaver multiplication
+// (pcg_ole_impl.h:222-290) also runs here, on device-resident sums:
+//   <A> = (-1)^party sumT, <B> = (-1)^(1-party) sumC + <beta>
+//   open d = <A> - r, e = <B> - s;  <CW> = d*s + e*r + rs (+ d*e, party 0).
 #include "pcgb_internal.h"
 
 #include <algorithm>
@@ -30,9 +42,14 @@ __device__ __forceinline__ uint64_t leaf_C(const ulonglong2& v) {
     return reduce_p(out_hash_lo64(v.x, v.y));
 }
 
+constexpr uint64_t kTauBit = uint64_t{1} << 63;
+
 // grid = (parts, B): partials[b*parts + part] (C lane), [B*parts + ...] (T lane).
+// KEEP: also write conv[b*D + d] = C | tau << 63.
+template <bool KEEP>
 __global__ void __launch_bounds__(kTPB) out_sum_kernel(const ulonglong2* __restrict__ leaves,
-                                                       size_t D, uint64_t* __restrict__ partials) {
+                                                       size_t D, uint64_t* __restrict__ partials,
+                                                       uint64_t* __restrict__ conv) {
     __shared__ uint64_t sc[kTPB / 32], stt[kTPB / 32];
     const int b = blockIdx.y, parts = gridDim.x;
     const ulonglong2* L = leaves + static_cast<size_t>(b) * D;
@@ -40,8 +57,10 @@ __global__ void __launch_bounds__(kTPB) out_sum_kernel(const ulonglong2* __restr
     for (size_t d = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; d < D;
          d += static_cast<size_t>(parts) * blockDim.x) {
         const ulonglong2 v = __ldg(L + d);
-        c = add_p(c, leaf_C(v));
+        const uint64_t C = leaf_C(v);
+        c = add_p(c, C);
         t += v.x & 1;
+        if (KEEP) conv[static_cast<size_t>(b) * D + d] = C | (v.x << 63);
     }
 #pragma unroll
     for (int off = 16; off; off >>= 1) {
@@ -73,8 +92,22 @@ __global__ void out_fold_kernel(const uint64_t* __restrict__ partials, int parts
     sums[B + b] = t;
 }
 
+// y = C + tau*CW of one leaf, from the leaf itself (hashed) or from its
+// converted word.
+__device__ __forceinline__ uint64_t leaf_y(const ulonglong2* leaves, size_t i, uint64_t cw) {
+    const ulonglong2 v = __ldg(leaves + i);
+    const uint64_t y = leaf_C(v);
+    return (v.x & 1) ? add_p(y, cw) : y;
+}
+__device__ __forceinline__ uint64_t leaf_y(const uint64_t* conv, size_t i, uint64_t cw) {
+    const uint64_t w = __ldg(conv + i);
+    const uint64_t y = w & ~kTauBit;
+    return (w & kTauBit) ? add_p(y, cw) : y;
+}
+
 // Gather scatter: thread per output word p < N.
-__global__ void __launch_bounds__(kTPB) out_gather_kernel(const ulonglong2* __restrict__ leaves,
+template <class In>
+__global__ void __launch_bounds__(kTPB) out_gather_kernel(const In* __restrict__ leaves,
                                                           int B, size_t D, int t, int party,
                                                           const uint64_t* __restrict__ cws,
                                                           uint64_t* __restrict__ g, size_t N) {
@@ -96,15 +129,48 @@ __global__ void __launch_bounds__(kTPB) out_gather_kernel(const ulonglong2* __re
             for (int kk = kk0; kk <= kk1; ++kk) {
                 const int b = kk * t + static_cast<int>(s - kk);
                 if (b >= B) continue;
-                const ulonglong2 v = __ldg(leaves + static_cast<size_t>(b) * D + d);
-                uint64_t y = leaf_C(v);
-                if (v.x & 1) y = add_p(y, __ldg(cws + b));
+                uint64_t y = leaf_y(leaves, static_cast<size_t>(b) * D + d, __ldg(cws + b));
                 if ((party != 0) != (f != 0)) y = neg_p(y);
                 acc = add_p(acc, y);
             }
         }
     }
     g[p] = acc;
+}
+
+__global__ void beaver_open_kernel(int B, int party, const uint64_t* __restrict__ sumC,
+                                   const uint64_t* __restrict__ sumT,
+                                   const uint64_t* __restrict__ beta,
+                                   const uint64_t* __restrict__ r, const uint64_t* __restrict__ s,
+                                   uint64_t* __restrict__ de) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    uint64_t A = reduce_p(sumT[b]), Bs = reduce_p(sumC[b]);
+    if (party) A = neg_p(A);
+    else Bs = neg_p(Bs);
+    Bs = add_p(Bs, reduce_p(beta[b]));
+    de[b] = sub_p(A, reduce_p(r[b]));
+    de[B + b] = sub_p(Bs, reduce_p(s[b]));
+}
+
+// a*b mod p for a, b < p: two Montgomery products, the second by R^2.
+__device__ __forceinline__ uint64_t mul_p(uint64_t a, uint64_t b, uint64_t r2) {
+    return mont_mul(mont_mul(a, b), r2);
+}
+
+__global__ void beaver_close_kernel(int B, int party, const uint64_t* __restrict__ de_my,
+                                    const uint64_t* __restrict__ de_peer,
+                                    const uint64_t* __restrict__ r, const uint64_t* __restrict__ s,
+                                    const uint64_t* __restrict__ rs, uint64_t r2,
+                                    uint64_t* __restrict__ cw) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    const uint64_t d = add_p(reduce_p(de_my[b]), reduce_p(de_peer[b]));
+    const uint64_t e = add_p(reduce_p(de_my[B + b]), reduce_p(de_peer[B + b]));
+    uint64_t v = add_p(mul_p(d, reduce_p(s[b]), r2), mul_p(e, reduce_p(r[b]), r2));
+    v = add_p(v, reduce_p(rs[b]));
+    if (party == 0) v = add_p(v, mul_p(d, e, r2));
+    cw[b] = v;
 }
 
 struct ConvPool {
@@ -156,8 +222,8 @@ int out_sums_parts(size_t D) {
 void out_sums_launch(const Blk* d_leaves, int B, size_t D, uint64_t* partials, uint64_t* sums,
                      cudaStream_t st) {
     const int parts = out_sums_parts(D);
-    out_sum_kernel<<<dim3(parts, B), kTPB, 0, st>>>(reinterpret_cast<const ulonglong2*>(d_leaves),
-                                                    D, partials);
+    out_sum_kernel<false><<<dim3(parts, B), kTPB, 0, st>>>(
+        reinterpret_cast<const ulonglong2*>(d_leaves), D, partials, nullptr);
     PCGB_POST_LAUNCH();
     out_fold_kernel<<<(B + 127) / 128, 128, 0, st>>>(partials, parts, B, sums);
     PCGB_POST_LAUNCH();
@@ -165,7 +231,7 @@ void out_sums_launch(const Blk* d_leaves, int B, size_t D, uint64_t* partials, u
 
 void out_gather_launch(const Blk* d_leaves, int B, size_t D, int t, int party,
                        const uint64_t* d_cws, uint64_t* d_g, size_t N, cudaStream_t st) {
-    out_gather_kernel<<<static_cast<unsigned>((N + kTPB - 1) / kTPB), kTPB, 0, st>>>(
+    out_gather_kernel<ulonglong2><<<static_cast<unsigned>((N + kTPB - 1) / kTPB), kTPB, 0, st>>>(
         reinterpret_cast<const ulonglong2*>(d_leaves), B, D, t, party, d_cws, d_g, N);
     PCGB_POST_LAUNCH();
 }
@@ -246,8 +312,8 @@ void dpf_out_sums_noalloc(const Blk* d_leaves, int B, size_t D, uint64_t prime, 
     const size_t fit = kNoAllocScratchWords / (2 * static_cast<size_t>(B));
     const int parts = static_cast<int>(std::min<size_t>(out_sums_parts(D), fit));
     uint64_t* partials = noalloc_partials();
-    out_sum_kernel<<<dim3(parts, B), kTPB, 0, st>>>(reinterpret_cast<const ulonglong2*>(d_leaves),
-                                                    D, partials);
+    out_sum_kernel<false><<<dim3(parts, B), kTPB, 0, st>>>(
+        reinterpret_cast<const ulonglong2*>(d_leaves), D, partials, nullptr);
     PCGB_POST_LAUNCH();
     out_fold_split_kernel<<<(B + 127) / 128, 128, 0, st>>>(partials, parts, B, d_sumC, d_sumT);
     PCGB_POST_LAUNCH();
@@ -291,6 +357,61 @@ void dpf_out_scatter_device(const Blk* d_leaves, int B, size_t D, int t, int par
     if ((s_max + 2) * bin > 2 * static_cast<size_t>(N))
         fail(PCGB_EINVAL, "dpf_out_scatter_g_device: N smaller than the instances' span");
     out_gather_launch(d_leaves, B, D, t, party, d_cw, d_g, static_cast<size_t>(N), st);
+}
+
+void dpf_out_convert_device(const Blk* d_leaves, int B, size_t D, uint64_t* d_conv,
+                            uint64_t* d_sumC, uint64_t* d_sumT, cudaStream_t st) {
+    if (B <= 0) return;
+    check_common(d_leaves, B, D, kP);
+    if (!d_conv || !d_sumC || !d_sumT) fail(PCGB_EINVAL, "dpf_out_convert_device: null pointer");
+    const int parts = out_sums_parts(D);
+    uint64_t* partials =
+        static_cast<uint64_t*>(pool_alloc(2 * static_cast<size_t>(B) * parts * sizeof(uint64_t), st));
+    out_sum_kernel<true><<<dim3(parts, B), kTPB, 0, st>>>(
+        reinterpret_cast<const ulonglong2*>(d_leaves), D, partials, d_conv);
+    PCGB_POST_LAUNCH();
+    out_fold_split_kernel<<<(B + 127) / 128, 128, 0, st>>>(partials, parts, B, d_sumC, d_sumT);
+    PCGB_POST_LAUNCH();
+    PCGB_CK(cudaFreeAsync(partials, st));
+}
+
+void dpf_out_scatter_conv_device(const uint64_t* d_conv, int B, size_t D, int t, int party,
+                                 const uint64_t* d_cw, uint64_t* d_g, int N, cudaStream_t st) {
+    if (B <= 0) return;
+    check_common(d_conv, B, D, kP);
+    if (!d_cw || !d_g) fail(PCGB_EINVAL, "dpf_out_scatter_g_conv_device: null pointer");
+    if (t <= 0 || N <= 0) fail(PCGB_EINVAL, "dpf_out_scatter_g_conv_device: t and N must be positive");
+    const size_t bin = D >> 1;
+    const size_t s_max = static_cast<size_t>((B - 1) / t) + t - 1;
+    if ((s_max + 2) * bin > 2 * static_cast<size_t>(N))
+        fail(PCGB_EINVAL, "dpf_out_scatter_g_conv_device: N smaller than the instances' span");
+    out_gather_kernel<uint64_t><<<static_cast<unsigned>((N + kTPB - 1) / kTPB), kTPB, 0, st>>>(
+        d_conv, B, D, t, party, d_cw, d_g, static_cast<size_t>(N));
+    PCGB_POST_LAUNCH();
+}
+
+void out_beaver_open_device(int B, int party, const uint64_t* d_sumC, const uint64_t* d_sumT,
+                            const uint64_t* d_beta, const uint64_t* d_r, const uint64_t* d_s,
+                            uint64_t* d_de, cudaStream_t st) {
+    if (B <= 0) return;
+    if (party != 0 && party != 1) fail(PCGB_EINVAL, "out_beaver_open: party must be 0 or 1");
+    if (!d_sumC || !d_sumT || !d_beta || !d_r || !d_s || !d_de)
+        fail(PCGB_EINVAL, "out_beaver_open: null pointer");
+    beaver_open_kernel<<<(B + 255) / 256, 256, 0, st>>>(B, party, d_sumC, d_sumT, d_beta, d_r, d_s,
+                                                        d_de);
+    PCGB_POST_LAUNCH();
+}
+
+void out_beaver_close_device(int B, int party, const uint64_t* d_de_my, const uint64_t* d_de_peer,
+                             const uint64_t* d_r, const uint64_t* d_s, const uint64_t* d_rs,
+                             uint64_t* d_cw, cudaStream_t st) {
+    if (B <= 0) return;
+    if (party != 0 && party != 1) fail(PCGB_EINVAL, "out_beaver_close: party must be 0 or 1");
+    if (!d_de_my || !d_de_peer || !d_r || !d_s || !d_rs || !d_cw)
+        fail(PCGB_EINVAL, "out_beaver_close: null pointer");
+    beaver_close_kernel<<<(B + 255) / 256, 256, 0, st>>>(B, party, d_de_my, d_de_peer, d_r, d_s,
+                                                         d_rs, r2_mod_p(), d_cw);
+    PCGB_POST_LAUNCH();
 }
 
 }  // namespace pcgb

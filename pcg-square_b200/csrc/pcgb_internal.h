@@ -225,6 +225,9 @@ void pointwise_mul(uint64_t* c, const uint64_t* a, const uint64_t* b, size_t cou
 void reduce_mod_p(uint64_t* d, const uint64_t* s, size_t count, cudaStream_t st);
 
 // ---- triples and relation checks (triples.cu) ----------------------------
+// d = (u + v) mod p for any 64-bit u, v.
+void add_mod_p_device(uint64_t* d, const uint64_t* u, const uint64_t* v, size_t count,
+                      cudaStream_t st);
 void triples_device(int N, int party, const uint64_t* x1, const uint64_t* z1, const uint64_t* x2,
                     const uint64_t* z2, uint64_t* a, uint64_t* b, uint64_t* c, cudaStream_t st);
 void verify_ole_device(int N, const uint64_t* x0, const uint64_t* z0, const uint64_t* x1,

@@ -92,6 +92,12 @@ int log2_checked(int N, const char* what) {
 
 }  // namespace
 
+void add_mod_p_device(uint64_t* d, const uint64_t* u, const uint64_t* v, size_t count,
+                      cudaStream_t st) {
+    add_reduce_kernel<<<grid_for(count), kTpb, 0, st>>>(d, u, v, count);
+    PCGB_POST_LAUNCH();
+}
+
 void triples_device(int N, int party, const uint64_t* x1, const uint64_t* z1, const uint64_t* x2,
                     const uint64_t* z2, uint64_t* a, uint64_t* b, uint64_t* c, cudaStream_t st) {
     if (party != 0 && party != 1) fail(PCGB_EINVAL, "triples: party must be 0 or 1");

@@ -85,6 +85,12 @@ def _load():
         "pcgb_gmw_dltsft_gates": ([C.c_int, C.c_int], C.c_size_t),
         "pcgb_gmw_dltsft": ([C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                              _vp], C.c_int),
+        "pcgb_dpf_out_convert_device": ([_vp, C.c_int, C.c_size_t, _vp, _vp, _vp, _vp], C.c_int),
+        "pcgb_dpf_out_scatter_g_conv_device": ([_vp, C.c_int, C.c_size_t, C.c_int, C.c_int, _vp,
+                                                _vp, C.c_int, _vp], C.c_int),
+        "pcgb_out_beaver_open_device": ([C.c_int, C.c_int] + [_vp] * 6 + [_vp], C.c_int),
+        "pcgb_out_beaver_close_device": ([C.c_int, C.c_int] + [_vp] * 6 + [_vp], C.c_int),
+        "pcgb_add_mod_p_device": ([_vp, _vp, _vp, C.c_size_t, _vp], C.c_int),
         "pcgb_dpf_out_sums": ([_vp, C.c_int, C.c_size_t, C.c_uint64, _u64p, _u64p], C.c_int),
         "pcgb_dpf_out_scatter_g": ([_vp, C.c_int, C.c_size_t, C.c_int, C.c_int, C.c_uint64, _u64p,
                                     _u64p, C.c_int], C.c_int),
@@ -423,6 +429,34 @@ def dpf_out_sums(d_leaves, B, D, prime=P):
 def dpf_out_scatter_g_device(d_leaves, B, D, t, party, d_cw, d_g, N, stream=None):
     """Folded g of the B instances into device d_g; CWs on the device."""
     _check(lib.pcgb_dpf_out_scatter_g_device(d_leaves, B, D, t, party, d_cw, d_g, N, stream))
+
+
+def dpf_out_convert_device(d_leaves, B, D, d_conv, d_sumC, d_sumT, stream=None):
+    """Sums of the B instances into device d_sumC/d_sumT and each leaf's
+    converted word C | tau << 63 into d_conv (B*D words)."""
+    _check(lib.pcgb_dpf_out_convert_device(d_leaves, B, D, d_conv, d_sumC, d_sumT, stream))
+
+
+def dpf_out_scatter_g_conv_device(d_conv, B, D, t, party, d_cw, d_g, N, stream=None):
+    """Folded g from the converted words of dpf_out_convert_device."""
+    _check(lib.pcgb_dpf_out_scatter_g_conv_device(d_conv, B, D, t, party, d_cw, d_g, N, stream))
+
+
+def out_beaver_open_device(B, party, d_sumC, d_sumT, d_beta, d_r, d_s, d_de, stream=None):
+    """This party's Beaver opening [<A> - r | <B> - s] (2B words) into d_de."""
+    _check(lib.pcgb_out_beaver_open_device(B, party, d_sumC, d_sumT, d_beta, d_r, d_s, d_de,
+                                           stream))
+
+
+def out_beaver_close_device(B, party, d_de_my, d_de_peer, d_r, d_s, d_rs, d_cw, stream=None):
+    """This party's share of CW = A*B from both openings."""
+    _check(lib.pcgb_out_beaver_close_device(B, party, d_de_my, d_de_peer, d_r, d_s, d_rs, d_cw,
+                                            stream))
+
+
+def add_mod_p_device(d, u, v, count, stream=None):
+    """d = (u + v) mod p over `count` device words."""
+    _check(lib.pcgb_add_mod_p_device(d, u, v, count, stream))
 
 
 def dpf_out_scatter_g(d_leaves, B, D, t, party, CW, N, prime=P):

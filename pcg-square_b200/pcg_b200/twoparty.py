@@ -6,11 +6,12 @@ run by each party in its own process:
 
   for every block (i, j):
     leaves = dpf_gpu_batch_full_eval_device(...)   one CW exchange per level
-    sumC, sumT = dpf_out_sums(leaves)
+    sumC, sumT = dpf_out_sums(leaves)              (pcgb_dpf_out_convert_device,
+                                                    which keeps C | tau<<63 per leaf)
     <A> = (-1)^party sumT, <B> = (-1)^(1-party) sumC + <beta>
-    open d = A - r, e = B - s                      Beaver triple (r, s, rs)
-    <CW> = d<s> + e<r> + <rs> (+ d e for party 0); open CW
-    g_ij = dpf_out_scatter_g(leaves, ..., CW)
+    open d = A - r, e = B - s                      Beaver triple (r, s, rs), on
+    <CW> = d<s> + e<r> + <rs> (+ d e for party 0);  the device; open CW
+    g_ij = dpf_out_scatter_g(leaves, ..., CW)      (from the kept words)
   x, z = step 4 over the g_ij (pcgb_expand_from_g_device)
 
 By default all c*c blocks run as one batch (see gen_and_expand), which
@@ -21,8 +22,9 @@ Kogge-Stone position add, then the DltSft circuit) runs on the GPU by
 two-party GMW (`preprocess`, over pcgb_gmw_*), given AND triples.  What the
 reference draws from OT -- the AND triples, beta shares (Gilboa) and the F_p
 Beaver triples -- is an input (`PartyMaterial`, `bool_triples_dealer`); the
-OT layer itself is outside this library.  Messages travel over a `Channel`: party 0 sends first and
-party 1 receives first, as the reference's NetIO exchange does.  With
+OT layer itself is outside this library.  Messages travel over a
+`Channel`: party 0 sends first and party 1 receives first, as the
+reference's NetIO exchange does.  With
 torch.distributed the two parties may share one GPU: they exchange through
 the host between kernels and no kernel waits on the other party.
 """
@@ -30,8 +32,10 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import (DeviceBuffer, P, PRG_CHACHA8, dpf_gpu_batch_full_eval_device, dpf_out_sums,
-               dpf_out_scatter_g_device, gmw_dltsft, gmw_position_add, synchronize, to_device)
+from . import (DeviceBuffer, PRG_CHACHA8, add_mod_p_device, dpf_gpu_batch_full_eval_device,
+               dpf_out_convert_device, dpf_out_scatter_g_conv_device, gmw_dltsft,
+               gmw_position_add, out_beaver_close_device, out_beaver_open_device, synchronize,
+               to_device)
 
 # The public block W both parties add to their Delta share to form the DPF
 # root (HalfTreeDPF::setup_params, dpf.cpp:289-296, draws it from a PRG with
@@ -88,27 +92,39 @@ class Channel:
         return t_peer.numpy().view(np.uint64).reshape(mine.shape)
 
 
-def _beaver_cw(party, chan, sumC, sumT, beta, r, s, rs):
-    """Output-layer correction words of a batch of instances: <A> =
+# Device scratch reused across calls in this process (the converted leaf
+# words alone are 8 bytes per leaf: 4.3 GB at N = 2^20, c = 4, t = 16).
+_scratch = {}
+
+
+def _scratch_buf(name, nbytes):
+    b = _scratch.get(name)
+    if b is None or b.nbytes < nbytes:
+        if b is not None:
+            b.free()
+        b = _scratch[name] = DeviceBuffer(nbytes)
+    return b
+
+
+def _beaver_cw_device(party, chan, nB, d_sumC, d_sumT, beta, r, s, rs, d_cw):
+    """Output-layer correction words of nB instances into d_cw (a
+    DeviceBuffer of nB words): <A> =
     (-1)^party sumT, <B> = (-1)^(1-party) sumC + <beta>, CW = A*B by one
-    Beaver triple per instance (two opens; pcg_ole_impl.h:222-290)."""
-    A = [(P - int(v) % P) % P if party == 1 else int(v) % P for v in sumT]
-    Bsh = [((P - int(v)) % P if party == 0 else int(v)) for v in sumC]
-    Bsh = [(b + int(x)) % P for b, x in zip(Bsh, beta)]
-    n = len(A)
-    de_my = np.array([(a - int(x)) % P for a, x in zip(A, r)] +
-                     [(b - int(x)) % P for b, x in zip(Bsh, s)], np.uint64)
-    de_peer = chan.exchange(de_my)
-    cw_my = np.empty(n, np.uint64)
-    for k in range(n):
-        d = (int(de_my[k]) + int(de_peer[k])) % P
-        e = (int(de_my[n + k]) + int(de_peer[n + k])) % P
-        v = (d * int(s[k]) + e * int(r[k]) + int(rs[k])) % P
-        if party == 0:
-            v = (v + d * e) % P
-        cw_my[k] = v
-    cw_peer = chan.exchange(cw_my)
-    return np.array([(int(a) + int(b)) % P for a, b in zip(cw_my, cw_peer)], np.uint64)
+    Beaver triple per instance (two opens; pcg_ole_impl.h:222-290).  The
+    arithmetic runs on the device; only the 2nB + nB words of the two
+    openings cross to the host for the exchange."""
+    w = 8 * nB
+    d_in = _scratch_buf("beaver_in", 4 * w)          # beta | r | s | rs
+    for k, a in enumerate((beta, r, s, rs)):
+        d_in.upload_at(np.ascontiguousarray(a, np.uint64), k * w)
+    d_beta, d_r, d_s, d_rs = (d_in.ptr + k * w for k in range(4))
+    d_de = _scratch_buf("beaver_de", 4 * w)          # mine (2nB) | peer (2nB)
+    out_beaver_open_device(nB, party, d_sumC, d_sumT, d_beta, d_r, d_s, d_de.ptr)
+    peer = chan.exchange(d_de.download(np.uint64, 2 * nB))
+    d_de.upload_at(peer, 2 * w)
+    out_beaver_close_device(nB, party, d_de.ptr, d_de.ptr + 2 * w, d_r, d_s, d_rs, d_cw.ptr)
+    d_peer = _scratch_buf("beaver_cw_peer", w).upload(chan.exchange(d_cw.download(np.uint64, nB)))
+    add_mod_p_device(d_cw.ptr, d_cw.ptr, d_peer.ptr, nB)
 
 
 def gen_and_expand(party, chan, expander, material, prg=PRG_CHACHA8, batched=True):
@@ -119,7 +135,9 @@ def gen_and_expand(party, chan, expander, material, prg=PRG_CHACHA8, batched=Tru
     blocks' t*t keys as one batch of c*c*t*t instances -- levels + 2 message
     exchanges in all -- where the reference runs block by block
     (c*c*(levels + 2) exchanges; batched=False does the same).  Both parties
-    must use the same mode.  The output layers stay on the device."""
+    must use the same mode.  Everything but the messages stays on the
+    device: the sums pass keeps each leaf's converted word, so the scatter
+    after the Beaver opens hashes no leaf a second time."""
     e = expander
     N, c, t = e.N, e.c, e.t
     B, n = t * t, e.levels
@@ -129,17 +147,22 @@ def gen_and_expand(party, chan, expander, material, prg=PRG_CHACHA8, batched=Tru
     groups = [list(range(c * c))] if batched else [[blk] for blk in range(c * c)]
     for blocks in groups:
         nb = len(blocks)
+        nB = nb * B
         roots = np.ascontiguousarray(np.concatenate([m.roots[b] for b in blocks]))
         dlt = np.ascontiguousarray(np.concatenate([m.dltsft[b] for b in blocks]))
-        d_leaves = dpf_gpu_batch_full_eval_device(nb * B, n, 1, roots, dlt, party=party,
+        d_leaves = dpf_gpu_batch_full_eval_device(nB, n, 1, roots, dlt, party=party,
                                                   exchange=chan.exchange, prg=prg)
-        sumC, sumT = dpf_out_sums(d_leaves, nb * B, D)
+        d_conv = _scratch_buf("conv", 8 * nB * D)
+        d_sums = _scratch_buf("sums", 2 * 8 * nB)     # sumC | sumT
+        d_sumC, d_sumT = d_sums.ptr, d_sums.ptr + 8 * nB
+        d_cw = _scratch_buf("cw", 8 * nB)
+        dpf_out_convert_device(d_leaves, nB, D, d_conv.ptr, d_sumC, d_sumT)
         cat = lambda a: np.concatenate([a[b] for b in blocks])
-        CW = _beaver_cw(party, chan, sumC, sumT, cat(m.beta), cat(m.r), cat(m.s), cat(m.rs))
-        d_cw = to_device(CW)
+        _beaver_cw_device(party, chan, nB, d_sumC, d_sumT, cat(m.beta), cat(m.r), cat(m.s),
+                          cat(m.rs), d_cw)
         for k, blk in enumerate(blocks):
-            dpf_out_scatter_g_device(d_leaves + 16 * k * B * D, B, D, t, party,
-                                     d_cw.ptr + 8 * k * B, d_g.ptr + 8 * blk * N, N)
+            dpf_out_scatter_g_conv_device(d_conv.ptr + 8 * k * B * D, B, D, t, party,
+                                          d_cw.ptr + 8 * k * B, d_g.ptr + 8 * blk * N, N)
         synchronize()   # d_leaves is valid until the next DPF call
     d_pos, d_val = to_device(m.pos), to_device(m.val)
     d_x, d_z = DeviceBuffer(8 * N), DeviceBuffer(8 * N)
