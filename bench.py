@@ -134,6 +134,9 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=200,
                     help="seeded subsample of the serving stream (0 = skip)")
     # Smaller shapes for profiler captures; the bench line is quoted at the defaults.
+    ap.add_argument("--leaf-shape", default=None,
+                    help="pin the leaf kernel to THREADSxLEAVES (e.g. 128x8) instead of "
+                         "autotuning it (profiler captures need one fixed shape)")
     ap.add_argument("--N", type=int, default=N)
     ap.add_argument("--c", type=int, default=C_)
     ap.add_argument("--t", type=int, default=T_)
@@ -304,7 +307,10 @@ def run_ours(args, d):
     flush = L.DeviceBuffer(2 * L2_BYTES)
     args_dev = (d_r0.ptr, d_cws.ptr, d_cwo.ptr, d_pos.ptr, d_val.ptr, d_x.ptr, d_z.ptr)
 
-    e.autotune()                # leaf-kernel shape for this expansion shape (untimed)
+    if args.leaf_shape:         # leaf-kernel shape pinned, or tuned for this shape (untimed)
+        e.set_leaf_shape(*(int(v) for v in args.leaf_shape.lower().split("x")))
+    else:
+        e.autotune()
     leaf_tpb, leaf_lpt = e.leaf_shape()
     for _ in range(args.warmup):
         e.expand_device(0, *args_dev)
@@ -483,6 +489,7 @@ def run_ours(args, d):
                        "l2": "flushed between timed steps (256 MiB write)",
                        "cuda_graph": bool(args.graph), "leaf_cta_threads": leaf_tpb,
                        "leaf_leaves_per_thread": leaf_lpt,
+                       "leaf_shape": "pinned" if args.leaf_shape else "autotuned",
                        "vs_baseline_ref": "1x L40S serial arm 5.46M corr/s "
                                           "(GPU_baseline/final_l40s/e2e_arms.csv:32)"},
             "stage_ms": dict(zip(["tops", "leaf_gather", "x", "ntt"], stage_means))

@@ -329,6 +329,12 @@ int pcgb_expander_set_graph(pcgb_expander* e, int enable);
  * library stream.  Server plans are tuned on creation. */
 int pcgb_expander_autotune(pcgb_expander* e, int* tpb_out);
 int pcgb_expander_leaf_shape(const pcgb_expander* e, int* tpb, int* leaves_per_thread);
+/* Pins the leaf shape instead of tuning it (no reference counterpart): tpb
+ * in {32, 64, 128, 256}, leaves_per_thread one of the autotuner's
+ * candidates (2^(w*s) for the default s and up to two smaller), tpb x
+ * leaves_per_thread <= N/t.  Drops a captured graph (the next call
+ * re-captures); the workspace size may change. */
+int pcgb_expander_set_leaf_shape(pcgb_expander* e, int tpb, int leaves_per_thread);
 
 /* ---- native: consumers of the expansion -------------------------------- */
 /* One party's N Beaver-triple slot shares from its two ring OLEs (x1, z1)

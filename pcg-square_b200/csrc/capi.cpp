@@ -738,6 +738,13 @@ int pcgb_expander_autotune(pcgb_expander* e, int* tpb_out) {
     });
 }
 
+int pcgb_expander_set_leaf_shape(pcgb_expander* e, int tpb, int leaves_per_thread) {
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander");
+        pcgb::expander_set_leaf_shape(e, tpb, leaves_per_thread);
+    });
+}
+
 int pcgb_expander_leaf_shape(const pcgb_expander* e, int* tpb, int* leaves_per_thread) {
     return guarded([&] {
         if (!e) pcgb::fail(PCGB_EINVAL, "null expander");

@@ -53,17 +53,22 @@ void keyed_expand_tops(int K, int n, int w, int prg, const Blk* roots, const Blk
 // (kk+ll)*bin + [0, 2*bin) (pcg_ole_impl.h:435-444), so with s = kk+ll:
 //   s = r     -> first half,  kept;   s = r-1   -> second half, kept;
 //   s = r+t   -> first half,  negated; s = r+t-1 -> second half, negated.
+int leaf_sl_max(int n, int w) {
+    // Leaves per thread: 16 for w in {1,2,4}, 8 for w = 3; fewer when the
+    // half domain is smaller.
+    int sl = (w == 3) ? 1 : 4 / w;
+    while (sl > 1 && w * sl > n - 1) --sl;
+    if (w * sl > n - 1) fail(PCGB_EINVAL, "domain too small for the fused leaf kernel");
+    return sl;
+}
+
 void gather_plan_build(GatherPlan& gp, int N, int c, int t, int n, int w, int rank, int world) {
     gather_plan_free(gp);
     if (world < 1 || rank < 0 || rank >= world) fail(PCGB_EINVAL, "expander: bad shard rank/world");
     gp.N = N; gp.c = c; gp.t = t; gp.n = n; gp.w = w;
     gp.rank = rank; gp.world = world;
     const int levels = n / w;
-    // Leaves per thread: 16 for w in {1,2,4}, 8 for w = 3; fewer when the
-    // half domain is smaller.
-    int sl = (w == 3) ? 1 : 4 / w;
-    while (sl > 1 && w * sl > n - 1) --sl;
-    if (w * sl > n - 1) fail(PCGB_EINVAL, "domain too small for the fused leaf kernel");
+    const int sl = leaf_sl_max(n, w);
     gp.sl = sl;
     gp.S = 1 << (w * sl);
     gp.hl = levels - sl;

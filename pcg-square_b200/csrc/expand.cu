@@ -509,6 +509,27 @@ int expander_autotune(pcgb_expander* e) {
     return best_tpb;
 }
 
+void expander_set_leaf_shape(pcgb_expander* e, int tpb, int leaves_per_thread) {
+    const int sl_max = leaf_sl_max(e->n, e->w);
+    int sl = 0;
+    for (int k = 1; k <= sl_max; ++k)
+        if (leaves_per_thread == (1 << (e->w * k))) sl = k;
+    const size_t bin = static_cast<size_t>(e->N) / e->t;
+    if (sl == 0 || sl < sl_max - 2)
+        fail(PCGB_EINVAL, "set_leaf_shape: leaves per thread must be m^s for one of the "
+                          "autotuner's candidates s in [max(1, s_max - 2), s_max]");
+    if (tpb != 32 && tpb != 64 && tpb != 128 && tpb != 256)
+        fail(PCGB_EINVAL, "set_leaf_shape: CTA size must be 32, 64, 128 or 256");
+    if (static_cast<size_t>(tpb) * leaves_per_thread > bin)
+        fail(PCGB_EINVAL, "set_leaf_shape: CTA size x leaves per thread exceeds the bin N/t");
+    const bool graph = e->use_graph;
+    expander_set_graph(e, false);   // a captured graph replays the old shape
+    set_leaf_sl(e, sl);
+    e->gp.tpb = tpb;
+    e->scratch_bytes = workspace_bytes(e);
+    e->use_graph = graph;
+}
+
 void expander_leaf_shape(const pcgb_expander* e, int* tpb, int* leaves_per_thread) {
     if (tpb) *tpb = e->gp.tpb > 0 ? e->gp.tpb : 256;
     if (leaves_per_thread) *leaves_per_thread = e->gp.S;

@@ -165,6 +165,10 @@ void expander_shard(const pcgb_expander* e, int* rank, int* world, int* q_local,
 void expander_destroy(pcgb_expander* e);
 void expander_info(const pcgb_expander* e, int* K, int* levels, int* nk, size_t* scratch);
 int expander_autotune(pcgb_expander* e);  // leaf shape (leaves/thread, CTA size), cached per shape
+// Pins the leaf shape to one of the autotuner's candidates.
+void expander_set_leaf_shape(pcgb_expander* e, int tpb, int leaves_per_thread);
+// Largest leaves-per-thread exponent of the fused leaf kernel for (n, w).
+int leaf_sl_max(int n, int w);
 void expander_leaf_shape(const pcgb_expander* e, int* tpb, int* leaves_per_thread);
 void expand_host_async(pcgb_expander* e, int party, const Blk* roots, const Blk* cws,
                        const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val,

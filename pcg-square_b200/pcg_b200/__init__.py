@@ -126,6 +126,7 @@ def _load():
                                            C.c_int, _vp], C.c_int),
         "pcgb_expander_autotune": ([_vp, C.POINTER(C.c_int)], C.c_int),
         "pcgb_expander_leaf_shape": ([_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+        "pcgb_expander_set_leaf_shape": ([_vp, C.c_int, C.c_int], C.c_int),
         "pcgb_expand_host_async": ([_vp, C.c_int] + [_vp] * 7, C.c_int),
         "pcgb_expander_wait": ([_vp], C.c_int),
         "pcgb_expander_stage_times": ([_vp, C.POINTER(C.c_float), C.c_int], C.c_int),
@@ -636,6 +637,13 @@ class Expander:
         _check(lib.pcgb_expander_info(self.h, C.byref(K), C.byref(L), C.byref(nk), C.byref(sb)))
         self.scratch_bytes = sb.value
         return v.value
+
+    def set_leaf_shape(self, tpb, leaves_per_thread):
+        """Pin the fused leaf kernel's shape (one of the autotuner's candidates)."""
+        _check(lib.pcgb_expander_set_leaf_shape(self.h, int(tpb), int(leaves_per_thread)))
+        K, L, nk, sb = C.c_int(), C.c_int(), C.c_int(), C.c_size_t()
+        _check(lib.pcgb_expander_info(self.h, C.byref(K), C.byref(L), C.byref(nk), C.byref(sb)))
+        self.scratch_bytes = sb.value
 
     def leaf_shape(self):
         """(CTA threads, leaves per thread) of the fused leaf kernel."""

@@ -96,3 +96,25 @@ def test_async_host_expansions_match_sync(pcg):
     for p, _, (x, z) in bufs:
         assert (x == want[p][0]).all() and (z == want[p][1]).all()
     e.close()
+
+
+def test_pinned_leaf_shape_keeps_outputs(pcg):
+    """pcgb_expander_set_leaf_shape: every candidate shape gives the same x, z;
+    shapes outside the candidates are refused; a captured graph is dropped
+    and re-captured with the new shape."""
+    N, c, t = 1 << 14, 2, 8
+    _, _, e, d, _ = _material(pcg, N, c, t, 321)
+    x, z = pcg.DeviceBuffer(8 * N), pcg.DeviceBuffer(8 * N)
+    want = _expand(pcg, e, d, x, z)
+    e.set_graph(True)
+    for tpb, lpt in ((128, 16), (64, 8), (32, 4), (256, 4)):
+        e.set_leaf_shape(tpb, lpt)
+        assert e.leaf_shape() == (tpb, lpt)
+        for _ in range(2):
+            got = _expand(pcg, e, d, x, z)
+            assert (got[0] == want[0]).all() and (got[1] == want[1]).all(), (tpb, lpt)
+    for tpb, lpt in ((96, 16), (128, 2), (128, 32), (256, 16)):
+        with pytest.raises(pcg.PcgError):
+            e.set_leaf_shape(tpb, lpt)
+    assert e.leaf_shape() == (256, 4)
+    e.close()
