@@ -124,3 +124,18 @@ def test_output_layer_beaver_on_device(pcg):
         A = (int(sumT[0][k]) - int(sumT[1][k])) % P
         Bv = (int(sumC[1][k]) - int(sumC[0][k]) + int(beta[0][k]) + int(beta[1][k])) % P
         assert int(got[k]) == A * Bv % P, k
+
+
+def test_one_hash_output_layer_rejects_bad_arguments(pcg):
+    d = pcg.DeviceBuffer(16 * 64)
+    s = pcg.DeviceBuffer(64)
+    with pytest.raises(pcg.PcgError, match="null pointer"):
+        pcg.dpf_out_convert_device(d.ptr, 2, 32, None, s.ptr, s.ptr + 16)
+    with pytest.raises(pcg.PcgError, match="power of two"):
+        pcg.dpf_out_convert_device(d.ptr, 2, 24, d.ptr, s.ptr, s.ptr + 16)
+    with pytest.raises(pcg.PcgError, match="N smaller"):
+        pcg.dpf_out_scatter_g_conv_device(d.ptr, 4, 16, 2, 0, s.ptr, d.ptr, 8)
+    with pytest.raises(pcg.PcgError, match="party"):
+        pcg.out_beaver_open_device(4, 2, s.ptr, s.ptr, s.ptr, s.ptr, s.ptr, d.ptr)
+    with pytest.raises(pcg.PcgError, match="null pointer"):
+        pcg.out_beaver_close_device(4, 0, s.ptr, None, s.ptr, s.ptr, s.ptr, d.ptr)

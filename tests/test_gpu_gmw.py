@@ -234,3 +234,28 @@ def test_expansion_from_gmw_preprocessing_matches_fused(pcg, N, c, t):
     prod = O.poly_mul(out[0]["x"], out[1]["x"], N)
     zz = (out[0]["z"].astype(object) + out[1]["z"].astype(object)) % P
     assert all(int(a) == int(b) for a, b in zip(prod, zz))
+
+
+def test_gmw_rejects_bad_arguments(pcg):
+    """Argument errors come back as PCGB_EINVAL before any exchange."""
+    from pcg_b200 import twoparty as T
+    rng = np.random.default_rng(5)
+    B = 40
+    tri = T.bool_triples_dealer(pcg.gmw_position_add_gates(8), B, rng)[0]
+    off = np.arange(B, dtype=np.uint64)
+    never = lambda my: (_ for _ in ()).throw(AssertionError("no exchange expected"))
+    with pytest.raises(pcg.PcgError, match="party") as e:
+        pcg.gmw_position_add(2, off, 8, tri, never)
+    assert e.value.code == -1
+    with pytest.raises(pcg.PcgError, match="off_bits"):
+        pcg.gmw_position_add(0, off, 64, ((), (), ()), never)
+    with pytest.raises(pcg.PcgError, match="exchange callback is required"):
+        pcg.gmw_position_add(0, off, 8, tri, None)
+    with pytest.raises(ValueError, match="triples"):
+        pcg.gmw_position_add(0, off, 8, [v[:-1] for v in tri], never)
+    delta = np.zeros((B, 2), np.uint64)
+    for n, w in ((7, 2), (18, 9)):
+        with pytest.raises(pcg.PcgError, match=r"w \| n"):
+            pcg.gmw_dltsft(0, off, delta, n, w, ((), (), ()), never)
+    # Calls with B = 0 are no-ops.
+    assert pcg.gmw_position_add(0, np.zeros(0, np.uint64), 8, ((), (), ()), never).size == 0
