@@ -168,8 +168,7 @@ __global__ void __launch_bounds__(kTPB) expand_level_kernel(
 #pragma unroll
         for (int k = 0; k < M; ++k) dst[k] = kids[k];
         if (hash_next) {
-#pragma unroll 1
-            for (int k = 0; k < M; ++k) {
+            auto hash_child = [&](int k) {
                 Blk h[NK];
                 hash_node<W, PRG>(kids[k], a, h);
                 Blk* hd = Hn + static_cast<size_t>(b) * HS + (j * M + k) * NK;
@@ -179,6 +178,16 @@ __global__ void __launch_bounds__(kTPB) expand_level_kernel(
                     acc[kk].lo ^= h[kk].lo;
                     acc[kk].hi ^= h[kk].hi;
                 }
+            };
+            if constexpr (PRG == PCGB_PRG_CHACHA8 && W == 1) {
+                // Both children's blocks in flight: independent ARX chains
+                // keep the integer pipe busy while the level's loads and
+                // stores are outstanding.
+#pragma unroll
+                for (int k = 0; k < M; ++k) hash_child(k);
+            } else {
+#pragma unroll 1
+                for (int k = 0; k < M; ++k) hash_child(k);
             }
         }
     }
