@@ -417,6 +417,8 @@ def run_ours(args, d):
             check(lib.pcgb_expand_host_async(e.h, 0, *ptrs[k]))
         check(lib.pcgb_expander_wait(e.h))
         s, t = L.Event(), L.Event()
+        d.barrier()                              # all ranks start together
+        L.synchronize()
         s.record()
         for i in range(args.e2e_steps):
             check(lib.pcgb_expand_host_async(e.h, 0, *ptrs[i & 1]))
