@@ -164,6 +164,17 @@ int pcgb_dpf_out_scatter_g_device(const pcgb_blk* d_leaves, int B, size_t D, int
  * ordered on `stream`. */
 int pcgb_dpf_out_convert_device(const pcgb_blk* d_leaves, int B, size_t D, uint64_t* d_conv,
                                 uint64_t* d_sumC, uint64_t* d_sumT, void* stream);
+/* pcgb_dpf_batch_full_eval_device followed by pcgb_dpf_out_convert_device
+ * in one call, with the last level fused into the sums pass: the leaves are
+ * hashed as they are made and never stored (saves writing and re-reading
+ * 16 bytes per leaf, and the leaf buffer).  Same arguments as the drop-in
+ * plus the three device outputs of the convert pass, identical bit for bit;
+ * complete when the call returns. */
+int pcgb_dpf_batch_full_eval_convert_device(int B, int n, int w, const pcgb_blk* roots,
+                                            const pcgb_blk* dltsft, const uint8_t* round_keys,
+                                            int party, pcgb_exchange_fn exchange, void* user,
+                                            int prg, uint64_t* d_conv, uint64_t* d_sumC,
+                                            uint64_t* d_sumT);
 int pcgb_dpf_out_scatter_g_conv_device(const uint64_t* d_conv, int B, size_t D, int t, int party,
                                        const uint64_t* d_cw, uint64_t* d_g, int N, void* stream);
 

@@ -19,6 +19,9 @@ namespace pcgb {
 const Blk* dpf_interactive_device(int B, int n, int w, const Blk* roots, const Blk* dltsft,
                                   const uint8_t* rks, int prg, pcgb_exchange_fn ex, void* user,
                                   Blk* host_out);
+void dpf_interactive_convert_device(int B, int n, int w, const Blk* roots, const Blk* dltsft,
+                                    const uint8_t* rks, int prg, pcgb_exchange_fn ex, void* user,
+                                    uint64_t* d_conv, uint64_t* d_sumC, uint64_t* d_sumT);
 void dpf_out_sums_host(const Blk* d_leaves, int B, size_t D, uint64_t prime, uint64_t* sumC,
                        uint64_t* sumT);
 void dpf_out_scatter_host(const Blk* d_leaves, int B, size_t D, int t, int party, uint64_t prime,
@@ -397,6 +400,20 @@ int pcgb_dpf_out_sums_noalloc(const pcgb_blk* d_leaves, int B, size_t D, uint64_
     return guarded([&] {
         pcgb::dpf_out_sums_noalloc(reinterpret_cast<const Blk*>(d_leaves), B, D, prime, d_sumC,
                                    d_sumT, pcgb::as_stream(stream));
+    });
+}
+
+int pcgb_dpf_batch_full_eval_convert_device(int B, int n, int w, const pcgb_blk* roots,
+                                            const pcgb_blk* dltsft, const uint8_t* round_keys,
+                                            int party, pcgb_exchange_fn exchange, void* user,
+                                            int prg, uint64_t* d_conv, uint64_t* d_sumC,
+                                            uint64_t* d_sumT) {
+    (void)party;
+    if (B <= 0) return PCGB_OK;
+    return guarded([&] {
+        pcgb::dpf_interactive_convert_device(B, n, w, reinterpret_cast<const Blk*>(roots),
+                                             reinterpret_cast<const Blk*>(dltsft), round_keys, prg,
+                                             exchange, user, d_conv, d_sumC, d_sumT);
     });
 }
 

@@ -194,6 +194,90 @@ __global__ void __launch_bounds__(kTPB) expand_level_kernel(
     if (hash_next) cta_xor_reduce<NK>(acc, my_next + static_cast<size_t>(b) * NK, red);
 }
 
+// Last level fused with the output layer's first pass (the two-party
+// expansion's form): expands level levels-1 with its CW like
+// expand_level_kernel, but instead of storing the leaves it hashes each one
+// (ChaCha8 out-hash, leaf_convert_cuda.cu's C and tau) into the converted
+// word conv[b*D + d] = C | tau << 63 and reduces C (mod p) and tau over the
+// CTA into partials[b*parts + x] and partials[(B + b)*parts + x].
+// grid = (parts, B), parts = ceil(sz / kTPB).
+template <int W>
+__global__ void __launch_bounds__(kTPB) last_level_convert_kernel(
+    const Blk* __restrict__ cur, const Blk* __restrict__ H, const Blk* __restrict__ my,
+    const Blk* __restrict__ peer, size_t sz, size_t D, size_t HS, uint64_t* __restrict__ conv,
+    uint64_t* __restrict__ partials) {
+    constexpr int M = 1 << W, NK = M - 1;
+    __shared__ uint64_t sc[kTPB / 32], st[kTPB / 32];
+    const int b = blockIdx.y, parts = gridDim.x;
+    const size_t j = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    Blk cw[NK];
+    Blk cwf{0, 0};
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+        const Blk m0 = my[static_cast<size_t>(b) * NK + k], p0 = peer[static_cast<size_t>(b) * NK + k];
+        cw[k] = Blk{m0.lo ^ p0.lo, m0.hi ^ p0.hi};
+        cwf.lo ^= cw[k].lo;
+        cwf.hi ^= cw[k].hi;
+    }
+    uint64_t csum = 0, tsum = 0;
+    if (j < sz) {
+        const Blk p = cur[static_cast<size_t>(b) * D + j];
+        const bool t = (p.lo & 1) != 0;
+        Blk kids[M];
+        uint64_t xl = 0, xh = 0;
+#pragma unroll
+        for (int k = 0; k < NK; ++k) {
+            const Blk h = H[static_cast<size_t>(b) * HS + j * NK + k];
+            xl ^= h.lo;
+            xh ^= h.hi;
+            kids[k] = Blk{h.lo ^ (t ? cw[k].lo : 0), h.hi ^ (t ? cw[k].hi : 0)};
+        }
+        kids[NK] = Blk{xl ^ p.lo ^ (t ? cwf.lo : 0), xh ^ p.hi ^ (t ? cwf.hi : 0)};
+        uint64_t* dst = conv + static_cast<size_t>(b) * D + j * M;
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            const uint64_t C = reduce_p(out_hash_lo64(kids[k].lo, kids[k].hi));
+            csum = add_p(csum, C);
+            tsum += kids[k].lo & 1;
+            dst[k] = C | (kids[k].lo << 63);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        csum = add_p(csum, __shfl_xor_sync(0xffffffffu, csum, off));
+        tsum += __shfl_xor_sync(0xffffffffu, tsum, off);
+    }
+    if ((threadIdx.x & 31) == 0) { sc[threadIdx.x >> 5] = csum; st[threadIdx.x >> 5] = tsum; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t cc = 0, tt = 0;
+        for (int w = 0; w < kTPB / 32; ++w) { cc = add_p(cc, sc[w]); tt += st[w]; }
+        const size_t slot = static_cast<size_t>(b) * parts + blockIdx.x;
+        partials[slot] = cc;
+        partials[static_cast<size_t>(gridDim.y) * parts + slot] = tt;
+    }
+}
+
+// sumC[b], sumT[b] from the B x parts partials, in a fixed order.
+__global__ void convert_fold_kernel(const uint64_t* __restrict__ partials, int parts, int B,
+                                    uint64_t* __restrict__ sumC, uint64_t* __restrict__ sumT) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    uint64_t c = 0, t = 0;
+    for (int i = 0; i < parts; ++i) {
+        c = add_p(c, partials[static_cast<size_t>(b) * parts + i]);
+        t += partials[static_cast<size_t>(B) * parts + static_cast<size_t>(b) * parts + i];
+    }
+    sumC[b] = c;
+    sumT[b] = t;
+}
+
+// Where the fused last level writes (see last_level_convert_kernel).
+struct ConvOut {
+    uint64_t* conv;
+    uint64_t* partials;
+};
+
 // my[b][k] = dlt[b][level][k].
 __global__ void seed_kernel(Blk* my, const Blk* dlt, int B, int levels, int nk, int level) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -236,7 +320,7 @@ void grow(T*& p, size_t& cap, size_t need) {
 
 template <int W, int PRG>
 Blk* run_levels(Pool& pl, int B, int n, const Blk* roots, const Blk* dltsft,
-                pcgb_exchange_fn ex, void* user, cudaStream_t st) {
+                pcgb_exchange_fn ex, void* user, cudaStream_t st, const ConvOut* conv) {
     constexpr int M = 1 << W, NK = M - 1;
     const int levels = n / W;
     const size_t D = static_cast<size_t>(1) << n;
@@ -272,6 +356,12 @@ Blk* run_levels(Pool& pl, int B, int n, const Blk* roots, const Blk* dltsft,
         }
         const size_t sz = static_cast<size_t>(1) << (W * i);
         const dim3 grid(static_cast<unsigned>((sz + kTPB - 1) / kTPB), static_cast<unsigned>(B));
+        if (!hash_next && conv) {
+            last_level_convert_kernel<W><<<grid, kTPB, 0, st>>>(cur, H, my, pl.peer, sz, D, HS,
+                                                                conv->conv, conv->partials);
+            PCGB_POST_LAUNCH();
+            return nullptr;
+        }
         expand_level_kernel<W, PRG><<<grid, kTPB, smem, st>>>(cur, H, my, pl.peer, nxt, Hn, myn, sz,
                                                               D, HS, hash_next, te, pl.rk);
         PCGB_POST_LAUNCH();
@@ -291,7 +381,8 @@ void grow_pair(Blk*& a, Blk*& b, size_t& cap, size_t need) {
 }
 
 Blk* interactive_eval(int B, int n, int w, const Blk* roots, const Blk* dltsft, const uint8_t* rks,
-                      int prg, pcgb_exchange_fn ex, void* user, cudaStream_t st, Pool& pl) {
+                      int prg, pcgb_exchange_fn ex, void* user, cudaStream_t st, Pool& pl,
+                      const ConvOut* conv = nullptr) {
     if (w < 1 || w > 4)
         fail(PCGB_EINVAL, "dpf_gpu_batch_full_eval: w must be in [1,4] (expand_kernel CW[16])");
     if (n < 1 || n % w != 0) fail(PCGB_EINVAL, "dpf_gpu_batch_full_eval: w must divide n");
@@ -326,8 +417,8 @@ Blk* interactive_eval(int B, int n, int w, const Blk* roots, const Blk* dltsft, 
 #define PCGB_RUN(W_)                                                                        \
     case W_:                                                                                \
         return prg == PCGB_PRG_AES                                                          \
-                   ? run_levels<W_, PCGB_PRG_AES>(pl, B, n, roots, dltsft, ex, user, st)     \
-                   : run_levels<W_, PCGB_PRG_CHACHA8>(pl, B, n, roots, dltsft, ex, user, st);
+                   ? run_levels<W_, PCGB_PRG_AES>(pl, B, n, roots, dltsft, ex, user, st, conv) \
+                   : run_levels<W_, PCGB_PRG_CHACHA8>(pl, B, n, roots, dltsft, ex, user, st, conv);
     switch (w) {
         PCGB_RUN(1)
         PCGB_RUN(2)
@@ -355,6 +446,36 @@ const Blk* dpf_interactive_device(int B, int n, int w, const Blk* roots, const B
                                 cudaMemcpyDeviceToHost, st));
     PCGB_CK(cudaStreamSynchronize(st));
     return leaves;
+}
+
+// The interactive evaluation with its last level fused into the output
+// layer's sums pass: no leaves are stored.  Outputs are complete on return.
+void dpf_interactive_convert_device(int B, int n, int w, const Blk* roots, const Blk* dltsft,
+                                    const uint8_t* rks, int prg, pcgb_exchange_fn ex, void* user,
+                                    uint64_t* d_conv, uint64_t* d_sumC, uint64_t* d_sumT) {
+    if (B <= 0) return;
+    if (!d_conv || !d_sumC || !d_sumT)
+        fail(PCGB_EINVAL, "dpf_gpu_batch_full_eval_convert: null output pointer");
+    if (w < 1 || w > 4 || n < 1 || n % w != 0 || n > 30)
+        fail(PCGB_EINVAL, "dpf_gpu_batch_full_eval: w must be in [1,4] and divide n <= 30");
+    Pool& pl = pool_for_device();
+    std::lock_guard<std::mutex> lk(pl.mu);
+    cudaStream_t st = default_stream();
+    const size_t last = static_cast<size_t>(1) << (n - w);   // parents at the last level
+    const int parts = static_cast<int>((last + kTPB - 1) / kTPB);
+    uint64_t* partials = static_cast<uint64_t*>(
+        pool_alloc(2 * static_cast<size_t>(B) * parts * sizeof(uint64_t), st));
+    const ConvOut conv{d_conv, partials};
+    try {
+        interactive_eval(B, n, w, roots, dltsft, rks, prg, ex, user, st, pl, &conv);
+    } catch (...) {
+        cudaFreeAsync(partials, st);
+        throw;
+    }
+    convert_fold_kernel<<<(B + 127) / 128, 128, 0, st>>>(partials, parts, B, d_sumC, d_sumT);
+    PCGB_POST_LAUNCH();
+    PCGB_CK(cudaFreeAsync(partials, st));
+    PCGB_CK(cudaStreamSynchronize(st));
 }
 
 }  // namespace pcgb

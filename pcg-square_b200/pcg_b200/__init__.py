@@ -85,6 +85,9 @@ def _load():
         "pcgb_gmw_dltsft_gates": ([C.c_int, C.c_int], C.c_size_t),
         "pcgb_gmw_dltsft": ([C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                              _vp], C.c_int),
+        "pcgb_dpf_batch_full_eval_convert_device": ([C.c_int, C.c_int, C.c_int, _vp, _vp, _vp,
+                                                     C.c_int, _vp, _vp, C.c_int, _vp, _vp, _vp],
+                                                    C.c_int),
         "pcgb_dpf_out_convert_device": ([_vp, C.c_int, C.c_size_t, _vp, _vp, _vp, _vp], C.c_int),
         "pcgb_dpf_out_scatter_g_conv_device": ([_vp, C.c_int, C.c_size_t, C.c_int, C.c_int, _vp,
                                                 _vp, C.c_int, _vp], C.c_int),
@@ -430,6 +433,20 @@ def dpf_out_sums(d_leaves, B, D, prime=P):
 def dpf_out_scatter_g_device(d_leaves, B, D, t, party, d_cw, d_g, N, stream=None):
     """Folded g of the B instances into device d_g; CWs on the device."""
     _check(lib.pcgb_dpf_out_scatter_g_device(d_leaves, B, D, t, party, d_cw, d_g, N, stream))
+
+
+def dpf_gpu_batch_full_eval_convert_device(B, n, w, roots, dltsft, d_conv, d_sumC, d_sumT,
+                                           round_keys=None, party=0, exchange=None,
+                                           prg=PRG_AES):
+    """Interactive evaluation fused with the convert pass: converted words
+    (B * 2^n) and sums into the device buffers; no leaves are stored."""
+    roots = _blocks(roots, B)
+    dltsft = _blocks(dltsft)
+    cb = _exchange_cb(exchange)
+    rk = None if round_keys is None else _u8(round_keys)
+    _check(lib.pcgb_dpf_batch_full_eval_convert_device(
+        B, n, w, _p(roots), _p(dltsft), _p(rk), party, C.cast(cb, C.c_void_p) if cb else None,
+        None, prg, d_conv, d_sumC, d_sumT))
 
 
 def dpf_out_convert_device(d_leaves, B, D, d_conv, d_sumC, d_sumT, stream=None):

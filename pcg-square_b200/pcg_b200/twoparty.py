@@ -6,8 +6,10 @@ run by each party in its own process:
 
   for every block (i, j):
     leaves = dpf_gpu_batch_full_eval_device(...)   one CW exchange per level
-    sumC, sumT = dpf_out_sums(leaves)              (pcgb_dpf_out_convert_device,
-                                                    which keeps C | tau<<63 per leaf)
+    sumC, sumT = dpf_out_sums(leaves)              (one call, pcgb_dpf_batch_full_
+                                                    eval_convert_device: the last
+                                                    level keeps C | tau<<63 per
+                                                    leaf, no leaves stored)
     <A> = (-1)^party sumT, <B> = (-1)^(1-party) sumC + <beta>
     open d = A - r, e = B - s                      Beaver triple (r, s, rs), on
     <CW> = d<s> + e<r> + <rs> (+ d e for party 0);  the device; open CW
@@ -32,8 +34,8 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import (DeviceBuffer, PRG_CHACHA8, add_mod_p_device, dpf_gpu_batch_full_eval_device,
-               dpf_out_convert_device, dpf_out_scatter_g_conv_device, gmw_dltsft,
+from . import (DeviceBuffer, PRG_CHACHA8, add_mod_p_device,
+               dpf_gpu_batch_full_eval_convert_device, dpf_out_scatter_g_conv_device, gmw_dltsft,
                gmw_position_add, out_beaver_close_device, out_beaver_open_device, synchronize,
                to_device)
 
@@ -150,20 +152,21 @@ def gen_and_expand(party, chan, expander, material, prg=PRG_CHACHA8, batched=Tru
         nB = nb * B
         roots = np.ascontiguousarray(np.concatenate([m.roots[b] for b in blocks]))
         dlt = np.ascontiguousarray(np.concatenate([m.dltsft[b] for b in blocks]))
-        d_leaves = dpf_gpu_batch_full_eval_device(nB, n, 1, roots, dlt, party=party,
-                                                  exchange=chan.exchange, prg=prg)
         d_conv = _scratch_buf("conv", 8 * nB * D)
         d_sums = _scratch_buf("sums", 2 * 8 * nB)     # sumC | sumT
         d_sumC, d_sumT = d_sums.ptr, d_sums.ptr + 8 * nB
         d_cw = _scratch_buf("cw", 8 * nB)
-        dpf_out_convert_device(d_leaves, nB, D, d_conv.ptr, d_sumC, d_sumT)
+        # DPF levels with their CW exchanges, the last level fused with the
+        # sums pass (leaves hashed as they are made, never stored).
+        dpf_gpu_batch_full_eval_convert_device(nB, n, 1, roots, dlt, d_conv.ptr, d_sumC, d_sumT,
+                                               party=party, exchange=chan.exchange, prg=prg)
         cat = lambda a: np.concatenate([a[b] for b in blocks])
         _beaver_cw_device(party, chan, nB, d_sumC, d_sumT, cat(m.beta), cat(m.r), cat(m.s),
                           cat(m.rs), d_cw)
         for k, blk in enumerate(blocks):
             dpf_out_scatter_g_conv_device(d_conv.ptr + 8 * k * B * D, B, D, t, party,
                                           d_cw.ptr + 8 * k * B, d_g.ptr + 8 * blk * N, N)
-        synchronize()   # d_leaves is valid until the next DPF call
+        synchronize()
     d_pos, d_val = to_device(m.pos), to_device(m.val)
     d_x, d_z = DeviceBuffer(8 * N), DeviceBuffer(8 * N)
     e.expand_from_g_device(d_g.ptr, d_pos.ptr, d_val.ptr, d_x.ptr, d_z.ptr)

@@ -94,3 +94,38 @@ def test_dpf_real_bench_golden_checksums(pcg, n, B, t, want):
     sc, st = pcg.dpf_out_sums(d_leaves, B, D)
     g = pcg.dpf_out_scatter_g(d_leaves, B, D, t, 0, CW, t * (D // 2))
     assert real_bench_checksum(sc, st, g) == want
+
+
+@pytest.mark.parametrize("prg", [O.PRG_CHACHA8, O.PRG_AES])
+@pytest.mark.parametrize("n,w,B", [(1, 1, 3), (10, 1, 5), (10, 2, 5), (9, 3, 4), (8, 4, 6),
+                                   (12, 1, 300)])
+def test_interactive_fused_convert_matches_two_calls(pcg, prg, n, w, B):
+    """pcgb_dpf_batch_full_eval_convert_device (last level fused with the
+    sums pass, no leaves stored) gives the converted words and sums of
+    dpf_gpu_batch_full_eval_device + pcgb_dpf_out_convert_device, and the
+    oracle's sums, with a real per-level exchange."""
+    nk, L = (1 << w) - 1, n // w
+    rks = O.aes_tree_round_keys(np.arange(16, dtype=np.uint8), nk) if prg == O.PRG_AES else None
+    rng = np.random.default_rng(31 * n + w + B)
+    roots = rng.integers(0, 2**64 - 1, (B, 2), dtype=np.uint64, endpoint=True)
+    dlt = rng.integers(0, 2**64 - 1, (B * L * nk, 2), dtype=np.uint64, endpoint=True)
+    mask = rng.integers(0, 2**64 - 1, (B * nk, 2), dtype=np.uint64, endpoint=True)
+    exchange = lambda my: my ^ mask            # a deterministic stand-in for the peer
+    D = 1 << n
+    d_leaves = pcg.dpf_gpu_batch_full_eval_device(B, n, w, roots, dlt, round_keys=rks,
+                                                  exchange=exchange, prg=prg)
+    conv0, sums0 = pcg.DeviceBuffer(8 * B * D), pcg.DeviceBuffer(16 * B)
+    pcg.dpf_out_convert_device(d_leaves, B, D, conv0.ptr, sums0.ptr, sums0.ptr + 8 * B)
+    pcg.synchronize()
+    leaves = np.zeros((B * D, 2), np.uint64)
+    pcg.lib.pcgb_memcpy_d2h(leaves.ctypes.data, d_leaves, leaves.nbytes, None)
+    conv1, sums1 = pcg.DeviceBuffer(8 * B * D), pcg.DeviceBuffer(16 * B)
+    pcg.lib.pcgb_memset(conv1.ptr, 0xA5, conv1.nbytes, None)   # every word must be written
+    pcg.dpf_gpu_batch_full_eval_convert_device(B, n, w, roots, dlt, conv1.ptr, sums1.ptr,
+                                               sums1.ptr + 8 * B, round_keys=rks,
+                                               exchange=exchange, prg=prg)
+    assert (conv1.download(np.uint64, B * D) == conv0.download(np.uint64, B * D)).all()
+    s0, s1 = sums0.download(np.uint64, 2 * B), sums1.download(np.uint64, 2 * B)
+    assert (s0 == s1).all()
+    wc, wt = O.out_sums(leaves, B, D)
+    assert (s1[:B] == wc).all() and (s1[B:] == wt).all()
