@@ -137,6 +137,9 @@ def parse():
     ap.add_argument("--leaf-shape", default=None,
                     help="pin the leaf kernel to THREADSxLEAVES (e.g. 128x8) instead of "
                          "autotuning it (profiler captures need one fixed shape)")
+    ap.add_argument("--a0-public", action="store_true",
+                    help="all c public polynomials a_0 .. a_{c-1} uniform (the reference "
+                         "fixes a_0 = 1)")
     ap.add_argument("--N", type=int, default=N)
     ap.add_argument("--c", type=int, default=C_)
     ap.add_argument("--t", type=int, default=T_)
@@ -293,8 +296,11 @@ def run_ours(args, d):
     import pcg_b200 as L
     N, C_, T_ = args.N, args.c, args.t
     L.set_device(d.local)
-    a = L.public_a(N, C_, A_SEED)
-    e = L.Expander(N, C_, T_, W_, L.PRG_CHACHA8, public_a=a)
+    if args.a0_public:          # all c public polynomials uniform, a_0 too
+        a = L.public_a(N, C_ + 1, A_SEED)
+    else:                       # the reference's a_0 = 1, a_1 .. a_{c-1} uniform
+        a = L.public_a(N, C_, A_SEED)
+    e = L.Expander(N, C_, T_, W_, L.PRG_CHACHA8, public_a=a, a0_public=args.a0_public)
     K, levels = e.K, e.levels
     seed = 1000 + d.rank
     d_r0, d_r1 = L.DeviceBuffer(16 * K), L.DeviceBuffer(16 * K)
@@ -487,6 +493,8 @@ def run_ours(args, d):
             "config": {"workload": f"pcg-ole expansion N=2^{N.bit_length() - 1} c={C_} t={T_} "
                                    "w=1 chacha8 (one party, keyed DPF from the GPU dealer)",
                        "N": N, "c": C_, "t": T_, "w": W_, "keys": K, "leaves": K * D,
+                       "public_a": ("a_0 .. a_{c-1} uniform" if args.a0_public
+                                    else "a_0 = 1, a_1 .. a_{c-1} uniform"),
                        "parallelism": f"replicas x{d.world}",
                        "l2": "flushed between timed steps (256 MiB write)",
                        "cuda_graph": bool(args.graph), "leaf_cta_threads": leaf_tpb,

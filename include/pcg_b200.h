@@ -268,6 +268,13 @@ int pcgb_expander_create(pcgb_expander** e, int N, int c, int t, int w, int prg,
 int pcgb_expander_destroy(pcgb_expander* e);
 /* Shape-derived sizes: K keys, levels, nk CWs per level. */
 int pcgb_expander_info(const pcgb_expander* e, int* K, int* levels, int* nk, size_t* scratch_bytes);
+/* An expander whose c public polynomials are all given, a_0 included
+ * (public_a = a_0 .. a_{c-1}, N coefficients each), where the reference
+ * fixes a_0 = 1 (pcg_ole_impl.h:455-483) and pcgb_expander_create takes
+ * a_1 .. a_{c-1}.  x = sum a_i e_i and z = sum a_i a_j g_ij as before; the
+ * cost is t extra products per x word.  No reference counterpart. */
+int pcgb_expander_create_public_a0(pcgb_expander** e, int N, int c, int t, int w, int prg,
+                                   const uint64_t* public_a, const uint8_t* master_key);
 /* A shard of one expansion for multi-GPU runs (no reference counterpart):
  * the c(c+1)/2 pair blocks (i <= j) are split over `world` expanders,
  * balanced by work (off-diagonal pairs carry two blocks), and this one

@@ -80,6 +80,7 @@ def lib():
         L.orc_expand.argtypes = [C.POINTER(Shape), C.c_int, u64p, u64p, u64p, u64p, u64p,
                                  u64p, C.c_void_p, C.c_uint64, C.c_int, u64p, u64p,
                                  C.c_void_p]
+        L.orc_step4.argtypes = [C.c_int, C.c_int, C.c_int, u64p, u64p, u64p, u64p, u64p, u64p]
         L.orc_mt64_fill.argtypes = [C.c_uint64, u64p, C.c_size_t]
         L.orc_bench_sample.argtypes = [C.POINTER(Shape), C.c_int, u64p, u64p, u64p, u64p,
                                        C.c_int, C.c_int, C.c_int, C.c_int,
@@ -267,6 +268,18 @@ def expand(s, party, roots, cws, cw_out, pos, val, a, rks=None, blocks_mask=(1 <
                           blocks_mask, threads, x, z, _ptr(g))
     assert rc == 0, rc
     return (x, z, g) if want_g else (x, z)
+
+
+def step4(N, c, t, pos, val, a_all, g):
+    """x, z from the c*c block outputs g and all c public polynomials a_all
+    (a_0 included)."""
+    x, z = np.zeros(N, np.uint64), np.zeros(N, np.uint64)
+    rc = lib().orc_step4(N, c, t, np.ascontiguousarray(pos, np.uint64),
+                         np.ascontiguousarray(val, np.uint64),
+                         np.ascontiguousarray(a_all, np.uint64), np.ascontiguousarray(g, np.uint64),
+                         x, z)
+    assert rc == 0, rc
+    return x, z
 
 
 # ---- reference code compiled from its own sources (oracle/_ref) -----------

@@ -753,16 +753,26 @@ int orc_expand(const orc_shape* s, int party, const orc_blk* roots,
         for (int b = 0; b < c * c; ++b)
             std::memcpy(g_out + static_cast<size_t>(b) * N, g[b].data(), sizeof(uint64_t) * N);
 
-    // Step 4 (pcg_ole_impl.h:455-483): a_0 = 1, a_i = public_a[i-1];
-    // x = sum a_i e_i; z = sum_{i,j} (a_i a_j) g_ij.
+    // Step 4 with the reference's a_0 = 1, a_i = public_a[i-1].
+    std::vector<uint64_t> a_all(static_cast<size_t>(c) * N, 0), g_all(static_cast<size_t>(c) * c * N);
+    a_all[0] = 1;
+    if (c > 1) std::memcpy(a_all.data() + N, a, sizeof(uint64_t) * N * (c - 1));
+    for (int b = 0; b < c * c; ++b)
+        std::memcpy(g_all.data() + static_cast<size_t>(b) * N, g[b].data(), sizeof(uint64_t) * N);
+    return orc_step4(N, c, t, pos, val, a_all.data(), g_all.data(), x, z);
+}
+
+// Step 4 (pcg_ole_impl.h:455-483) for any public a_0 .. a_{c-1}:
+// x = sum a_i e_i; z = sum_{i,j} (a_i a_j) g_ij.
+int orc_step4(int N, int c, int t, const uint64_t* pos, const uint64_t* val, const uint64_t* a,
+              const uint64_t* g, uint64_t* x, uint64_t* z) {
     std::vector<std::vector<uint64_t>> av(c, std::vector<uint64_t>(N, 0));
-    av[0][0] = 1;
-    for (int i = 1; i < c; ++i)
-        std::memcpy(av[i].data(), a + static_cast<size_t>(i - 1) * N, sizeof(uint64_t) * N);
-    std::vector<uint64_t> acc(N, 0), tmp(N), e(N), aa(N);
+    for (int i = 0; i < c; ++i)
+        for (int d = 0; d < N; ++d) av[i][d] = a[static_cast<size_t>(i) * N + d] % P;
+    std::vector<uint64_t> acc(N, 0), tmp(N), e(N), aa(N), gb(N);
     for (int i = 0; i < c; ++i) {
         std::fill(e.begin(), e.end(), 0);
-        for (int k = 0; k < t; ++k) e[pos[i * t + k]] = val[i * t + k] % P;
+        for (int k = 0; k < t; ++k) e[pos[i * t + k] % N] = val[i * t + k] % P;
         poly_mul1(tmp.data(), av[i].data(), e.data(), N);
         for (int d = 0; d < N; ++d) acc[d] = addm(acc[d], tmp[d]);
     }
@@ -770,8 +780,9 @@ int orc_expand(const orc_shape* s, int party, const orc_blk* roots,
     std::fill(acc.begin(), acc.end(), 0);
     for (int i = 0; i < c; ++i)
         for (int j = 0; j < c; ++j) {
+            for (int d = 0; d < N; ++d) gb[d] = g[static_cast<size_t>(i * c + j) * N + d] % P;
             poly_mul1(aa.data(), av[i].data(), av[j].data(), N);
-            poly_mul1(tmp.data(), aa.data(), g[i * c + j].data(), N);
+            poly_mul1(tmp.data(), aa.data(), gb.data(), N);
             for (int d = 0; d < N; ++d) acc[d] = addm(acc[d], tmp[d]);
         }
     std::memcpy(z, acc.data(), sizeof(uint64_t) * N);

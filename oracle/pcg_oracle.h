@@ -143,6 +143,12 @@ int orc_expand(const orc_shape* s, int party, const orc_blk* roots,
                uint64_t blocks_mask, int threads, uint64_t* x, uint64_t* z,
                uint64_t* g_out);
 
+/* Step 4 of the expansion (pcg_ole_impl.h:455-483) for any public a_0 ..
+ * a_{c-1} (a: c*N; the reference fixes a_0 = 1) and block outputs g (c*c*N,
+ * block (i, j) at (i*c + j)*N): x = sum a_i e_i, z = sum_{i,j} a_i a_j g_ij. */
+int orc_step4(int N, int c, int t, const uint64_t* pos, const uint64_t* val, const uint64_t* a,
+              const uint64_t* g, uint64_t* x, uint64_t* z);
+
 /* Bounded CPU sample of one party's expansion for the timed baseline:
  * output layer of n_blocks blocks x keys_per_block keys (keyed DPF + convert
  * + scatter, as orc_expand) and n_polymuls length-N products, the work split

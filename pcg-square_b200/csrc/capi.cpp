@@ -641,6 +641,15 @@ int pcgb_expander_create_shard(pcgb_expander** e, int N, int c, int t, int w, in
     });
 }
 
+int pcgb_expander_create_public_a0(pcgb_expander** e, int N, int c, int t, int w, int prg,
+                                   const uint64_t* public_a, const uint8_t* master_key) {
+    if (e) *e = nullptr;
+    return guarded([&] {
+        if (!e) pcgb::fail(PCGB_EINVAL, "null expander handle");
+        *e = pcgb::expander_create(N, c, t, w, prg, public_a, master_key, 0, 1, 1);
+    });
+}
+
 int pcgb_expander_shard(const pcgb_expander* e, int* rank, int* world, int* pairs_local,
                         int* pairs_total) {
     return guarded([&] {

@@ -2,7 +2,8 @@
 // CPU_baseline/pcg_ole_2pc/pcg_ole_impl.h:213-312 and :453-484):
 //
 //   g_ij   = output layer of the t^2 DPF keys of block (i, j), folded mod X^N+1
-//   x      = sum_i a_i e_i                      (a_0 = 1, e_i the regular noise)
+//   x      = sum_i a_i e_i                      (e_i the regular noise; a_0 = 1 as
+//                                                the reference has it, or public)
 //   z      = sum_{i,j} a_i a_j g_ij = INTT( sum_{i<=j} (a^_i a^_j) . NTT(g_ij + g_ji) )
 //
 // The expander keeps, per shape, the a_i coefficients (Montgomery form, for
@@ -33,11 +34,12 @@ void deal_keys_launch(int N, int c, int t, int n, int w, int prg, uint64_t seed,
 
 namespace {
 
-// x[p] = sum_k [p == pos_0k] val_0k + sum_{i>=1,k} val_ik * a_i[p - pos_ik]
-// with the negacyclic sign when p < pos_ik.  aR holds a_i * 2^64 mod p, so
-// one Montgomery product gives a_i * val.
+// x[p] = sum_{i>=i0,k} val_ik * a_i[p - pos_ik] with the negacyclic sign
+// when p < pos_ik, plus sum_k [p == pos_0k] val_0k when a_0 = 1 (i0 = 1).
+// aR holds a_i0 .. a_{c-1} times 2^64 mod p, so one Montgomery product
+// gives a_i * val.
 __global__ void x_kernel(const uint64_t* __restrict__ pos, const uint64_t* __restrict__ val,
-                         const uint64_t* __restrict__ aR, int c, int t, size_t N,
+                         const uint64_t* __restrict__ aR, int c, int t, int i0, size_t N,
                          uint64_t* __restrict__ x) {
     extern __shared__ uint64_t nz[];  // [c*t] positions then [c*t] values
     const int ct = c * t;
@@ -49,10 +51,11 @@ __global__ void x_kernel(const uint64_t* __restrict__ pos, const uint64_t* __res
     const size_t p = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (p >= N) return;
     uint64_t acc = 0;
-    for (int k = 0; k < t; ++k)
-        if (nz[k] == p) acc = add_p(acc, nz[ct + k]);
-    for (int i = 1; i < c; ++i) {
-        const uint64_t* a = aR + static_cast<size_t>(i - 1) * N;
+    if (i0 == 1)
+        for (int k = 0; k < t; ++k)
+            if (nz[k] == p) acc = add_p(acc, nz[ct + k]);
+    for (int i = i0; i < c; ++i) {
+        const uint64_t* a = aR + static_cast<size_t>(i - i0) * N;
         for (int k = 0; k < t; ++k) {
             const uint64_t ps = nz[i * t + k];
             const bool wrap = p < ps;
@@ -139,7 +142,8 @@ struct pcgb_expander {
     const pcgb::NttPlan* ntt = nullptr;
     pcgb::GatherPlan gp;
     uint64_t* d_img = nullptr;   // Q*N
-    uint64_t* d_aR = nullptr;    // (c-1)*N
+    uint64_t* d_aR = nullptr;    // (c-i0)*N: a_i0 .. a_{c-1}, Montgomery form
+    int i0 = 1;                  // 1: a_0 = 1 (the reference); 0: a_0 public
     pcgb::Blk* d_F = nullptr;
     pcgb::Blk* d_tops = nullptr;
     uint64_t* d_g = nullptr;     // Q*N
@@ -177,14 +181,15 @@ struct pcgb_expander {
 namespace pcgb {
 
 pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64_t* public_a,
-                               const uint8_t* master_key, int rank, int world) {
+                               const uint8_t* master_key, int rank, int world, int a0_public) {
     if (N < 4 || (N & (N - 1)) || N > (1 << kMaxLogN))
         fail(PCGB_EINVAL, "expander: N must be a power of two in [4, 2^24]");
     if (c < 1 || c > 8) fail(PCGB_EINVAL, "expander: c must be in [1, 8]");
     if (t < 1 || (t & (t - 1)) || N / t < 2) fail(PCGB_EINVAL, "expander: t must be a power of two <= N/2");
     if (prg != PCGB_PRG_AES && prg != PCGB_PRG_CHACHA8) fail(PCGB_EINVAL, "expander: unknown PRG");
     if (prg == PCGB_PRG_AES && !master_key) fail(PCGB_EINVAL, "expander: AES needs a master key");
-    if (c > 1 && !public_a) fail(PCGB_EINVAL, "expander: public_a required for c > 1");
+    const int i0 = a0_public ? 0 : 1, na = c - i0;   // public polynomials given
+    if (na > 0 && !public_a) fail(PCGB_EINVAL, "expander: public_a required");
     const int n = ilog2(2ull * (N / t));
     if (w < 1 || w > 4 || n % w) fail(PCGB_EINVAL, "expander: w must be in [1,4] and divide log2(2N/t)");
     auto* e = new pcgb_expander();
@@ -192,32 +197,33 @@ pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64
         PCGB_CK(cudaGetDevice(&e->dev));
         e->N = N; e->c = c; e->t = t; e->w = w; e->prg = prg; e->n = n;
         e->levels = n / w; e->nk = (1 << w) - 1; e->K = c * c * t * t; e->Q = c * (c + 1) / 2;
+        e->i0 = i0;
         cudaStream_t st = default_stream();
         e->ntt = &ntt_plan(ilog2(N));
         gather_plan_build(e->gp, N, c, t, n, w, rank, world);
         const size_t NN = static_cast<size_t>(N);
         const int Qs = e->gp.Qs;
         PCGB_CK(cudaMalloc(&e->d_img, sizeof(uint64_t) * NN * std::max(Qs, 1)));
-        if (c > 1) PCGB_CK(cudaMalloc(&e->d_aR, sizeof(uint64_t) * NN * (c - 1)));
+        if (na > 0) PCGB_CK(cudaMalloc(&e->d_aR, sizeof(uint64_t) * NN * na));
         // a_i coefficients (Montgomery form) and evaluations.
         std::vector<uint64_t*> ahat(c, nullptr);
         const uint64_t r2 = r2_mod_p(), r3 = mul_p_host(r2, r_mod_p());
-        if (c > 1) {
+        if (na > 0) {
             uint64_t* tmp = nullptr;
-            PCGB_CK(cudaMalloc(&tmp, sizeof(uint64_t) * NN * (c - 1)));
-            upload_blocking(tmp, public_a, sizeof(uint64_t) * NN * (c - 1));
-            reduce_mod_p(tmp, tmp, NN * (c - 1), st);
-            scale_kernel<<<blocks_for(NN * (c - 1), 256), 256, 0, st>>>(e->d_aR, tmp, NN * (c - 1), r2);
+            PCGB_CK(cudaMalloc(&tmp, sizeof(uint64_t) * NN * na));
+            upload_blocking(tmp, public_a, sizeof(uint64_t) * NN * na);
+            reduce_mod_p(tmp, tmp, NN * na, st);
+            scale_kernel<<<blocks_for(NN * na, 256), 256, 0, st>>>(e->d_aR, tmp, NN * na, r2);
             PCGB_POST_LAUNCH();
-            ntt_forward(*e->ntt, tmp, c - 1, st);
-            for (int i = 1; i < c; ++i) ahat[i] = tmp + NN * (i - 1);
-            // Images of this shard's pairs, in slot order.
+            ntt_forward(*e->ntt, tmp, na, st);
+            for (int i = i0; i < c; ++i) ahat[i] = tmp + NN * (i - i0);
+            // Images of this shard's pairs, in slot order (a null factor is a_0 = 1).
             for (int k = 0; k < Qs; ++k) {
                 const int ij = static_cast<int>(e->gp.pair_ij[e->gp.shard_pairs[k]]);
-                const int i = ij / c, j = ij % c;
+                const uint64_t* A = ahat[ij / c];
+                const uint64_t* B = ahat[ij % c];
                 image_kernel<<<blocks_for(NN, 256), 256, 0, st>>>(
-                    e->d_img + NN * k, i == 0 ? (j == 0 ? nullptr : ahat[j]) : ahat[i],
-                    i == 0 ? nullptr : ahat[j], NN, r2, r3);
+                    e->d_img + NN * k, A ? A : B, A ? B : nullptr, NN, r2, r3);
                 PCGB_POST_LAUNCH();
             }
             PCGB_CK(cudaStreamSynchronize(st));
@@ -299,7 +305,7 @@ void expand_device_ws(pcgb_expander* e, const Workspace& ws, int party, const Bl
     keyed_leaf_gather(e->gp, party, e->prg, ws.F, cws, cw_out, e->d_rk, ws.g, st);
     if (ev) PCGB_CK(cudaEventRecord(ev[2], st));
     const size_t sm = sizeof(uint64_t) * 2 * static_cast<size_t>(e->c) * e->t;
-    x_kernel<<<blocks_for(NN, 256), 256, sm, st>>>(pos, val, e->d_aR, e->c, e->t, NN, x);
+    x_kernel<<<blocks_for(NN, 256), 256, sm, st>>>(pos, val, e->d_aR, e->c, e->t, e->i0, NN, x);
     PCGB_POST_LAUNCH();
     if (ev) PCGB_CK(cudaEventRecord(ev[3], st));
     if (e->gp.Qs > 0) ntt_mac_inverse(*e->ntt, ws.g, e->d_img, e->gp.Qs, z, st);
@@ -639,7 +645,7 @@ void expand_from_g_device(pcgb_expander* e, const uint64_t* g, const uint64_t* p
     pair_merge_kernel<<<dim3(blocks_for(NN, 256), e->Q), 256, 0, st>>>(g, e->c, NN, e->d_g);
     PCGB_POST_LAUNCH();
     const size_t sm = sizeof(uint64_t) * 2 * static_cast<size_t>(e->c) * e->t;
-    x_kernel<<<blocks_for(NN, 256), 256, sm, st>>>(pos, val, e->d_aR, e->c, e->t, NN, x);
+    x_kernel<<<blocks_for(NN, 256), 256, sm, st>>>(pos, val, e->d_aR, e->c, e->t, e->i0, NN, x);
     PCGB_POST_LAUNCH();
     ntt_mac_inverse(*e->ntt, e->d_g, e->d_img, e->Q, z, st);
 }

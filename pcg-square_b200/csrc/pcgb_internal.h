@@ -159,8 +159,11 @@ struct Workspace {
     uint64_t* g = nullptr;
 };
 // rank/world: this expander's shard of the pair blocks (see GatherPlan).
+// public_a: a_1 .. a_{c-1} (a_0 = 1, the reference's convention), or with
+// a0_public a_0 .. a_{c-1}; N coefficients each.
 pcgb_expander* expander_create(int N, int c, int t, int w, int prg, const uint64_t* public_a,
-                               const uint8_t* master_key, int rank = 0, int world = 1);
+                               const uint8_t* master_key, int rank = 0, int world = 1,
+                               int a0_public = 0);
 void expander_shard(const pcgb_expander* e, int* rank, int* world, int* q_local, int* q_total);
 void expander_destroy(pcgb_expander* e);
 void expander_info(const pcgb_expander* e, int* K, int* levels, int* nk, size_t* scratch);

@@ -123,6 +123,8 @@ def _load():
         "pcgb_expander_create_shard": ([_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp,
                                         _vp, C.c_int, C.c_int], C.c_int),
         "pcgb_expander_shard": ([_vp] * 5, C.c_int),
+        "pcgb_expander_create_public_a0": ([C.POINTER(_vp), C.c_int, C.c_int, C.c_int, C.c_int,
+                                            C.c_int, _vp, _vp], C.c_int),
         "pcgb_reduce_mod_p": ([_vp, _vp, C.c_size_t, _vp], C.c_int),
         "pcgb_expand_from_g_device": ([_vp] * 6 + [_vp], C.c_int),
         "pcgb_dpf_out_scatter_g_device": ([_vp, C.c_int, C.c_size_t, C.c_int, C.c_int, _vp, _vp,
@@ -587,15 +589,23 @@ class Expander:
     """Resident per-shape state of the fused PCG-OLE expansion (one device)."""
 
     def __init__(self, N, c, t, w=1, prg=PRG_CHACHA8, public_a=None, master_key=None,
-                 rank=0, world=1):
-        """rank/world: this expander's shard of the pair blocks (see
-        pcgb_expander_create_shard); Q is then the shard's own pair count."""
+                 rank=0, world=1, a0_public=False):
+        """public_a: a_1 .. a_{c-1} (a_0 = 1, the reference's convention), or
+        with a0_public=True all of a_0 .. a_{c-1}.  rank/world: this
+        expander's shard of the pair blocks (see pcgb_expander_create_shard);
+        Q is then the shard's own pair count."""
         self.N, self.c, self.t, self.w, self.prg = N, c, t, w, prg
         pa = None if public_a is None else np.ascontiguousarray(public_a, np.uint64)
         mk = None if master_key is None else _u8(master_key)
         h = C.c_void_p()
-        _check(lib.pcgb_expander_create_shard(C.byref(h), N, c, t, w, prg, _p(pa), _p(mk),
-                                              rank, world))
+        if a0_public:
+            if (rank, world) != (0, 1):
+                raise ValueError("a0_public expanders are not sharded")
+            _check(lib.pcgb_expander_create_public_a0(C.byref(h), N, c, t, w, prg, _p(pa),
+                                                      _p(mk)))
+        else:
+            _check(lib.pcgb_expander_create_shard(C.byref(h), N, c, t, w, prg, _p(pa), _p(mk),
+                                                  rank, world))
         self.h = h.value
         K, L, nk, sb = C.c_int(), C.c_int(), C.c_int(), C.c_size_t()
         _check(lib.pcgb_expander_info(self.h, C.byref(K), C.byref(L), C.byref(nk), C.byref(sb)))

@@ -161,3 +161,53 @@ def test_full_shape_against_independent_paths(pcg):
             zz = (zz + p.astype(object)) % P
             q += 1
     assert (z == np.asarray(zz, dtype=np.uint64)).all()
+
+
+@pytest.mark.parametrize("N,c,t", [(1 << 12, 2, 4), (1 << 12, 3, 4), (1 << 11, 1, 2)])
+def test_public_a0_expander_matches_oracle(pcg, N, c, t):
+    """pcgb_expander_create_public_a0: all c public polynomials given (a_0
+    too).  x and z equal the oracle's step 4 on the oracle's own block
+    outputs, for both parties, and satisfy the OLE relation."""
+    s = O.shape(N, c, t)
+    rng = np.random.default_rng(N + c)
+    a_all = rng.integers(0, P, c * N, dtype=np.uint64)
+    r0, r1, cws, cwo = O.deal_keys(s, 404)
+    e = pcg.Expander(N, c, t, 1, pcg.PRG_CHACHA8, public_a=a_all, a0_public=True)
+    xs, zs = [], []
+    for p in (0, 1):
+        pos, val = O.noise(s, 404, p)
+        _, _, g = O.expand(s, p, (r0, r1)[p], cws, cwo, pos, val,
+                           O.public_a(s, 1) if c > 1 else np.zeros(0, np.uint64), want_g=True)
+        wx, wz = O.step4(N, c, t, pos, val, a_all, g)
+        x, z = e.expand_host(p, (r0, r1)[p], cws, cwo, pos, val)
+        assert (x == wx).all() and (z == wz).all(), p
+        xs.append(x)
+        zs.append(z)
+    prod = O.poly_mul(xs[0], xs[1], N)
+    zz = (zs[0].astype(object) + zs[1].astype(object)) % P
+    assert all(int(u) == int(v) for u, v in zip(prod, zz))
+    e.close()
+
+
+def test_public_a0_expander_ole_relation_full_shape(pcg):
+    """The same mode at N = 2^20, c = 4, t = 16, checked on the device."""
+    N, c, t = 1 << 20, 4, 16
+    a_all = np.random.default_rng(9).integers(0, P, c * N, dtype=np.uint64)
+    e = pcg.Expander(N, c, t, 1, pcg.PRG_CHACHA8, public_a=a_all, a0_public=True)
+    K, L = e.K, e.levels
+    d_r0, d_r1 = pcg.DeviceBuffer(16 * K), pcg.DeviceBuffer(16 * K)
+    d_cws, d_cwo = pcg.DeviceBuffer(16 * K * L), pcg.DeviceBuffer(8 * K)
+    e.deal_keys_device(777, d_r0.ptr, d_r1.ptr, d_cws.ptr, d_cwo.ptr)
+    outs = []
+    for party, d_r in ((0, d_r0), (1, d_r1)):
+        pos, val = pcg.noise(N, c, t, 777, party)
+        d_pos, d_val = dev(pcg, pos), dev(pcg, val)
+        d_x, d_z = pcg.DeviceBuffer(8 * N), pcg.DeviceBuffer(8 * N)
+        e.expand_device(party, d_r.ptr, d_cws.ptr, d_cwo.ptr, d_pos.ptr, d_val.ptr, d_x.ptr,
+                        d_z.ptr)
+        outs += [d_x, d_z]
+    bad = pcg.DeviceBuffer(8)
+    pcg.verify_ole_device(N, *[b.ptr for b in outs], bad.ptr)
+    pcg.synchronize()
+    assert int(bad.download(np.uint64, 1)[0]) == 0
+    e.close()

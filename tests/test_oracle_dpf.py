@@ -85,3 +85,26 @@ def test_ole_relation(N, c, t):
     prod = O.poly_mul(x0, x1, N)
     zz = (z0.astype(object) + z1.astype(object)) % P
     assert all(int(p) == int(q) for p, q in zip(prod, zz))
+
+
+def test_step4_with_a_public_a0_keeps_the_ole_relation():
+    """orc_step4 with a_0 = 1 is orc_expand's own step 4; with a_0 drawn
+    uniformly as well, the two parties' outputs still satisfy
+    z0 + z1 = x0 * x1 (x_p = sum a_i e_i^p, so the relation holds for any a)."""
+    N, c, t = 1 << 10, 2, 4
+    s = O.shape(N, c, t)
+    a = O.public_a(s, 7)
+    r0, r1, cws, cwo = O.deal_keys(s, 55)
+    noise = [O.noise(s, 55, p) for p in (0, 1)]
+    outs = [O.expand(s, p, (r0, r1)[p], cws, cwo, *noise[p], a, want_g=True) for p in (0, 1)]
+    one = np.zeros(N, np.uint64)
+    one[0] = 1
+    for p in (0, 1):
+        x, z = O.step4(N, c, t, *noise[p], np.concatenate([one, a]), outs[p][2])
+        assert (x == outs[p][0]).all() and (z == outs[p][1]).all()
+    a0 = np.random.default_rng(3).integers(0, O.P, N, dtype=np.uint64)
+    (x0, z0), (x1, z1) = [O.step4(N, c, t, *noise[p], np.concatenate([a0, a]), outs[p][2])
+                          for p in (0, 1)]
+    prod = O.poly_mul(x0, x1, N)
+    zz = (z0.astype(object) + z1.astype(object)) % O.P
+    assert all(int(u) == int(v) for u, v in zip(prod, zz))
