@@ -69,3 +69,54 @@ def test_reference_arm_prints_once_under_torchrun():
 
 if __name__ == "__main__":
     sys.exit(pytest.main([__file__, "-q"]))
+
+
+def _z_rank(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "pcg-square_b200"))
+        from pcg_b200 import P
+        from pcg_b200.shard import allreduce_z
+        z = np.random.default_rng(rank).integers(P - 1000, P, 257, dtype=np.uint64)
+        z[:5] = [0, 1, P - 1, P - 2, rank]
+        t = torch.from_numpy(z.view(np.int64).copy())
+        allreduce_z(t)
+        q.put((rank, t.numpy().view(np.uint64).tolist()))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [3, 8])
+def test_shard_z_sum_is_exact_beyond_four_ranks(world):
+    """pcg_b200.shard.allreduce_z: the partial z's (values near p, where a
+    plain uint64 all-reduce of 8 of them would overflow) sum mod p exactly on
+    every rank."""
+    import numpy as np
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_z_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=300) for _ in range(world))
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs)
+    sys.path.insert(0, os.path.join(ROOT, "pcg-square_b200"))
+    from pcg_b200 import P
+    parts = []
+    for r in range(world):
+        z = np.random.default_rng(r).integers(P - 1000, P, 257, dtype=np.uint64)
+        z[:5] = [0, 1, P - 1, P - 2, r]
+        parts.append([int(v) for v in z])
+    want = [sum(col) % P for col in zip(*parts)]
+    for r in range(world):
+        assert got[r] == want, r
