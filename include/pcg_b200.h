@@ -52,6 +52,12 @@ typedef struct pcgb_blk {
  * (reported as PCGB_ECALLBACK).  Replaces the std::function DpfExchangeFn
  * (GPU_baseline/common/dpf_gpu.h:31-32). */
 typedef int (*pcgb_exchange_fn)(const pcgb_blk* my, pcgb_blk* peer, size_t count, void* user);
+/* The same exchange between device arrays (no reference counterpart): the
+ * library has finished writing d_my when it calls; the callback fills
+ * d_peer[0..count) on the same device (NCCL send/recv or peer copies over
+ * NVLink) and returns once the data has landed. */
+typedef int (*pcgb_exchange_device_fn)(const pcgb_blk* d_my, pcgb_blk* d_peer, size_t count,
+                                       void* user);
 
 const char* pcgb_last_error(void);
 int pcgb_version(void); /* major*10000 + minor*100 + patch */
@@ -175,6 +181,13 @@ int pcgb_dpf_batch_full_eval_convert_device(int B, int n, int w, const pcgb_blk*
                                             int party, pcgb_exchange_fn exchange, void* user,
                                             int prg, uint64_t* d_conv, uint64_t* d_sumC,
                                             uint64_t* d_sumT);
+/* Same, with the per-level CW shares exchanged device to device: no host
+ * round trip per level, for parties on separate GPUs. */
+int pcgb_dpf_batch_full_eval_convert_device_dx(int B, int n, int w, const pcgb_blk* roots,
+                                               const pcgb_blk* dltsft, const uint8_t* round_keys,
+                                               int party, pcgb_exchange_device_fn exchange,
+                                               void* user, int prg, uint64_t* d_conv,
+                                               uint64_t* d_sumC, uint64_t* d_sumT);
 int pcgb_dpf_out_scatter_g_conv_device(const uint64_t* d_conv, int B, size_t D, int t, int party,
                                        const uint64_t* d_cw, uint64_t* d_g, int N, void* stream);
 

@@ -21,7 +21,9 @@ const Blk* dpf_interactive_device(int B, int n, int w, const Blk* roots, const B
                                   Blk* host_out);
 void dpf_interactive_convert_device(int B, int n, int w, const Blk* roots, const Blk* dltsft,
                                     const uint8_t* rks, int prg, pcgb_exchange_fn ex, void* user,
-                                    uint64_t* d_conv, uint64_t* d_sumC, uint64_t* d_sumT);
+                                    uint64_t* d_conv, uint64_t* d_sumC, uint64_t* d_sumT,
+                                    pcgb_exchange_device_fn dex = nullptr,
+                                    void* dex_user = nullptr);
 void dpf_out_sums_host(const Blk* d_leaves, int B, size_t D, uint64_t prime, uint64_t* sumC,
                        uint64_t* sumT);
 void dpf_out_scatter_host(const Blk* d_leaves, int B, size_t D, int t, int party, uint64_t prime,
@@ -414,6 +416,22 @@ int pcgb_dpf_batch_full_eval_convert_device(int B, int n, int w, const pcgb_blk*
         pcgb::dpf_interactive_convert_device(B, n, w, reinterpret_cast<const Blk*>(roots),
                                              reinterpret_cast<const Blk*>(dltsft), round_keys, prg,
                                              exchange, user, d_conv, d_sumC, d_sumT);
+    });
+}
+
+int pcgb_dpf_batch_full_eval_convert_device_dx(int B, int n, int w, const pcgb_blk* roots,
+                                               const pcgb_blk* dltsft, const uint8_t* round_keys,
+                                               int party, pcgb_exchange_device_fn exchange,
+                                               void* user, int prg, uint64_t* d_conv,
+                                               uint64_t* d_sumC, uint64_t* d_sumT) {
+    (void)party;
+    if (B <= 0) return PCGB_OK;
+    return guarded([&] {
+        if (!exchange) pcgb::fail(PCGB_EINVAL, "device exchange callback required");
+        pcgb::dpf_interactive_convert_device(B, n, w, reinterpret_cast<const Blk*>(roots),
+                                             reinterpret_cast<const Blk*>(dltsft), round_keys, prg,
+                                             nullptr, nullptr, d_conv, d_sumC, d_sumT, exchange,
+                                             user);
     });
 }
 

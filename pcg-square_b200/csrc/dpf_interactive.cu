@@ -272,10 +272,13 @@ __global__ void convert_fold_kernel(const uint64_t* __restrict__ partials, int p
     sumT[b] = t;
 }
 
-// Where the fused last level writes (see last_level_convert_kernel).
+// Where the fused last level writes (see last_level_convert_kernel), and an
+// optional device-side exchange that replaces the host round trip.
 struct ConvOut {
     uint64_t* conv;
     uint64_t* partials;
+    pcgb_exchange_device_fn dex = nullptr;
+    void* dex_user = nullptr;
 };
 
 // my[b][k] = dlt[b][level][k].
@@ -339,16 +342,26 @@ Blk* run_levels(Pool& pl, int B, int n, const Blk* roots, const Blk* dltsft,
     PCGB_POST_LAUNCH();
     Blk *cur = pl.cur, *nxt = pl.nxt, *H = pl.H, *Hn = pl.Hn, *my = pl.my, *myn = pl.myn;
     for (int i = 0; i < levels; ++i) {
-        PCGB_CK(cudaMemcpyAsync(pl.h_my, my, ncw * sizeof(Blk), cudaMemcpyDeviceToHost, st));
-        PCGB_CK(cudaStreamSynchronize(st));
-        if (ex) {
-            if (ex(reinterpret_cast<const pcgb_blk*>(pl.h_my), reinterpret_cast<pcgb_blk*>(pl.h_peer),
-                   ncw, user) != 0)
-                fail(PCGB_ECALLBACK, "dpf_gpu_batch_full_eval: exchange callback failed");
+        if (conv && conv->dex) {
+            // Shares stay on the device: the callback moves them (NCCL,
+            // peer copies) after the level's reduction has finished.
+            PCGB_CK(cudaStreamSynchronize(st));
+            if (conv->dex(reinterpret_cast<const pcgb_blk*>(my), reinterpret_cast<pcgb_blk*>(pl.peer),
+                          ncw, conv->dex_user) != 0)
+                fail(PCGB_ECALLBACK, "dpf_gpu_batch_full_eval: device exchange callback failed");
         } else {
-            for (size_t k = 0; k < ncw; ++k) pl.h_peer[k] = Blk{0, 0};
+            PCGB_CK(cudaMemcpyAsync(pl.h_my, my, ncw * sizeof(Blk), cudaMemcpyDeviceToHost, st));
+            PCGB_CK(cudaStreamSynchronize(st));
+            if (ex) {
+                if (ex(reinterpret_cast<const pcgb_blk*>(pl.h_my),
+                       reinterpret_cast<pcgb_blk*>(pl.h_peer), ncw, user) != 0)
+                    fail(PCGB_ECALLBACK, "dpf_gpu_batch_full_eval: exchange callback failed");
+            } else {
+                for (size_t k = 0; k < ncw; ++k) pl.h_peer[k] = Blk{0, 0};
+            }
+            PCGB_CK(cudaMemcpyAsync(pl.peer, pl.h_peer, ncw * sizeof(Blk), cudaMemcpyHostToDevice,
+                                    st));
         }
-        PCGB_CK(cudaMemcpyAsync(pl.peer, pl.h_peer, ncw * sizeof(Blk), cudaMemcpyHostToDevice, st));
         const int hash_next = (i + 1 < levels) ? 1 : 0;
         if (hash_next) {
             seed_kernel<<<sgrid, 256, 0, st>>>(myn, pl.dlt, B, levels, NK, i + 1);
@@ -452,7 +465,8 @@ const Blk* dpf_interactive_device(int B, int n, int w, const Blk* roots, const B
 // layer's sums pass: no leaves are stored.  Outputs are complete on return.
 void dpf_interactive_convert_device(int B, int n, int w, const Blk* roots, const Blk* dltsft,
                                     const uint8_t* rks, int prg, pcgb_exchange_fn ex, void* user,
-                                    uint64_t* d_conv, uint64_t* d_sumC, uint64_t* d_sumT) {
+                                    uint64_t* d_conv, uint64_t* d_sumC, uint64_t* d_sumT,
+                                    pcgb_exchange_device_fn dex, void* dex_user) {
     if (B <= 0) return;
     if (!d_conv || !d_sumC || !d_sumT)
         fail(PCGB_EINVAL, "dpf_gpu_batch_full_eval_convert: null output pointer");
@@ -465,7 +479,7 @@ void dpf_interactive_convert_device(int B, int n, int w, const Blk* roots, const
     const int parts = static_cast<int>((last + kTPB - 1) / kTPB);
     uint64_t* partials = static_cast<uint64_t*>(
         pool_alloc(2 * static_cast<size_t>(B) * parts * sizeof(uint64_t), st));
-    const ConvOut conv{d_conv, partials};
+    const ConvOut conv{d_conv, partials, dex, dex_user};
     try {
         interactive_eval(B, n, w, roots, dltsft, rks, prg, ex, user, st, pl, &conv);
     } catch (...) {

@@ -88,6 +88,9 @@ def _load():
         "pcgb_dpf_batch_full_eval_convert_device": ([C.c_int, C.c_int, C.c_int, _vp, _vp, _vp,
                                                      C.c_int, _vp, _vp, C.c_int, _vp, _vp, _vp],
                                                     C.c_int),
+        "pcgb_dpf_batch_full_eval_convert_device_dx": ([C.c_int, C.c_int, C.c_int, _vp, _vp,
+                                                        _vp, C.c_int, _vp, _vp, C.c_int, _vp,
+                                                        _vp, _vp], C.c_int),
         "pcgb_dpf_out_convert_device": ([_vp, C.c_int, C.c_size_t, _vp, _vp, _vp, _vp], C.c_int),
         "pcgb_dpf_out_scatter_g_conv_device": ([_vp, C.c_int, C.c_size_t, C.c_int, C.c_int, _vp,
                                                 _vp, C.c_int, _vp], C.c_int),
@@ -449,6 +452,30 @@ def dpf_gpu_batch_full_eval_convert_device(B, n, w, roots, dltsft, d_conv, d_sum
     _check(lib.pcgb_dpf_batch_full_eval_convert_device(
         B, n, w, _p(roots), _p(dltsft), _p(rk), party, C.cast(cb, C.c_void_p) if cb else None,
         None, prg, d_conv, d_sumC, d_sumT))
+
+
+def dpf_gpu_batch_full_eval_convert_device_dx(B, n, w, roots, dltsft, d_conv, d_sumC, d_sumT,
+                                              exchange_device, round_keys=None, party=0,
+                                              prg=PRG_AES):
+    """As dpf_gpu_batch_full_eval_convert_device, with the per-level CW
+    shares exchanged between device arrays: exchange_device(d_my, d_peer,
+    count) gets device pointers to `count` 16-byte shares and must fill
+    d_peer (and have it landed) before returning."""
+    roots = _blocks(roots, B)
+    dltsft = _blocks(dltsft)
+
+    def cb(my, peer, count, user):
+        try:
+            exchange_device(my, peer, count)
+            return 0
+        except Exception:
+            return 1
+
+    fn = EXCHANGE_FN(cb)
+    rk = None if round_keys is None else _u8(round_keys)
+    _check(lib.pcgb_dpf_batch_full_eval_convert_device_dx(
+        B, n, w, _p(roots), _p(dltsft), _p(rk), party, C.cast(fn, C.c_void_p), None, prg, d_conv,
+        d_sumC, d_sumT))
 
 
 def dpf_out_convert_device(d_leaves, B, D, d_conv, d_sumC, d_sumT, stream=None):

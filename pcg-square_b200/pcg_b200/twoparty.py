@@ -35,7 +35,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import (DeviceBuffer, PRG_CHACHA8, add_mod_p_device,
-               dpf_gpu_batch_full_eval_convert_device, dpf_out_scatter_g_conv_device, gmw_dltsft,
+               dpf_gpu_batch_full_eval_convert_device,
+               dpf_gpu_batch_full_eval_convert_device_dx, dpf_out_scatter_g_conv_device, gmw_dltsft,
                gmw_position_add, out_beaver_close_device, out_beaver_open_device, synchronize,
                to_device)
 
@@ -108,6 +109,43 @@ def _scratch_buf(name, nbytes):
     return b
 
 
+def device_words(ptr, nwords):
+    """A torch int64 view (no copy) of nwords device words at ptr."""
+    import torch
+
+    class _Cai:
+        __cuda_array_interface__ = {"shape": (nwords,), "typestr": "<i8", "data": (ptr, False),
+                                    "version": 3}
+    return torch.as_tensor(_Cai(), device="cuda")
+
+
+class DeviceChannel(Channel):
+    """Exchange for parties on separate GPUs: torch.distributed over NCCL,
+    the messages sent from and received into device memory (the CW shares
+    and Beaver openings never visit the host).  Needs one GPU per party;
+    this pool runs one GPU per job, so it is not exercised on a GPU pair
+    here (the library side is, through a one-GPU loopback)."""
+
+    def exchange_device(self, d_my, d_peer, nwords):
+        my, peer = device_words(d_my, nwords), device_words(d_peer, nwords)
+        if self.party == 0:
+            self.dist.send(my, self.peer)
+            self.dist.recv(peer, self.peer)
+        else:
+            self.dist.recv(peer, self.peer)
+            self.dist.send(my, self.peer)
+        self.torch.cuda.current_stream().synchronize()
+        self.messages += 1
+        self.bytes += 8 * nwords
+
+    def exchange(self, mine):
+        mine = np.ascontiguousarray(mine, np.uint64)
+        t_my = self.torch.from_numpy(mine.view(np.int64).copy()).cuda()
+        t_peer = self.torch.empty_like(t_my)
+        self.exchange_device(t_my.data_ptr(), t_peer.data_ptr(), t_my.numel())
+        return t_peer.cpu().numpy().view(np.uint64).reshape(mine.shape)
+
+
 def _beaver_cw_device(party, chan, nB, d_sumC, d_sumT, beta, r, s, rs, d_cw):
     """Output-layer correction words of nB instances into d_cw (a
     DeviceBuffer of nB words): <A> =
@@ -122,10 +160,18 @@ def _beaver_cw_device(party, chan, nB, d_sumC, d_sumT, beta, r, s, rs, d_cw):
     d_beta, d_r, d_s, d_rs = (d_in.ptr + k * w for k in range(4))
     d_de = _scratch_buf("beaver_de", 4 * w)          # mine (2nB) | peer (2nB)
     out_beaver_open_device(nB, party, d_sumC, d_sumT, d_beta, d_r, d_s, d_de.ptr)
-    peer = chan.exchange(d_de.download(np.uint64, 2 * nB))
-    d_de.upload_at(peer, 2 * w)
-    out_beaver_close_device(nB, party, d_de.ptr, d_de.ptr + 2 * w, d_r, d_s, d_rs, d_cw.ptr)
-    d_peer = _scratch_buf("beaver_cw_peer", w).upload(chan.exchange(d_cw.download(np.uint64, nB)))
+    d_peer = _scratch_buf("beaver_cw_peer", w)
+    if hasattr(chan, "exchange_device"):       # openings stay on the device
+        synchronize()
+        chan.exchange_device(d_de.ptr, d_de.ptr + 2 * w, 2 * nB)
+        out_beaver_close_device(nB, party, d_de.ptr, d_de.ptr + 2 * w, d_r, d_s, d_rs, d_cw.ptr)
+        synchronize()
+        chan.exchange_device(d_cw.ptr, d_peer.ptr, nB)
+    else:
+        peer = chan.exchange(d_de.download(np.uint64, 2 * nB))
+        d_de.upload_at(peer, 2 * w)
+        out_beaver_close_device(nB, party, d_de.ptr, d_de.ptr + 2 * w, d_r, d_s, d_rs, d_cw.ptr)
+        d_peer.upload(chan.exchange(d_cw.download(np.uint64, nB)))
     add_mod_p_device(d_cw.ptr, d_cw.ptr, d_peer.ptr, nB)
 
 
@@ -158,8 +204,15 @@ def gen_and_expand(party, chan, expander, material, prg=PRG_CHACHA8, batched=Tru
         d_cw = _scratch_buf("cw", 8 * nB)
         # DPF levels with their CW exchanges, the last level fused with the
         # sums pass (leaves hashed as they are made, never stored).
-        dpf_gpu_batch_full_eval_convert_device(nB, n, 1, roots, dlt, d_conv.ptr, d_sumC, d_sumT,
-                                               party=party, exchange=chan.exchange, prg=prg)
+        if hasattr(chan, "exchange_device"):
+            dpf_gpu_batch_full_eval_convert_device_dx(
+                nB, n, 1, roots, dlt, d_conv.ptr, d_sumC, d_sumT,
+                lambda d_my, d_peer, count: chan.exchange_device(d_my, d_peer, 2 * count),
+                party=party, prg=prg)
+        else:
+            dpf_gpu_batch_full_eval_convert_device(nB, n, 1, roots, dlt, d_conv.ptr, d_sumC,
+                                                   d_sumT, party=party, exchange=chan.exchange,
+                                                   prg=prg)
         cat = lambda a: np.concatenate([a[b] for b in blocks])
         _beaver_cw_device(party, chan, nB, d_sumC, d_sumT, cat(m.beta), cat(m.r), cat(m.s),
                           cat(m.rs), d_cw)

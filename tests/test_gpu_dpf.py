@@ -129,3 +129,44 @@ def test_interactive_fused_convert_matches_two_calls(pcg, prg, n, w, B):
     assert (s0 == s1).all()
     wc, wt = O.out_sums(leaves, B, D)
     assert (s1[:B] == wc).all() and (s1[B:] == wt).all()
+
+
+@pytest.mark.parametrize("prg", [O.PRG_CHACHA8, O.PRG_AES])
+def test_interactive_fused_convert_device_exchange(pcg, prg):
+    """pcgb_dpf_batch_full_eval_convert_device_dx: the per-level shares go to
+    a device-side callback (here a one-GPU loopback, peer = my ^ mask
+    computed by torch on the device) and the outputs equal the host-exchange
+    call's with the same peer values, one callback per level."""
+    torch = pytest.importorskip("torch")
+    from pcg_b200.twoparty import device_words
+    B, n, w = 64, 12, 1
+    nk, L = (1 << w) - 1, n // w
+    rks = O.aes_tree_round_keys(np.arange(16, dtype=np.uint8), nk) if prg == O.PRG_AES else None
+    rng = np.random.default_rng(77)
+    roots = rng.integers(0, 2**64 - 1, (B, 2), dtype=np.uint64, endpoint=True)
+    dlt = rng.integers(0, 2**64 - 1, (B * L * nk, 2), dtype=np.uint64, endpoint=True)
+    mask = rng.integers(0, 2**64 - 1, (B * nk, 2), dtype=np.uint64, endpoint=True)
+    d_mask = torch.from_numpy(mask.view(np.int64).reshape(-1).copy()).cuda()
+    calls = []
+
+    def dex(d_my, d_peer, count):
+        my, peer = device_words(d_my, 2 * count), device_words(d_peer, 2 * count)
+        peer.copy_(my ^ d_mask)
+        torch.cuda.synchronize()
+        calls.append(count)
+
+    D = 1 << n
+    outs = []
+    for use_dev in (False, True):
+        conv, sums = pcg.DeviceBuffer(8 * B * D), pcg.DeviceBuffer(16 * B)
+        if use_dev:
+            pcg.dpf_gpu_batch_full_eval_convert_device_dx(B, n, w, roots, dlt, conv.ptr, sums.ptr,
+                                                          sums.ptr + 8 * B, dex, round_keys=rks,
+                                                          prg=prg)
+        else:
+            pcg.dpf_gpu_batch_full_eval_convert_device(B, n, w, roots, dlt, conv.ptr, sums.ptr,
+                                                       sums.ptr + 8 * B, round_keys=rks,
+                                                       exchange=lambda my: my ^ mask, prg=prg)
+        outs.append((conv.download(np.uint64, B * D), sums.download(np.uint64, 2 * B)))
+    assert calls == [B * nk] * L
+    assert (outs[0][0] == outs[1][0]).all() and (outs[0][1] == outs[1][1]).all()
