@@ -100,6 +100,13 @@ class Channel:
 _scratch = {}
 
 
+def release_scratch():
+    """Free the device scratch gen_and_expand keeps between calls."""
+    for b in _scratch.values():
+        b.free()
+    _scratch.clear()
+
+
 def _scratch_buf(name, nbytes):
     b = _scratch.get(name)
     if b is None or b.nbytes < nbytes:
