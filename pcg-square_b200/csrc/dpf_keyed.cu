@@ -163,7 +163,7 @@ void keyed_leaf_gather(const GatherPlan& gp, int party, int prg, const Blk* F, c
     if (gp.Qs == 0) return;   // a shard with no pairs
     L.grid = dim3(static_cast<unsigned>(L.bin / (static_cast<size_t>(tpb) * gp.S)),
                   static_cast<unsigned>(gp.t), static_cast<unsigned>(gp.Qs));
-    L.smem = static_cast<size_t>(tpb) * (gp.S + 1) * sizeof(uint64_t) +
+    L.smem = static_cast<size_t>(tpb) * (gp.S + 1) * 2 * sizeof(uint64_t) +
              (prg == PCGB_PRG_AES ? keyed_aes_smem_bytes_aes() : 0);
     L.st = st;
     L.F = F; L.cws = cws; L.cw_out = cw_out;

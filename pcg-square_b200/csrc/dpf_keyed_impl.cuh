@@ -192,23 +192,46 @@ __device__ __forceinline__ void out_hash_x2(const Blk& a, const Blk& b, uint64_t
     hb = out_hash_lo64(b.lo, b.hi);
 }
 
+// Output-layer accumulation with one reduction per output word.  Each
+// position keeps a 128-bit two's-complement sum (lo, hi) of its leaves'
+// y = h + tau*cwo, h the raw 64-bit out-hash word (so y < 2^65), added for
+// one sign and subtracted for the other; it is reduced mod p once, at
+// write-out.  Exact, since only the sum mod p is used, and far from
+// overflow: a position receives at most 4t key halves.  Against reducing h,
+// adding cwo mod p, negating and adding mod p for every leaf, this leaves a
+// few integer adds per leaf on the ALU pipe the ChaCha8 rounds saturate.
 struct LeafCtx {
-    uint64_t* acc;   // shared accumulator row of this thread (stride 1)
-    uint64_t cwo;    // output-layer CW of the current key
-    bool neg;        // party ^ fold
+    ulonglong2* acc;  // this thread's accumulator row: (lo, hi) per position
+    uint64_t cwo;     // output-layer CW of the current key
+    bool neg;         // party ^ fold; the same for every thread of the CTA
 };
 
-__device__ __forceinline__ uint64_t leaf_value(const Blk& leaf, uint64_t h, const LeafCtx& c) {
-    uint64_t y = reduce_p(h);
-    if (leaf.lo & 1) y = add_p(y, c.cwo);
-    return c.neg ? neg_p(y) : y;
+__device__ __forceinline__ void leaf_acc(const Blk& leaf, uint64_t h, int u, const LeafCtx& c) {
+    const unsigned __int128 y =
+        static_cast<unsigned __int128>(h) + ((leaf.lo & 1) ? c.cwo : uint64_t{0});
+    const ulonglong2 a = c.acc[u];
+    unsigned __int128 A = (static_cast<unsigned __int128>(a.y) << 64) | a.x;
+    if (c.neg) A -= y;
+    else A += y;
+    c.acc[u] = make_ulonglong2(static_cast<uint64_t>(A), static_cast<uint64_t>(A >> 64));
+}
+
+// A 128-bit two's-complement accumulator mod p: hi*2^64 + lo with hi a
+// small signed count, and 2^64 = 3*2^27 - 4 (mod p).
+constexpr uint64_t kTwo64ModP = 402653180ULL;
+__device__ __forceinline__ uint64_t acc_mod_p(const ulonglong2& a) {
+    const int64_t hi = static_cast<int64_t>(a.y);
+    const uint64_t mag = hi < 0 ? static_cast<uint64_t>(-hi) : static_cast<uint64_t>(hi);
+    uint64_t t = reduce_p(mag * kTwo64ModP);   // |hi| <= 4t key halves: < 2^55
+    if (hi < 0) t = neg_p(t);
+    return add_p(reduce_p(a.x), t);
 }
 
 __device__ __forceinline__ void leaf_pair(const Blk& a, const Blk& b, int u, LeafCtx& c) {
     uint64_t ha, hb;
     out_hash_x2(a, b, ha, hb);
-    c.acc[u] = add_p(c.acc[u], leaf_value(a, ha, c));
-    c.acc[u + 1] = add_p(c.acc[u + 1], leaf_value(b, hb, c));
+    leaf_acc(a, ha, u, c);
+    leaf_acc(b, hb, u + 1, c);
 }
 
 // Binary (w = 1) subtree of SL levels below `node`, leaves u_base.. in order.
@@ -265,7 +288,7 @@ __global__ void __launch_bounds__(256) leaf_gather_kernel(
     constexpr int M = 1 << W, NK = M - 1;
     constexpr int S = 1 << (W * SL);
     constexpr int STRIDE = S + 1;  // padded accumulator rows: conflict-free
-    extern __shared__ __align__(16) uint64_t acc_s[];
+    extern __shared__ __align__(16) ulonglong2 acc_s[];
     AesSmem& aes_s = *reinterpret_cast<AesSmem*>(acc_s + blockDim.x * STRIDE);
     if constexpr (PRG == kPrgAes) load_aes_smem(aes_s, aes_te, aes_rk, NK);
 
@@ -274,9 +297,9 @@ __global__ void __launch_bounds__(256) leaf_gather_kernel(
     const int slot = q_slot[blockIdx.z];
     const size_t tile = static_cast<size_t>(blockDim.x) * S;
     const size_t o = static_cast<size_t>(blockIdx.x) * tile + static_cast<size_t>(threadIdx.x) * S;
-    uint64_t* acc = acc_s + threadIdx.x * STRIDE;
+    ulonglong2* acc = acc_s + threadIdx.x * STRIDE;
 #pragma unroll
-    for (int u = 0; u < S; ++u) acc[u] = 0;
+    for (int u = 0; u < S; ++u) acc[u] = make_ulonglong2(0, 0);
 
     const size_t per_key = static_cast<size_t>(1) << (W * hl);
     const uint32_t e0 = off[q * t + r], e1 = off[q * t + r + 1];
@@ -298,7 +321,7 @@ __global__ void __launch_bounds__(256) leaf_gather_kernel(
     uint64_t* dst = gq + static_cast<size_t>(slot) * N + static_cast<size_t>(r) * bin +
                     static_cast<size_t>(blockIdx.x) * tile;
     for (size_t e = threadIdx.x; e < tile; e += blockDim.x)
-        dst[e] = acc_s[(e / S) * STRIDE + (e % S)];
+        dst[e] = acc_mod_p(acc_s[(e / S) * STRIDE + (e % S)]);
 }
 
 template <int W, int PRG>
