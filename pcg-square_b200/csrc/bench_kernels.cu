@@ -8,6 +8,8 @@
 // peak for exactly the instruction mix of the DPF kernels.
 #include "pcgb_internal.h"
 
+#include <algorithm>
+
 #include <atomic>
 
 #include "chacha8.cuh"
@@ -59,13 +61,17 @@ double arx_probe(float* ms_out) {
     cudaEvent_t e0, e1;
     PCGB_CK(cudaEventCreate(&e0));
     PCGB_CK(cudaEventCreate(&e1));
-    PCGB_CK(cudaEventRecord(e0, st));
-    arx_probe_kernel<<<blocks, threads, 0, st>>>(2, iters, sink);
-    PCGB_POST_LAUNCH();
-    PCGB_CK(cudaEventRecord(e1, st));
-    PCGB_CK(cudaEventSynchronize(e1));
     float ms = 0;
-    PCGB_CK(cudaEventElapsedTime(&ms, e0, e1));
+    for (int rep = 0; rep < 3; ++rep) {   // the fastest of three launches
+        PCGB_CK(cudaEventRecord(e0, st));
+        arx_probe_kernel<<<blocks, threads, 0, st>>>(2 + rep, iters, sink);
+        PCGB_POST_LAUNCH();
+        PCGB_CK(cudaEventRecord(e1, st));
+        PCGB_CK(cudaEventSynchronize(e1));
+        float t = 0;
+        PCGB_CK(cudaEventElapsedTime(&t, e0, e1));
+        ms = rep == 0 ? t : std::min(ms, t);
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     PCGB_CK(cudaFreeAsync(sink, st));

@@ -44,6 +44,17 @@ __device__ __forceinline__ uint64_t leaf_C(const ulonglong2& v) {
 
 constexpr uint64_t kTauBit = uint64_t{1} << 63;
 
+// Sums are kept as 128-bit integers and reduced mod p once per output:
+// hi*2^64 + lo with hi small and signed, and 2^64 = 3*2^27 - 4 (mod p).
+constexpr uint64_t kTwo64ModP = 402653180ULL;
+__device__ __forceinline__ uint64_t mod_p_128(unsigned __int128 a) {
+    const int64_t hi = static_cast<int64_t>(static_cast<uint64_t>(a >> 64));
+    const uint64_t mag = hi < 0 ? static_cast<uint64_t>(-hi) : static_cast<uint64_t>(hi);
+    uint64_t t = reduce_p(mag * kTwo64ModP);   // |hi| < 2^35: no wrap
+    if (hi < 0) t = neg_p(t);
+    return add_p(reduce_p(static_cast<uint64_t>(a)), t);
+}
+
 // grid = (parts, B): partials[b*parts + part] (C lane), [B*parts + ...] (T lane).
 // KEEP: also write conv[b*D + d] = C | tau << 63.
 template <bool KEEP>
@@ -54,14 +65,20 @@ __global__ void __launch_bounds__(kTPB) out_sum_kernel(const ulonglong2* __restr
     const int b = blockIdx.y, parts = gridDim.x;
     const ulonglong2* L = leaves + static_cast<size_t>(b) * D;
     uint64_t c = 0, t = 0;
+    unsigned __int128 c128 = 0;   // without KEEP: raw hash words, reduced at the end
     for (size_t d = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; d < D;
          d += static_cast<size_t>(parts) * blockDim.x) {
         const ulonglong2 v = __ldg(L + d);
-        const uint64_t C = leaf_C(v);
-        c = add_p(c, C);
         t += v.x & 1;
-        if (KEEP) conv[static_cast<size_t>(b) * D + d] = C | (v.x << 63);
+        if (KEEP) {
+            const uint64_t C = leaf_C(v);
+            c = add_p(c, C);
+            conv[static_cast<size_t>(b) * D + d] = C | (v.x << 63);
+        } else {
+            c128 += out_hash_lo64(v.x, v.y);
+        }
     }
+    if (!KEEP) c = mod_p_128(c128);
 #pragma unroll
     for (int off = 16; off; off >>= 1) {
         c = add_p(c, __shfl_xor_sync(0xffffffffu, c, off));
@@ -92,22 +109,21 @@ __global__ void out_fold_kernel(const uint64_t* __restrict__ partials, int parts
     sums[B + b] = t;
 }
 
-// y = C + tau*CW of one leaf, from the leaf itself (hashed) or from its
-// converted word.
-__device__ __forceinline__ uint64_t leaf_y(const ulonglong2* leaves, size_t i, uint64_t cw) {
+// y = C + tau*CW of one leaf up to a multiple of p (below 2^65), from the
+// leaf itself (the raw hash word stands for C) or from its converted word.
+__device__ __forceinline__ unsigned __int128 leaf_y(const ulonglong2* leaves, size_t i,
+                                                    uint64_t cw) {
     const ulonglong2 v = __ldg(leaves + i);
-    const uint64_t y = leaf_C(v);
-    return (v.x & 1) ? add_p(y, cw) : y;
+    return static_cast<unsigned __int128>(out_hash_lo64(v.x, v.y)) + ((v.x & 1) ? cw : 0);
 }
-__device__ __forceinline__ uint64_t leaf_y(const uint64_t* conv, size_t i, uint64_t cw) {
+__device__ __forceinline__ unsigned __int128 leaf_y(const uint64_t* conv, size_t i, uint64_t cw) {
     const uint64_t w = __ldg(conv + i);
-    const uint64_t y = w & ~kTauBit;
-    return (w & kTauBit) ? add_p(y, cw) : y;
+    return static_cast<unsigned __int128>(w & ~kTauBit) + ((w & kTauBit) ? cw : 0);
 }
 
 // Gather scatter: thread per output word p < N.
 template <class In>
-__global__ void __launch_bounds__(kTPB) out_gather_kernel(const In* __restrict__ leaves,
+__global__ void __launch_bounds__(kTPB, 4) out_gather_kernel(const In* __restrict__ leaves,
                                                           int B, size_t D, int t, int party,
                                                           const uint64_t* __restrict__ cws,
                                                           uint64_t* __restrict__ g, size_t N) {
@@ -116,7 +132,7 @@ __global__ void __launch_bounds__(kTPB) out_gather_kernel(const In* __restrict__
     const size_t bin = D >> 1;
     const int kk_max = (B - 1) / t;
     const long s_max = static_cast<long>(kk_max) + t - 1;
-    uint64_t acc = 0;
+    unsigned __int128 acc = 0;   // two's complement; reduced mod p once, below
     for (int f = 0; f < 2; ++f) {
         const size_t P = p + (f ? N : 0);   // pre-fold position
         const long s_hi = static_cast<long>(P / bin);
@@ -129,13 +145,14 @@ __global__ void __launch_bounds__(kTPB) out_gather_kernel(const In* __restrict__
             for (int kk = kk0; kk <= kk1; ++kk) {
                 const int b = kk * t + static_cast<int>(s - kk);
                 if (b >= B) continue;
-                uint64_t y = leaf_y(leaves, static_cast<size_t>(b) * D + d, __ldg(cws + b));
-                if ((party != 0) != (f != 0)) y = neg_p(y);
-                acc = add_p(acc, y);
+                const unsigned __int128 y =
+                    leaf_y(leaves, static_cast<size_t>(b) * D + d, __ldg(cws + b));
+                if ((party != 0) != (f != 0)) acc -= y;
+                else acc += y;
             }
         }
     }
-    g[p] = acc;
+    g[p] = mod_p_128(acc);
 }
 
 __global__ void beaver_open_kernel(int B, int party, const uint64_t* __restrict__ sumC,
