@@ -304,7 +304,7 @@ def run_ours(args, d):
     K, levels = e.K, e.levels
     seed = 1000 + d.rank
     d_r0, d_r1 = L.DeviceBuffer(16 * K), L.DeviceBuffer(16 * K)
-    d_cws, d_cwo = L.DeviceBuffer(16 * K * levels), L.DeviceBuffer(8 * K)
+    d_cws, d_cwo = L.DeviceBuffer(16 * K * levels * e.nk), L.DeviceBuffer(8 * K)
     e.deal_keys_device(seed, d_r0.ptr, d_r1.ptr, d_cws.ptr, d_cwo.ptr)
     pos0, val0 = L.noise(N, C_, T_, seed, 0)
     pos1, val1 = L.noise(N, C_, T_, seed, 1)

@@ -55,7 +55,7 @@ def main():
     e = L.Expander(N, c, t, 1, L.PRG_CHACHA8, public_a=a)
     K = e.K
     d_r0, d_r1 = L.DeviceBuffer(16 * K), L.DeviceBuffer(16 * K)
-    d_cws, d_cwo = L.DeviceBuffer(16 * K * levels), L.DeviceBuffer(8 * K)
+    d_cws, d_cwo = L.DeviceBuffer(16 * K * levels * e.nk), L.DeviceBuffer(8 * K)
     e.deal_keys_device(args.seed, d_r0.ptr, d_r1.ptr, d_cws.ptr, d_cwo.ptr)
     roots = d_r0.download(np.uint64, 2 * K).reshape(K, 2)
     cws = d_cws.download(np.uint64, 2 * K * levels).reshape(K, levels, 2)

@@ -95,7 +95,7 @@ def test_ole_relation_full_shape(pcg):
     e = pcg.Expander(N, c, t, 1, pcg.PRG_CHACHA8, public_a=a)
     K, L = e.K, e.levels
     d_r0, d_r1 = pcg.DeviceBuffer(16 * K), pcg.DeviceBuffer(16 * K)
-    d_cws, d_cwo = pcg.DeviceBuffer(16 * K * L), pcg.DeviceBuffer(8 * K)
+    d_cws, d_cwo = pcg.DeviceBuffer(16 * K * L * e.nk), pcg.DeviceBuffer(8 * K)
     e.deal_keys_device(31337, d_r0.ptr, d_r1.ptr, d_cws.ptr, d_cwo.ptr)
     xs, zs = [], []
     for party, d_r in ((0, d_r0), (1, d_r1)):
@@ -125,7 +125,7 @@ def test_full_shape_against_independent_paths(pcg):
     e1 = pcg.Expander(N, c, t, 1, pcg.PRG_CHACHA8, public_a=a)
     K, L = e1.K, e1.levels
     d_r0, d_r1 = pcg.DeviceBuffer(16 * K), pcg.DeviceBuffer(16 * K)
-    d_cws, d_cwo = pcg.DeviceBuffer(16 * K * L), pcg.DeviceBuffer(8 * K)
+    d_cws, d_cwo = pcg.DeviceBuffer(16 * K * L * e1.nk), pcg.DeviceBuffer(8 * K)
     e1.deal_keys_device(seed, d_r0.ptr, d_r1.ptr, d_cws.ptr, d_cwo.ptr)
     pos, val = pcg.noise(N, c, t, seed, 0)
     d_pos, d_val = dev(pcg, pos), dev(pcg, val)
@@ -196,7 +196,7 @@ def test_public_a0_expander_ole_relation_full_shape(pcg):
     e = pcg.Expander(N, c, t, 1, pcg.PRG_CHACHA8, public_a=a_all, a0_public=True)
     K, L = e.K, e.levels
     d_r0, d_r1 = pcg.DeviceBuffer(16 * K), pcg.DeviceBuffer(16 * K)
-    d_cws, d_cwo = pcg.DeviceBuffer(16 * K * L), pcg.DeviceBuffer(8 * K)
+    d_cws, d_cwo = pcg.DeviceBuffer(16 * K * L * e.nk), pcg.DeviceBuffer(8 * K)
     e.deal_keys_device(777, d_r0.ptr, d_r1.ptr, d_cws.ptr, d_cwo.ptr)
     outs = []
     for party, d_r in ((0, d_r0), (1, d_r1)):

@@ -15,7 +15,7 @@ def _material(pcg, N, c, t, seed):
     e = pcg.Expander(N, c, t, 1, pcg.PRG_CHACHA8, public_a=a)
     K, L = e.K, e.levels
     d = {k: pcg.DeviceBuffer(n) for k, n in
-         (("r0", 16 * K), ("r1", 16 * K), ("cws", 16 * K * L), ("cwo", 8 * K))}
+         (("r0", 16 * K), ("r1", 16 * K), ("cws", 16 * K * L * e.nk), ("cwo", 8 * K))}
     e.deal_keys_device(seed, d["r0"].ptr, d["r1"].ptr, d["cws"].ptr, d["cwo"].ptr)
     pos, val = pcg.noise(N, c, t, seed, 0)
     d["pos"], d["val"] = pcg.to_device(pos), pcg.to_device(val)

@@ -15,7 +15,7 @@ def direct_digests(pcg, N, c, t, seed, party):
     e = pcg.Expander(N, c, t, 1, pcg.PRG_CHACHA8, public_a=a)
     K, L = e.K, e.levels
     r0, r1 = pcg.DeviceBuffer(16 * K), pcg.DeviceBuffer(16 * K)
-    cws, cwo = pcg.DeviceBuffer(16 * K * L), pcg.DeviceBuffer(8 * K)
+    cws, cwo = pcg.DeviceBuffer(16 * K * L * e.nk), pcg.DeviceBuffer(8 * K)
     e.deal_keys_device(seed, r0.ptr, r1.ptr, cws.ptr, cwo.ptr)
     pos, val = pcg.noise(N, c, t, seed, party)
     dp, dv = pcg.to_device(pos), pcg.to_device(val)

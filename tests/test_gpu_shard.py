@@ -20,7 +20,7 @@ P = O.P
 def _expand(pcg, e, N, c, t, seed, party=0):
     K, L = e.K, e.levels
     r0, r1 = pcg.DeviceBuffer(16 * K), pcg.DeviceBuffer(16 * K)
-    cws, cwo = pcg.DeviceBuffer(16 * K * L), pcg.DeviceBuffer(8 * K)
+    cws, cwo = pcg.DeviceBuffer(16 * K * L * e.nk), pcg.DeviceBuffer(8 * K)
     e.deal_keys_device(seed, r0.ptr, r1.ptr, cws.ptr, cwo.ptr)
     pos, val = pcg.noise(N, c, t, seed, party)
     dp, dv = pcg.to_device(pos), pcg.to_device(val)

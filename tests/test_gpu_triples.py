@@ -26,12 +26,12 @@ def test_triples_match_oracle(pcg, N, party):
         assert (g == w).all()
 
 
-def _expand_both(pcg, N, c, t, seed):
+def _expand_both(pcg, N, c, t, seed, w=1):
     s = O.shape(N, c, t)
-    e = pcg.Expander(N, c, t, 1, pcg.PRG_CHACHA8, public_a=O.public_a(s, 7))
+    e = pcg.Expander(N, c, t, w, pcg.PRG_CHACHA8, public_a=O.public_a(s, 7))
     K, L = e.K, e.levels
     r0, r1 = pcg.DeviceBuffer(16 * K), pcg.DeviceBuffer(16 * K)
-    cws, cwo = pcg.DeviceBuffer(16 * K * L), pcg.DeviceBuffer(8 * K)
+    cws, cwo = pcg.DeviceBuffer(16 * K * L * e.nk), pcg.DeviceBuffer(8 * K)
     e.deal_keys_device(seed, r0.ptr, r1.ptr, cws.ptr, cwo.ptr)
     outs = []
     for party, roots in ((0, r0), (1, r1)):
@@ -90,3 +90,31 @@ def test_triples_rejects_bad_args(pcg):
         pcg.triples_device(6, 0, *([b.ptr] * 7))
     with pytest.raises(pcg.PcgError):
         pcg.triples_device(8, 2, *([b.ptr] * 7))
+
+
+@pytest.mark.parametrize("w", [1, 2, 3])
+def test_triples_at_the_reference_test_shape(pcg, w):
+    """The reference's triple test shape (CPU_baseline/test/triple.cpp:
+    N = 128, t = 4, w in {1, 2, 3}): two OLEs from the fused expansion, their
+    triples, and c0 + c1 = (a0 + a1)(b0 + b1) in every slot, checked on the
+    device and on the host."""
+    N = 128
+    oles = [_expand_both(pcg, N, 2, 4, seed, w) for seed in (11, 22)]
+    bad = pcg.DeviceBuffer(8)
+    for (x0, z0), (x1, z1) in oles:
+        pcg.verify_ole_device(N, x0.ptr, z0.ptr, x1.ptr, z1.ptr, bad.ptr)
+        assert int(bad.download(np.uint64, 1)[0]) == 0
+    shares = []
+    for party in (0, 1):
+        (x1, z1), (x2, z2) = oles[0][party], oles[1][party]
+        out = [pcg.DeviceBuffer(8 * N) for _ in range(3)]
+        pcg.triples_device(N, party, x1.ptr, z1.ptr, x2.ptr, z2.ptr, *[b.ptr for b in out])
+        shares.append([b.download(np.uint64, N) for b in out])
+        want = O.triples(N, party, x1.download(np.uint64, N), z1.download(np.uint64, N),
+                         x2.download(np.uint64, N), z2.download(np.uint64, N))
+        for g, ww in zip(shares[-1], want):
+            assert (g == ww).all()
+    (a0, b0, c0), (a1, b1, c1) = shares
+    for k in range(N):
+        lhs = (int(a0[k]) + int(a1[k])) % P * ((int(b0[k]) + int(b1[k])) % P) % P
+        assert lhs == (int(c0[k]) + int(c1[k])) % P, k
