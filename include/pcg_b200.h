@@ -257,6 +257,19 @@ int pcgb_aes_tree_round_keys(const uint8_t master[16], int nk, uint8_t* round_ke
 int pcgb_dpf_keyed_full_eval(int K, int n, int w, int prg, const pcgb_blk* d_roots,
                              const pcgb_blk* d_cws, const uint8_t* round_keys,
                              pcgb_blk* d_leaves, void* stream);
+/* Keyed full-domain evaluation of several key groups with different domains
+ * in one batch (no reference counterpart): group g has K[g] keys of domain
+ * 2^n[g]; all share w, the PRG and its round keys.  d_roots[g] (K[g]
+ * blocks), d_cws[g] ([K[g]][n[g]/w][2^w-1]) and d_leaves[g] ([K[g]][2^n[g]])
+ * are device arrays; K, n and the pointer arrays are host arrays.  One
+ * launch per top-walk stage serves every group (a persistent grid over a
+ * per-stage job table), so the batch takes as many launches as its deepest
+ * group has stages.  Leaves equal pcgb_dpf_keyed_full_eval's per group. */
+int pcgb_dpf_keyed_full_eval_multi(int groups, const int* K, const int* n, int w, int prg,
+                                   const pcgb_blk* const* d_roots, const pcgb_blk* const* d_cws,
+                                   const uint8_t* round_keys, pcgb_blk* const* d_leaves,
+                                   void* stream);
+
 
 /* ---- native: batched NTT ----------------------------------------------- */
 /* c[k] = a[k] * b[k] mod (X^N + 1) for k < batch (device, c may alias). */

@@ -541,6 +541,39 @@ int pcgb_aes_tree_round_keys(const uint8_t master[16], int nk, uint8_t* round_ke
 }
 
 // ---- keyed DPF --------------------------------------------------------------
+int pcgb_dpf_keyed_full_eval_multi(int groups, const int* K, const int* n, int w, int prg,
+                                   const pcgb_blk* const* d_roots, const pcgb_blk* const* d_cws,
+                                   const uint8_t* round_keys, pcgb_blk* const* d_leaves,
+                                   void* stream) {
+    if (groups <= 0) return PCGB_OK;
+    return guarded([&] {
+        if (prg != PCGB_PRG_AES && prg != PCGB_PRG_CHACHA8)
+            pcgb::fail(PCGB_EINVAL, "keyed eval multi: unknown PRG");
+        if (prg == PCGB_PRG_AES && !round_keys)
+            pcgb::fail(PCGB_EINVAL, "keyed eval multi: AES needs round keys");
+        if (w < 1 || w > 4) pcgb::fail(PCGB_EINVAL, "keyed eval multi: w must be in [1,4]");
+        cudaStream_t st = pcgb::as_stream(stream);
+        uint32_t* d_rk = nullptr;
+        if (prg == PCGB_PRG_AES) d_rk = pcgb::aes_upload_round_keys(round_keys, (1 << w) - 1, st);
+        try {
+            pcgb::keyed_full_eval_multi(groups, K, n, w, prg,
+                                        reinterpret_cast<const Blk* const*>(d_roots),
+                                        reinterpret_cast<const Blk* const*>(d_cws), d_rk,
+                                        reinterpret_cast<Blk* const*>(d_leaves), st);
+        } catch (...) {
+            if (d_rk) {
+                cudaStreamSynchronize(st);
+                cudaFree(d_rk);
+            }
+            throw;
+        }
+        if (d_rk) {   // a plain allocation: free once the launches that read it are done
+            PCGB_CK(cudaStreamSynchronize(st));
+            cudaFree(d_rk);
+        }
+    });
+}
+
 int pcgb_dpf_keyed_full_eval(int K, int n, int w, int prg, const pcgb_blk* d_roots,
                              const pcgb_blk* d_cws, const uint8_t* round_keys,
                              pcgb_blk* d_leaves, void* stream) {

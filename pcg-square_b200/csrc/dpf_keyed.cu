@@ -47,6 +47,76 @@ void keyed_expand_tops(int K, int n, int w, int prg, const Blk* roots, const Blk
         keyed_tops_chacha(K, levels, w, roots, cws, nullptr, nullptr, to_level, out, scratch, st);
 }
 
+// Stage plan of a multi-group evaluation: every group walks its own
+// geometric stages (tops_stages) with its own ping-pong scratch; launch s
+// carries stage s of every group that has one, so the whole batch takes as
+// many launches as its deepest plan has stages.
+void keyed_full_eval_multi(int groups, const int* K, const int* n, int w, int prg,
+                           const Blk* const* roots, const Blk* const* cws, const uint32_t* d_rk,
+                           Blk* const* leaves, cudaStream_t st) {
+    if (groups <= 0) return;
+    if (!K || !n || !roots || !cws || !leaves) fail(PCGB_EINVAL, "keyed eval multi: null array");
+    if (w < 1 || w > 4) fail(PCGB_EINVAL, "keyed eval multi: w must be in [1,4]");
+    if (prg == PCGB_PRG_AES && !d_rk) fail(PCGB_EINVAL, "keyed eval multi: AES needs round keys");
+    struct Plan {
+        std::vector<int> b;
+        size_t half = 0, off = 0;
+        int levels = 0;
+    };
+    std::vector<Plan> plan(groups);
+    size_t scratch_nodes = 0;
+    size_t stages = 0;
+    for (int g = 0; g < groups; ++g) {
+        if (K[g] < 0) fail(PCGB_EINVAL, "keyed eval multi: negative key count");
+        if (K[g] == 0) continue;
+        if (n[g] < 1 || n[g] > 30 || n[g] % w) fail(PCGB_EINVAL, "keyed eval multi: bad (n, w)");
+        if (!roots[g] || !cws[g] || !leaves[g]) fail(PCGB_EINVAL, "keyed eval multi: null group buffer");
+        Plan& P = plan[g];
+        P.levels = n[g] / w;
+        P.b = tops_stages(K[g], w, P.levels);
+        if (P.b.size() > 2) P.half = static_cast<size_t>(K[g]) << (w * P.b[P.b.size() - 2]);
+        P.off = scratch_nodes;
+        scratch_nodes += 2 * P.half;
+        stages = std::max(stages, P.b.size() - 1);
+    }
+    if (stages == 0) return;
+    Blk* scratch = scratch_nodes ? static_cast<Blk*>(pool_alloc(scratch_nodes * sizeof(Blk), st))
+                                 : nullptr;
+    TopsJob* d_jobs = static_cast<TopsJob*>(pool_alloc(groups * sizeof(TopsJob), st));
+    try {
+        for (size_t s = 0; s < stages; ++s) {
+            std::vector<TopsJob> jobs;
+            unsigned long long total = 0;
+            for (int g = 0; g < groups; ++g) {
+                const Plan& P = plan[g];
+                if (K[g] == 0 || s + 1 >= P.b.size()) continue;
+                Blk* base = scratch ? scratch + P.off : nullptr;
+                TopsJob J;
+                J.src = s == 0 ? roots[g] : base + ((s - 1) % 2) * P.half;
+                J.dst = (s + 2 == P.b.size()) ? leaves[g] : base + (s % 2) * P.half;
+                J.cws = cws[g];
+                J.first = total;
+                J.K = K[g];
+                J.src_lvl = P.b[s];
+                J.nlev = P.b[s + 1] - P.b[s];
+                J.levels = P.levels;
+                total += static_cast<unsigned long long>(K[g]) << (w * P.b[s]);
+                jobs.push_back(J);
+            }
+            if (prg == PCGB_PRG_AES)
+                keyed_tops_multi_aes(w, jobs, d_jobs, total, aes_te_table_device(), d_rk, st);
+            else
+                keyed_tops_multi_chacha(w, jobs, d_jobs, total, st);
+        }
+    } catch (...) {
+        if (scratch) cudaFreeAsync(scratch, st);
+        cudaFreeAsync(d_jobs, st);
+        throw;
+    }
+    if (scratch) PCGB_CK(cudaFreeAsync(scratch, st));
+    PCGB_CK(cudaFreeAsync(d_jobs, st));
+}
+
 // Gather plan: for pair q = (i <= j) and output bin r, the key halves of
 // blocks (i,j) and (j,i) whose leaves land in [r*bin, (r+1)*bin) after the
 // X^N = -1 fold.  Key (kk, ll) of a block covers pre-fold positions

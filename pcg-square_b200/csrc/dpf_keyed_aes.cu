@@ -19,6 +19,11 @@ void keyed_deal_aes(int w, unsigned grid, size_t smem, uint64_t seed, int c, int
                        r2, st);
 }
 
+void keyed_tops_multi_aes(int w, const std::vector<TopsJob>& jobs, TopsJob* d_jobs,
+                             unsigned long long total, const uint32_t* te, const uint32_t* rk, cudaStream_t st) {
+    tops_multi_for_prg<kPrgAes>(w, jobs, d_jobs, total, te, rk, st);
+}
+
 size_t keyed_aes_smem_bytes_aes() { return sizeof(AesSmem); }
 
 }  // namespace pcgb

@@ -19,6 +19,11 @@ void keyed_deal_chacha(int w, unsigned grid, size_t smem, uint64_t seed, int c, 
                        r2, st);
 }
 
+void keyed_tops_multi_chacha(int w, const std::vector<TopsJob>& jobs, TopsJob* d_jobs,
+                             unsigned long long total, cudaStream_t st) {
+    tops_multi_for_prg<kPrgChaCha>(w, jobs, d_jobs, total, nullptr, nullptr, st);
+}
+
 size_t keyed_aes_smem_bytes_chacha() { return sizeof(AesSmem); }
 
 }  // namespace pcgb

@@ -130,19 +130,15 @@ __device__ __forceinline__ void hash_raw(const Blk& p, const AesSmem* aes, Blk (
 
 // ---------------------------------------------------------------------------
 // expand_tops: depth-first expansion of `nlev` levels below each source node.
+// Thread `id` (< K * m^src_lvl) expands source node id: key id / m^src_lvl.
 template <int W, int PRG>
-__global__ void __launch_bounds__(128) expand_tops_kernel(
-    const Blk* __restrict__ src, int K, int src_lvl, int nlev, int levels,
-    const Blk* __restrict__ cws, const uint32_t* __restrict__ aes_te,
-    const uint32_t* __restrict__ aes_rk, Blk* __restrict__ dst) {
+__device__ __forceinline__ void tops_walk(const Blk* __restrict__ src, size_t id, int src_lvl,
+                                          int nlev, int levels, const Blk* __restrict__ cws,
+                                          const AesSmem* aes, Blk* __restrict__ dst) {
     constexpr int M = 1 << W, NK = M - 1;
     constexpr int MAXD = tops_max_depth<W>();
-    extern __shared__ __align__(16) uint64_t tops_dsm[];
-    AesSmem& aes_s = *reinterpret_cast<AesSmem*>(tops_dsm);
-    if constexpr (PRG == kPrgAes) load_aes_smem(aes_s, aes_te, aes_rk, NK);
+    const AesSmem& aes_s = *aes;
     const size_t per_key_src = static_cast<size_t>(1) << (W * src_lvl);
-    const size_t id = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (id >= static_cast<size_t>(K) * per_key_src) return;
     const size_t key = id / per_key_src;
     const size_t j = id % per_key_src;
     const Blk* kcw = cws + key * static_cast<size_t>(levels) * NK;
@@ -179,6 +175,41 @@ __global__ void __launch_bounds__(128) expand_tops_kernel(
         for (int k = 0; k < M; ++k) stack[d + 1][k] = kids[k];
         ++d;
         pos[d] = 0;
+    }
+}
+
+template <int W, int PRG>
+__global__ void __launch_bounds__(128) expand_tops_kernel(
+    const Blk* __restrict__ src, int K, int src_lvl, int nlev, int levels,
+    const Blk* __restrict__ cws, const uint32_t* __restrict__ aes_te,
+    const uint32_t* __restrict__ aes_rk, Blk* __restrict__ dst) {
+    constexpr int NK = (1 << W) - 1;
+    extern __shared__ __align__(16) uint64_t tops_dsm[];
+    AesSmem& aes_s = *reinterpret_cast<AesSmem*>(tops_dsm);
+    if constexpr (PRG == kPrgAes) load_aes_smem(aes_s, aes_te, aes_rk, NK);
+    const size_t id = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (id >= (static_cast<size_t>(K) << (W * src_lvl))) return;
+    tops_walk<W, PRG>(src, id, src_lvl, nlev, levels, cws, &aes_s, dst);
+}
+
+// One stage of several key groups of different domains in one persistent
+// launch: the grid strides over the concatenated source nodes of all jobs;
+// job j owns global thread indices [first, first + K << (W * src_lvl)).
+template <int W, int PRG>
+__global__ void __launch_bounds__(128) expand_tops_multi_kernel(
+    const TopsJob* __restrict__ jobs, int njobs, unsigned long long total,
+    const uint32_t* __restrict__ aes_te, const uint32_t* __restrict__ aes_rk) {
+    constexpr int NK = (1 << W) - 1;
+    extern __shared__ __align__(16) uint64_t tops_dsm[];
+    AesSmem& aes_s = *reinterpret_cast<AesSmem*>(tops_dsm);
+    if constexpr (PRG == kPrgAes) load_aes_smem(aes_s, aes_te, aes_rk, NK);
+    for (unsigned long long g = static_cast<unsigned long long>(blockIdx.x) * blockDim.x +
+                                threadIdx.x;
+         g < total; g += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        int j = 0;
+        while (j + 1 < njobs && jobs[j + 1].first <= g) ++j;
+        const TopsJob J = jobs[j];
+        tops_walk<W, PRG>(J.src, g - J.first, J.src_lvl, J.nlev, J.levels, J.cws, &aes_s, J.dst);
     }
 }
 
@@ -419,6 +450,38 @@ void tops_for_prg(int K, int levels, int w, const Blk* roots, const Blk* cws, co
         case 2: tops_dispatch<2, PRG>(K, levels, roots, cws, te, rk, to_level, out, scratch, st); break;
         case 3: tops_dispatch<3, PRG>(K, levels, roots, cws, te, rk, to_level, out, scratch, st); break;
         case 4: tops_dispatch<4, PRG>(K, levels, roots, cws, te, rk, to_level, out, scratch, st); break;
+        default: fail(PCGB_EINVAL, "w must be in [1,4]");
+    }
+}
+
+template <int W, int PRG>
+void tops_multi_launch(const std::vector<TopsJob>& jobs, TopsJob* d_jobs,
+                       unsigned long long total, const uint32_t* te, const uint32_t* rk,
+                       cudaStream_t st) {
+    for (const TopsJob& J : jobs)
+        if (J.nlev < 0 || J.nlev >= tops_max_depth<W>())
+            fail(PCGB_EINVAL, "keyed expansion deeper than the DFS stack");
+    PCGB_CK(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(TopsJob),
+                            cudaMemcpyHostToDevice, st));
+    const int TPB = 128;
+    const size_t smem = PRG == kPrgAes ? sizeof(AesSmem) : 0;
+    const unsigned long long blocks = (total + TPB - 1) / TPB;
+    const unsigned long long cap = static_cast<unsigned long long>(sm_count()) * 8;  // persistent
+    expand_tops_multi_kernel<W, PRG><<<static_cast<unsigned>(blocks < cap ? blocks : cap), TPB,
+                                      smem, st>>>(d_jobs, static_cast<int>(jobs.size()), total,
+                                                  te, rk);
+    PCGB_POST_LAUNCH();
+}
+
+template <int PRG>
+void tops_multi_for_prg(int w, const std::vector<TopsJob>& jobs, TopsJob* d_jobs,
+                        unsigned long long total, const uint32_t* te, const uint32_t* rk,
+                        cudaStream_t st) {
+    switch (w) {
+        case 1: tops_multi_launch<1, PRG>(jobs, d_jobs, total, te, rk, st); break;
+        case 2: tops_multi_launch<2, PRG>(jobs, d_jobs, total, te, rk, st); break;
+        case 3: tops_multi_launch<3, PRG>(jobs, d_jobs, total, te, rk, st); break;
+        case 4: tops_multi_launch<4, PRG>(jobs, d_jobs, total, te, rk, st); break;
         default: fail(PCGB_EINVAL, "w must be in [1,4]");
     }
 }

@@ -70,6 +70,25 @@ int sm_count();
 // must hold K * m^min(to_level, first_stage_levels) nodes (may be nullptr
 // when to_level is small; see keyed_tops_scratch_nodes).
 size_t keyed_tops_scratch_nodes(int K, int w, int to_level);
+
+// One key group's part of a multi-group top-walk stage (expand_tops_multi_kernel).
+struct TopsJob {
+    const Blk* src;             // source nodes [K][m^src_lvl]
+    Blk* dst;                   // written nodes [K][m^(src_lvl + nlev)]
+    const Blk* cws;             // the group's CWs [K][levels][m-1]
+    unsigned long long first;   // first global thread index of this job
+    int K, src_lvl, nlev, levels;
+};
+// Full-domain evaluation of `groups` key groups of different domains (same
+// w and PRG): one launch per top-walk stage for all groups.
+void keyed_full_eval_multi(int groups, const int* K, const int* n, int w, int prg,
+                           const Blk* const* roots, const Blk* const* cws, const uint32_t* d_rk,
+                           Blk* const* leaves, cudaStream_t st);
+void keyed_tops_multi_chacha(int w, const std::vector<TopsJob>& jobs, TopsJob* d_jobs,
+                             unsigned long long total, cudaStream_t st);
+void keyed_tops_multi_aes(int w, const std::vector<TopsJob>& jobs, TopsJob* d_jobs,
+                          unsigned long long total, const uint32_t* te, const uint32_t* rk,
+                          cudaStream_t st);
 void keyed_expand_tops(int K, int n, int w, int prg, const Blk* roots, const Blk* cws,
                        const uint32_t* d_aes_rk, int to_level, Blk* out, Blk* scratch,
                        cudaStream_t st);

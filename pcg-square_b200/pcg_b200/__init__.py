@@ -111,6 +111,9 @@ def _load():
         "pcgb_aes_tree_round_keys": ([_u8p, C.c_int, _u8p], C.c_int),
         "pcgb_dpf_keyed_full_eval": ([C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp],
                                      C.c_int),
+        "pcgb_dpf_keyed_full_eval_multi": ([C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                            C.c_int, C.c_int, C.POINTER(_vp), C.POINTER(_vp),
+                                            _vp, C.POINTER(_vp), _vp], C.c_int),
         "pcgb_poly_mul_device": ([_vp, _vp, _vp, C.c_int, C.c_int, _vp], C.c_int),
         "pcgb_poly_mul_device_multi": ([C.c_int, _vp, _vp, _vp, _vp, _vp], C.c_int),
         "pcgb_expander_create": ([C.POINTER(_vp), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp,
@@ -598,6 +601,18 @@ def dpf_keyed_full_eval_device(K, n, w, prg, d_roots, d_cws, d_leaves, round_key
                                stream=None):
     rk = None if round_keys is None else _u8(round_keys)
     _check(lib.pcgb_dpf_keyed_full_eval(K, n, w, prg, d_roots, d_cws, _p(rk), d_leaves, stream))
+
+
+def dpf_keyed_full_eval_multi_device(groups, w, prg, round_keys=None, stream=None):
+    """groups: [(K, n, d_roots, d_cws, d_leaves), ...] with device pointers;
+    all groups share w and the PRG.  One launch per top-walk stage."""
+    G = len(groups)
+    Ks = (C.c_int * G)(*[int(g[0]) for g in groups])
+    ns = (C.c_int * G)(*[int(g[1]) for g in groups])
+    ptrs = [(C.c_void_p * G)(*[g[i] for g in groups]) for i in (2, 3, 4)]
+    rk = None if round_keys is None else _u8(round_keys)
+    _check(lib.pcgb_dpf_keyed_full_eval_multi(G, Ks, ns, w, prg, ptrs[0], ptrs[1], _p(rk),
+                                              ptrs[2], stream))
 
 
 def noise(N, c, t, seed, party):

@@ -170,3 +170,55 @@ def test_interactive_fused_convert_device_exchange(pcg, prg):
         outs.append((conv.download(np.uint64, B * D), sums.download(np.uint64, 2 * B)))
     assert calls == [B * nk] * L
     assert (outs[0][0] == outs[1][0]).all() and (outs[0][1] == outs[1][1]).all()
+
+
+MULTI_CASES = [
+    (O.PRG_CHACHA8, 1, [(64, 10), (7, 12), (300, 8), (1, 16), (0, 9), (2048, 12)]),
+    (O.PRG_CHACHA8, 2, [(100, 10), (16, 12), (1, 4)]),
+    (O.PRG_AES, 1, [(64, 10), (9, 12), (0, 6), (33, 7)]),
+]
+
+
+@pytest.mark.parametrize("prg,w,groups", MULTI_CASES)
+def test_keyed_multi_domain_batch(pcg, prg, w, groups):
+    """pcgb_dpf_keyed_full_eval_multi: key groups of different domains in one
+    batch give each group's single-call leaves (and the oracle's for the
+    smallest group), in as many launches as the deepest group's stage plan."""
+    nk = (1 << w) - 1
+    rks = O.aes_tree_round_keys(np.arange(16, dtype=np.uint8), nk) if prg == O.PRG_AES else None
+    rng = np.random.default_rng(len(groups) * 10 + w)
+    bufs, want, stages = [], [], []
+    for K, n in groups:
+        roots = rng.integers(0, 2**64 - 1, (max(K, 1), 2), dtype=np.uint64, endpoint=True)
+        cws = rng.integers(0, 2**64 - 1, (max(K, 1) * (n // w) * nk, 2), dtype=np.uint64,
+                           endpoint=True)
+        d_r, d_c = pcg.to_device(roots), pcg.to_device(cws)
+        d_one = pcg.DeviceBuffer(16 * max(K, 1) << n)
+        before = pcg.launch_count()
+        pcg.dpf_keyed_full_eval_device(K, n, w, prg, d_r.ptr, d_c.ptr, d_one.ptr, round_keys=rks)
+        pcg.synchronize()
+        stages.append(pcg.launch_count() - before)
+        want.append(d_one.download(np.uint64, 2 * (K << n)))
+        if 0 < K <= 9 and n <= 12:   # pinned to the oracle too
+            o = O.dpf_keyed_full_eval(K, n, w, roots[:K], cws[:K * (n // w) * nk], prg, rks)
+            assert (want[-1] == o.reshape(-1)).all()
+        d_out = pcg.DeviceBuffer(16 * max(K, 1) << n)
+        pcg.lib.pcgb_memset(d_out.ptr, 0x5A, d_out.nbytes, None)
+        bufs.append((K, n, d_r, d_c, d_out))
+    before = pcg.launch_count()
+    pcg.dpf_keyed_full_eval_multi_device([(K, n, r.ptr, c.ptr, o.ptr) for K, n, r, c, o in bufs],
+                                         w, prg, round_keys=rks)
+    pcg.synchronize()
+    assert pcg.launch_count() - before == max(stages)
+    for (K, n, _, _, d_out), wv in zip(bufs, want):
+        assert (d_out.download(np.uint64, 2 * (K << n)) == wv).all(), (K, n)
+
+
+def test_keyed_multi_rejects_bad_groups(pcg):
+    d = pcg.DeviceBuffer(16 * 64)
+    with pytest.raises(pcg.PcgError, match="bad"):
+        pcg.dpf_keyed_full_eval_multi_device([(4, 7, d.ptr, d.ptr, d.ptr)], 2, pcg.PRG_CHACHA8)
+    with pytest.raises(pcg.PcgError, match="negative"):
+        pcg.dpf_keyed_full_eval_multi_device([(-1, 6, d.ptr, d.ptr, d.ptr)], 1, pcg.PRG_CHACHA8)
+    with pytest.raises(pcg.PcgError, match="round keys"):
+        pcg.dpf_keyed_full_eval_multi_device([(4, 6, d.ptr, d.ptr, d.ptr)], 1, pcg.PRG_AES)
