@@ -26,6 +26,10 @@ Times are wall-clock per call with the device synchronised (the interactive
 paths include their per-level host round trips, as the reference's do).
 
 Usage: python oracle/dpf_convert_bench.py [--B 4096] [--n 16] [--w 1] [--iters 3]
+
+--mixed instead times a batch of key groups with different domains (ChaCha8,
+w = 1): one pcgb_dpf_keyed_full_eval_multi call against one
+pcgb_dpf_keyed_full_eval call per group, device time by CUDA events.
 """
 import argparse
 import ctypes as C
@@ -43,6 +47,54 @@ sys.path.insert(0, os.path.join(os.path.dirname(HERE), "pcg-square_b200"))
 import oracle_lib as O  # noqa: E402
 
 
+MIXED_GROUPS = [(256, 17), (512, 16), (1024, 14), (2048, 12), (4096, 10), (64, 8), (8, 6)]
+
+
+def mixed_main(args):
+    import pcg_b200 as L
+    rng = np.random.default_rng(args.seed)
+    groups = []
+    for K, n in MIXED_GROUPS:
+        roots = rng.integers(0, 2**64 - 1, (K, 2), dtype=np.uint64)
+        cws = rng.integers(0, 2**64 - 1, (K * n, 2), dtype=np.uint64)
+        groups.append((K, n, L.to_device(roots), L.to_device(cws), L.DeviceBuffer(16 * K << n)))
+    spec = [(K, n, r.ptr, c.ptr, o.ptr) for K, n, r, c, o in groups]
+
+    def timed(fn):
+        fn()                                     # warm
+        best = None
+        for _ in range(args.iters):
+            a, b = L.Event(), L.Event()
+            a.record()
+            fn()
+            b.record()
+            ms = a.elapsed_ms(b)
+            best = ms if best is None else min(best, ms)
+        return best
+
+    def each():
+        for K, n, r, c, o in spec:
+            L.dpf_keyed_full_eval_device(K, n, 1, L.PRG_CHACHA8, r, c, o)
+
+    def batch():
+        L.dpf_keyed_full_eval_multi_device(spec, 1, L.PRG_CHACHA8)
+
+    c0 = L.launch_count()
+    each()
+    per_group_launches = L.launch_count() - c0
+    c0 = L.launch_count()
+    batch()
+    batch_launches = L.launch_count() - c0
+    t_each, t_batch = timed(each), timed(batch)
+    leaves = sum(K << n for K, n in MIXED_GROUPS)
+    print(json.dumps({
+        "workload": "keyed DPF full-domain eval, ChaCha8 w=1, groups (K, n) = "
+                    + str(MIXED_GROUPS), "leaves": leaves,
+        "per_group_calls": {"ms": t_each, "launches": per_group_launches},
+        "one_batch": {"ms": t_batch, "launches": batch_launches},
+        "speedup": t_each / t_batch, "device": L.device_name()}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--B", type=int, default=4096)
@@ -50,7 +102,11 @@ def main():
     ap.add_argument("--w", type=int, default=1)
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--seed", type=int, default=33)
+    ap.add_argument("--mixed", action="store_true",
+                    help="time a batch of key groups of different domains")
     args = ap.parse_args()
+    if args.mixed:
+        return mixed_main(args)
     import pcg_b200 as L
 
     R = O.ref_gpu()
