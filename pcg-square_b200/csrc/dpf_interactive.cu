@@ -38,6 +38,14 @@ struct AesSm {
     uint32_t te[1024];
     uint32_t rk[15 * 44];
 };
+// The per-lane replicated Te0 (bank-conflict-free, aes128.cuh) for the deep
+// levels, where a CTA walks enough parents to pay for its 32 KB fill.
+struct AesRepSm {
+    uint32_t te_rep[kAesRepWords];
+    uint32_t rk[15 * 44];
+};
+constexpr size_t kRepMinParents = 4096;   // per instance, to use AesRepSm
+constexpr int kRepParentsPerThread = 8;
 
 // H_0..H_{nk-1} of one node.
 template <int W, int PRG>
@@ -125,8 +133,10 @@ __global__ void __launch_bounds__(kTPB) hash_roots_kernel(const Blk* __restrict_
 
 // Expand level i (frontier size sz, hashes H) with CW = my ^ peer; write the
 // children to nxt; when hash_next, hash the children into Hn and reduce
-// their columns into my_next.  grid = (ceil(sz / kTPB), B).
-template <int W, int PRG>
+// their columns into my_next.  grid = (x, B); the CTAs of an instance
+// stride over its sz parents (one each, or several with REP).  REP (AES
+// only): hash with the replicated table staged once per CTA.
+template <int W, int PRG, bool REP>
 __global__ void __launch_bounds__(kTPB) expand_level_kernel(
     const Blk* __restrict__ cur, const Blk* __restrict__ H, const Blk* __restrict__ my,
     const Blk* __restrict__ peer, Blk* __restrict__ nxt, Blk* __restrict__ Hn,
@@ -135,10 +145,19 @@ __global__ void __launch_bounds__(kTPB) expand_level_kernel(
     constexpr int M = 1 << W, NK = M - 1;
     extern __shared__ __align__(16) unsigned char smraw[];
     Blk* red = reinterpret_cast<Blk*>(smraw);
-    AesSm& aes = *reinterpret_cast<AesSm*>(smraw + 32 * NK * sizeof(Blk));
-    const AesSm* a = stage_aes<PRG>(aes, te, rk, NK);
+    const AesSm* a = nullptr;
+    const AesRepSm* arep = nullptr;
+    if constexpr (REP) {
+        AesRepSm& rs = *reinterpret_cast<AesRepSm*>(smraw + 32 * NK * sizeof(Blk));
+        aes_fill_rep(rs.te_rep, te);
+        for (int i = threadIdx.x; i < NK * 44; i += blockDim.x) rs.rk[i] = rk[i];
+        __syncthreads();
+        arep = &rs;
+    } else {
+        AesSm& aes = *reinterpret_cast<AesSm*>(smraw + 32 * NK * sizeof(Blk));
+        a = stage_aes<PRG>(aes, te, rk, NK);
+    }
     const int b = blockIdx.y;
-    const size_t j = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     Blk cw[NK];
     Blk cwf{0, 0};
 #pragma unroll
@@ -151,7 +170,7 @@ __global__ void __launch_bounds__(kTPB) expand_level_kernel(
     Blk acc[NK];
 #pragma unroll
     for (int k = 0; k < NK; ++k) acc[k] = Blk{0, 0};
-    if (j < sz) {
+    auto parent = [&](const size_t j) {
         const Blk p = cur[static_cast<size_t>(b) * D + j];
         const bool t = (p.lo & 1) != 0;
         Blk kids[M];
@@ -170,7 +189,14 @@ __global__ void __launch_bounds__(kTPB) expand_level_kernel(
         if (hash_next) {
             auto hash_child = [&](int k) {
                 Blk h[NK];
-                hash_node<W, PRG>(kids[k], a, h);
+                if constexpr (REP) {
+#pragma unroll 1
+                    for (int q = 0; q < NK; ++q)
+                        aes_ccr_rep(arep->te_rep, arep->rk + 44 * q, kids[k].lo, kids[k].hi,
+                                    h[q].lo, h[q].hi);
+                } else {
+                    hash_node<W, PRG>(kids[k], a, h);
+                }
                 Blk* hd = Hn + static_cast<size_t>(b) * HS + (j * M + k) * NK;
 #pragma unroll
                 for (int kk = 0; kk < NK; ++kk) {
@@ -190,6 +216,12 @@ __global__ void __launch_bounds__(kTPB) expand_level_kernel(
                 for (int k = 0; k < M; ++k) hash_child(k);
             }
         }
+    };
+    const size_t j0 = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if constexpr (REP) {
+        for (size_t j = j0; j < sz; j += static_cast<size_t>(gridDim.x) * blockDim.x) parent(j);
+    } else if (j0 < sz) {
+        parent(j0);
     }
     if (hash_next) cta_xor_reduce<NK>(acc, my_next + static_cast<size_t>(b) * NK, red);
 }
@@ -368,15 +400,28 @@ Blk* run_levels(Pool& pl, int B, int n, const Blk* roots, const Blk* dltsft,
             PCGB_POST_LAUNCH();
         }
         const size_t sz = static_cast<size_t>(1) << (W * i);
-        const dim3 grid(static_cast<unsigned>((sz + kTPB - 1) / kTPB), static_cast<unsigned>(B));
+        const bool rep = PRG == PCGB_PRG_AES && sz >= kRepMinParents;
+        const size_t per_cta = static_cast<size_t>(kTPB) * (rep ? kRepParentsPerThread : 1);
+        const dim3 grid(static_cast<unsigned>((sz + per_cta - 1) / per_cta), static_cast<unsigned>(B));
         if (!hash_next && conv) {
             last_level_convert_kernel<W><<<grid, kTPB, 0, st>>>(cur, H, my, pl.peer, sz, D, HS,
                                                                 conv->conv, conv->partials);
             PCGB_POST_LAUNCH();
             return nullptr;
         }
-        expand_level_kernel<W, PRG><<<grid, kTPB, smem, st>>>(cur, H, my, pl.peer, nxt, Hn, myn, sz,
-                                                              D, HS, hash_next, te, pl.rk);
+        if constexpr (PRG == PCGB_PRG_AES) {
+            if (rep) {
+                const size_t smem_rep = 32 * NK * sizeof(Blk) + sizeof(AesRepSm);
+                expand_level_kernel<W, PRG, true><<<grid, kTPB, smem_rep, st>>>(
+                    cur, H, my, pl.peer, nxt, Hn, myn, sz, D, HS, hash_next, te, pl.rk);
+            } else {
+                expand_level_kernel<W, PRG, false><<<grid, kTPB, smem, st>>>(
+                    cur, H, my, pl.peer, nxt, Hn, myn, sz, D, HS, hash_next, te, pl.rk);
+            }
+        } else {
+            expand_level_kernel<W, PRG, false><<<grid, kTPB, smem, st>>>(
+                cur, H, my, pl.peer, nxt, Hn, myn, sz, D, HS, hash_next, te, pl.rk);
+        }
         PCGB_POST_LAUNCH();
         std::swap(cur, nxt);
         std::swap(H, Hn);

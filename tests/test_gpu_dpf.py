@@ -40,10 +40,12 @@ def test_interactive_stub_exchange_matches_oracle(pcg, prg, n, w):
 
 
 @pytest.mark.parametrize("prg", [O.PRG_CHACHA8, O.PRG_AES])
-@pytest.mark.parametrize("n,w", [(10, 1), (10, 2), (8, 4)])
+@pytest.mark.parametrize("n,w", [(10, 1), (10, 2), (8, 4), (14, 1), (14, 2)])
 def test_interactive_two_party_matches_keyed(pcg, prg, n, w):
     """Real DltSft shares; the peer's share is my ^ CW (what the other party
-    sends), so the drop-in must reproduce the dealer's keyed leaves."""
+    sends), so the drop-in must reproduce the dealer's keyed leaves.  n = 14
+    reaches levels of 4096+ parents, where the AES levels hash with the
+    replicated table and several parents per thread."""
     nk, L = (1 << w) - 1, n // w
     rks = O.aes_tree_round_keys(np.arange(16, dtype=np.uint8), nk) if prg == O.PRG_AES else None
     B = 5
