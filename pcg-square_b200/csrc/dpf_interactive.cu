@@ -205,10 +205,11 @@ __global__ void __launch_bounds__(kTPB) expand_level_kernel(
                     acc[kk].hi ^= h[kk].hi;
                 }
             };
-            if constexpr (PRG == PCGB_PRG_CHACHA8 && W == 1) {
-                // Both children's blocks in flight: independent ARX chains
-                // keep the integer pipe busy while the level's loads and
-                // stores are outstanding.
+            if constexpr (PRG == PCGB_PRG_CHACHA8 && W <= 2) {
+                // All children's blocks in flight (one block each for
+                // w <= 2): independent ARX chains keep the integer pipe busy
+                // while the level's loads and stores are outstanding, and
+                // the children stay in registers.
 #pragma unroll
                 for (int k = 0; k < M; ++k) hash_child(k);
             } else {
