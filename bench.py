@@ -114,6 +114,8 @@ def chacha8_live_ops(ctr, nonce, words):
 OPS_OUT_HASH = chacha8_live_ops(0, (0x68617368, 0x6F75745F), [0, 1])
 # Binary tree node (w = 1): H_0 = words 0-3 of block 0, nonce 0.
 OPS_TREE_W1 = chacha8_live_ops(0, (0, 0), [0, 1, 2, 3])
+# An unpruned block: 8 rounds x 4 quarter rounds x 12 ops + 4 feed-forward adds.
+OPS_FULL_BLOCK = 388
 
 
 def parse():
@@ -235,56 +237,90 @@ class Clocks:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-# ---- CPU baseline (oracle port, bounded sample) ------------------------------
-def cpu_sample(threads, n_blocks=None, keys=None, polymuls=None, shape=None):
-    """Times a bounded sample of the oracle's expansion and extrapolates to one
-    full expansion: returns (corr/s, seconds of CPU work, description).
-    shape = (N, c, t), default the headline shape."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle_lib as O
-    n_, c_, t_ = shape or (N, C_, T_)
-    key = (n_, c_, t_)
-    cache = cpu_sample.__dict__.setdefault("material", {})
-    s = O.shape(n_, c_, t_)
-    if key not in cache:
-        r0, _, cws, cwo = O.deal_keys(s, 1000)
-        cache[key] = (r0, cws, cwo, O.public_a(s, A_SEED))
-    r0, cws, cwo, a = cache[key]
-    B = t_ * t_
-    n_blocks = n_blocks or 1
-    keys = min(B, keys or max(threads, 32))
-    n_products = c_ + 2 * c_ * c_   # step 4 of pcg_ole_impl.h:460-483
-    polymuls = min(n_products, polymuls or threads)
-    t_dpf, t_ntt = O.bench_sample(s, 0, r0, cws, cwo, a, n_blocks, keys, polymuls, threads)
-    total_keys = c_ * c_ * B
-    t_full = t_dpf * total_keys / (n_blocks * keys) + t_ntt * n_products / polymuls
-    desc = (f"{n_blocks * keys} of {total_keys} keys (DPF+convert+scatter) and {polymuls} of "
-            f"{n_products} length-2^{n_.bit_length() - 1} products, {threads} threads, "
-            "extrapolated to one expansion")
-    return n_ / t_full, t_dpf + t_ntt, desc
+# ---- CPU baseline (oracle port, whole units of work) -------------------------
+def host_info():
+    """Core count and model of this host (for the CPU figures)."""
+    model = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count()
+    return {"nproc": usable, "cpu_count": os.cpu_count(), "model": model}
+
+
+class CpuExpansion:
+    """One party's expansion on the host (the oracle's CPU restatement of the
+    reference algorithm), cut into c^2 steps of equal work: step k runs every
+    key of block k mod c^2 (keyed DPF, output hash, convert, scatter into the
+    block's g) and its share of the c + 2c^2 step-4 products (2 or 3 of 36
+    at c = 4, so that any c^2 consecutive steps run all of them), from one
+    task queue on `threads` threads.  c^2 consecutive steps are exactly one
+    expansion; nothing is extrapolated."""
+
+    def __init__(self, shape=None):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle_lib as O
+        self.O = O
+        self.N, self.c, self.t = shape or (N, C_, T_)
+        self.s = O.shape(self.N, self.c, self.t)
+        r0, _, cws, cwo = O.deal_keys(self.s, 1000)
+        self.material = (r0, cws, cwo, O.public_a(self.s, A_SEED))
+        self.blocks = self.c * self.c
+        self.products = self.c + 2 * self.c * self.c   # pcg_ole_impl.h:460-483
+
+    def products_of_step(self, k):
+        return (self.products * (k + 1)) // self.blocks - (self.products * k) // self.blocks
+
+    def step(self, k, threads):
+        r0, cws, cwo, a = self.material
+        return self.O.bench_block(self.s, 0, r0, cws, cwo, a, k % self.blocks,
+                                  self.products_of_step(k), threads)
+
+    def corr_per_step(self):
+        return self.N / self.blocks
+
+
+def cpu_sample(threads, shape=None):
+    """One whole expansion on `threads` host threads (c^2 block steps):
+    returns (corr/s, seconds, description)."""
+    cpu = CpuExpansion(shape)
+    sec = [cpu.step(k, threads) for k in range(cpu.blocks)]
+    desc = (f"one whole expansion: {cpu.blocks} blocks x {cpu.t * cpu.t} keys "
+            f"(DPF+convert+scatter) and {cpu.products} length-2^{cpu.N.bit_length() - 1} "
+            f"products on {threads} threads")
+    return cpu.N / sum(sec), sum(sec), desc
 
 
 def run_reference(args, d):
     if d.rank != 0:
         return
-    threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        cpu_sample(threads, keys=threads)
-    vals, spent = [], 0.0
-    for _ in range(args.steps):
-        v, sec, desc = cpu_sample(threads, keys=threads)
-        vals.append(v)
-        spent += sec
-    value = float(np.mean(vals))
+    threads = host_info()["nproc"] or 1
+    cpu = CpuExpansion()
+    for k in range(args.warmup):
+        cpu.step(k, threads)
+    sec = [cpu.step(k, threads) for k in range(args.steps)]
+    value = cpu.corr_per_step() * args.steps / sum(sec)
+    desc = (f"each step one of the {cpu.blocks} blocks of one party's expansion: "
+            f"{cpu.t * cpu.t} keys (DPF+convert+scatter) and 2-3 of the {cpu.products} "
+            f"products, cycling; {cpu.blocks} steps = one expansion; {threads} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "corr/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * N / value, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1e3 * float(np.mean(sec)), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": value / PUBLISHED, "dtype": "u64", "data": "synthetic",
         "config": {"workload": "pcg-ole expansion N=2^20 c=4 t=16 w=1 chacha8 (one party)",
-                   "N": N, "c": C_, "t": T_, "host_threads": threads},
+                   "N": N, "c": C_, "t": T_, "host_threads": threads,
+                   "step": f"1/{cpu.blocks} of one expansion (one whole block)"},
         "cpu_baseline": {"value": value, "unit": "corr/s", "cores": threads, "kind": "port",
-                         "sample": desc},
+                         "sample": desc, "host": host_info(),
+                         "step_ms": [round(1e3 * x, 2) for x in sec]},
         "e2e": {"value": value, "unit": "corr/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -321,7 +357,13 @@ def run_ours(args, d):
     for _ in range(args.warmup):
         e.expand_device(0, *args_dev)
     L.synchronize()
-    gops_peak, _ = L.arx_peak()
+    # The ALU peak: 15 launches of the ARX probe (about 36 ms each), with
+    # the SM clock sampled while they run; the roofline divides by the median.
+    probe_clk = Clocks(d.local)
+    probe_clk.start()
+    probe = sorted(L.arx_peak_samples(15, 16384))
+    probe_clocks = probe_clk.stop()
+    gops_peak = float(np.median(probe))
 
     # Per-stage device times: a profiled pass of the same steps (direct
     # launches, events between the stages), not part of the timed region.
@@ -444,18 +486,29 @@ def run_ours(args, d):
     # Per leaf: one output hash; per internal node below the frontier (S - 1
     # of them per S leaves): one tree block.
     ops = K * D * (OPS_OUT_HASH + OPS_TREE_W1 * (S - 1) / S)
+    ops_full = K * D * (2 - 1 / S) * OPS_FULL_BLOCK
     achieved = ops / (leaf_ms * 1e-3) / 1e12 if leaf_ms else None
     peak = gops_peak / 1e3
+    # DRAM traffic of one launch: frontier nodes read (one per S leaves) and
+    # g' words written, at the per-node and per-word rates of the ncu capture.
+    traffic = (LEAF_READ_BYTES_PER_NODE * K * D / S + LEAF_WRITE_BYTES_PER_WORD * e.Q * N)
     roofline = {"bound": "int_alu",
                 "kernel": f"leaf_gather_kernel<1,{S.bit_length() - 1},chacha8>",
                 "achieved": achieved, "peak": peak, "unit": "Tops/s",
                 "frac": achieved / peak if achieved else None,
-                "traffic": LEAF_DRAM_BYTES_PER_LEAF * K * D,
-                "traffic_unit": "bytes per launch (ncu dram read+write, scaled by leaves)",
-                "peak_source": "ARX probe (pcgb_arx_peak) in this run; MEASURED_PEAKS.json has "
-                               "no integer-ALU figure",
+                "traffic": traffic,
+                "traffic_unit": "bytes per launch: frontier reads + g' writes at the rates "
+                                "of the ncu capture (profiles/leaf_gather_chacha8_*.txt)",
+                "algorithmic_bytes": 16 * K * D / S + 8 * e.Q * N,
+                "peak_source": "median of 15 launches of the ARX probe (pcgb_arx_peak_samples) "
+                               "in this run; MEASURED_PEAKS.json has no integer-ALU figure",
+                "peak_spread": {"min": probe[0] / 1e3, "median": peak, "max": probe[-1] / 1e3,
+                                "launches": len(probe), "clocks": probe_clocks},
                 "ops_per_launch": ops, "ops_per_block": {"out_hash": OPS_OUT_HASH,
                                                          "tree": OPS_TREE_W1},
+                "frac_at_full_blocks": (ops_full / (leaf_ms * 1e-3) / 1e12 / peak
+                                        if leaf_ms else None),
+                "full_block_ops": OPS_FULL_BLOCK,
                 "launch_ms": leaf_ms}
     ntt_ms = float(np.mean([s[3] for s in stages])) if stages else None
     Q = e.Q
@@ -468,14 +521,20 @@ def run_ours(args, d):
 
     cpu = None
     if d.world == 1 and d.rank == 0 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
+        host = host_info()
+        threads = host["nproc"] or 1
         v, sec, desc = cpu_sample(threads, shape=(N, C_, T_))
         cpu = {"value": v, "unit": "corr/s", "cores": threads, "kind": "port",
-               "sample": desc, "sample_seconds": sec}
+               "sample": desc, "sample_seconds": sec, "host": host}
         # The reference's CPU bench runs one thread per party (its OpenMP
-        # pragma is not compiled in): the same sample on one thread.
-        v1, sec1, desc1 = cpu_sample(1, keys=8, polymuls=2, shape=(N, C_, T_))
-        cpu["one_thread"] = {"value": v1, "cores": 1, "sample": desc1, "sample_seconds": sec1}
+        # pragma is not compiled in): one whole block step on one thread
+        # (its 256 keys and 2 of the 36 products).
+        one = CpuExpansion((N, C_, T_))
+        sec1 = one.step(0, 1)
+        cpu["one_thread"] = {"value": one.corr_per_step() / sec1, "cores": 1,
+                             "sample": "one whole block (1/16 of the expansion's keys) and 2 "
+                                       "of its 36 products on 1 thread",
+                             "sample_seconds": sec1}
 
     serve = None
     if d.world == 1 and args.serve_requests > 0:
@@ -631,12 +690,12 @@ def run_serving(L, n_req, seed=2025, util=0.85):
     return out
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per leaf of one
-# leaf-gather launch, from an ncu capture of the N=2^18, c=4, t=16 case
-# (135.06 MB read + 8.75 MB written for 4096 keys x 2^15 leaves).  The reads
-# are the 16-byte frontier nodes (one per 16 leaves); the traffic scales with
-# the leaf count.
-LEAF_DRAM_BYTES_PER_LEAF = (135.05792e6 + 8.749824e6) / (4096 * 2 ** 15)
+# DRAM bytes of one leaf-gather launch, from an ncu capture of the N=2^18,
+# c=4, t=16 case at 128 threads x 8 leaves per thread: 269.8 MB read for the
+# 4096 x 2^15 / 8 frontier nodes (16 B each), 14.8 MB written for the
+# 10 x 2^18 g' words (8 B each; part of them still in L2 at kernel end).
+LEAF_READ_BYTES_PER_NODE = 269.8e6 / (4096 * 2 ** 15 / 8)
+LEAF_WRITE_BYTES_PER_WORD = 14.8e6 / (10 * 2 ** 18)
 
 
 def hbm_peak():

@@ -90,6 +90,10 @@ unsigned long long pcgb_launch_count(void);
 /* Integer-ALU roofline probe: ChaCha8 quarter rounds on register-resident
  * states over every SM; *gops = G int-ops/s (12 ops per quarter round). */
 int pcgb_arx_peak(double* gops, float* ms);
+/* The same probe as `reps` launches of `iters` double-round iterations each
+ * (4096 iterations take about 9 ms on B200); gops[r] = G int-ops/s of launch
+ * r, so the caller can report the probe's spread. */
+int pcgb_arx_peak_samples(int reps, int iters, double* gops);
 /* CUDA events on the library's streams (device-side timing). */
 int pcgb_event_create(void** ev);
 int pcgb_event_destroy(void* ev);
@@ -222,7 +226,10 @@ int pcgb_add_mod_p_device(uint64_t* d, const uint64_t* u, const uint64_t* v, siz
  * only enqueues work on `stream`: synchronise before reading the outputs.
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  All calls on a device share the array, so
+ * before any stream capture.  The address is kept for the life of the
+ * process, like the library's other per-device state: after a
+ * cudaDeviceReset it is stale, so do not call the library again on that
+ * device in the same process.  All calls on a device share the array, so
  * calls that overlap on the GPU (unordered streams) race; each call
  * overwrites every partial it reads, so nothing needs clearing between
  * calls.  No cudaMalloc, cudaFree or allocating library routine is used. */

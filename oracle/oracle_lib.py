@@ -85,6 +85,8 @@ def lib():
         L.orc_bench_sample.argtypes = [C.POINTER(Shape), C.c_int, u64p, u64p, u64p, u64p,
                                        C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.orc_bench_block.argtypes = [C.POINTER(Shape), C.c_int, u64p, u64p, u64p, u64p,
+                                      C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -331,6 +333,20 @@ def ref_gpu():
         L.ref_free.argtypes = [C.c_void_p]
         _ref_gpu = L
     return _ref_gpu
+
+
+def bench_block(s, party, roots, cws, cw_out, a, blk, n_polymuls, threads):
+    """Wall seconds of one whole (i,j) block of one party's expansion (all its
+    keys through DPF + convert + scatter) plus n_polymuls step-4 products, on
+    `threads` host threads."""
+    sec = C.c_double()
+    rc = lib().orc_bench_block(C.byref(s), party, np.ascontiguousarray(roots, np.uint64),
+                               np.ascontiguousarray(cws, np.uint64),
+                               np.ascontiguousarray(cw_out, np.uint64),
+                               np.ascontiguousarray(a, np.uint64), blk, n_polymuls, threads,
+                               C.byref(sec))
+    assert rc == 0, rc
+    return sec.value
 
 
 def bench_sample(s, party, roots, cws, cw_out, a, n_blocks, keys_per_block, n_polymuls, threads):

@@ -4,6 +4,7 @@
 // See pcg_oracle.h for how parity is pinned.
 #include "pcg_oracle.h"
 
+#include <atomic>
 #include <chrono>
 #include <cstring>
 #include <mutex>
@@ -845,6 +846,61 @@ int orc_bench_sample(const orc_shape* s, int party, const orc_blk* roots, const 
     *t_dpf = std::chrono::duration<double>(t1 - t0).count();
     *t_ntt = std::chrono::duration<double>(t2 - t1).count();
     return 0;
+}
+
+// One whole unit of the expansion on the host: every key of block `blk`
+// (DPF, output hash, convert and the scatter into the block's g, the
+// per-thread partial g's summed at the end) and `n_polymuls` step-4 products
+// (pcg_ole_impl.h:460-483), all from one task queue on `threads` threads,
+// the products (the longest tasks) first.  Returns the wall seconds.
+int orc_bench_block(const orc_shape* s, int party, const orc_blk* roots, const orc_blk* cws,
+                    const uint64_t* cw_out, const uint64_t* a, int blk, int n_polymuls,
+                    int threads, double* seconds) {
+    const int N = s->N, t = s->t, B = t * t;
+    const size_t D = static_cast<size_t>(1) << s->n, bin = D / 2;
+    const size_t per = static_cast<size_t>(s->levels) * s->nk;
+    if (threads < 1) threads = 1;
+    if (blk < 0 || blk >= s->c * s->c || n_polymuls < 0) return -1;
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    std::vector<std::vector<uint64_t>> g2(threads);
+    std::atomic<int> next{0};
+    const int tasks = n_polymuls + B;
+    std::vector<std::thread> pool;
+    for (int w = 0; w < threads; ++w)
+        pool.emplace_back([&, w] {
+            std::vector<orc_blk> leaves;
+            std::vector<uint64_t> c;
+            for (int k = next++; k < tasks; k = next++) {
+                if (k < n_polymuls) {
+                    c.resize(N);
+                    const uint64_t* x = a + static_cast<size_t>(k % (s->c > 1 ? s->c - 1 : 1)) * N;
+                    poly_mul1(c.data(), x, x, N);
+                    continue;
+                }
+                const int b = k - n_polymuls;
+                const size_t id = static_cast<size_t>(blk) * B + b;
+                leaves.resize(D);
+                if (g2[w].empty()) g2[w].assign(2 * static_cast<size_t>(N), 0);
+                orc_dpf_keyed_full_eval(1, s->n, s->w, roots + id, cws + id * per, nullptr, s->prg,
+                                        leaves.data());
+                const size_t base = static_cast<size_t>(b / t + b % t) * bin;
+                for (size_t d = 0; d < D; ++d) {
+                    uint64_t y = orc_out_hash_lo64(leaves[d]) % P;
+                    if (leaves[d].lo & 1) y = addm(y, cw_out[id]);
+                    if (party == 1) y = subm(0, y);
+                    g2[w][base + d] = addm(g2[w][base + d], y);
+                }
+            }
+        });
+    for (auto& th : pool) th.join();
+    // The block's g: the threads' partial sums added word by word.
+    std::vector<uint64_t> g(2 * static_cast<size_t>(N), 0);
+    for (const auto& part : g2)
+        if (!part.empty())
+            for (size_t i = 0; i < g.size(); ++i) g[i] = addm(g[i], part[i]);
+    *seconds = std::chrono::duration<double>(clk::now() - t0).count();
+    return g[0] == P ? -2 : 0;   // keeps the sum live; g[0] < P always
 }
 
 // mt19937_64 (Matsumoto & Nishimura 2000; the parameters of C++

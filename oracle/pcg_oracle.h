@@ -158,6 +158,14 @@ int orc_bench_sample(const orc_shape* s, int party, const orc_blk* roots, const 
                      int keys_per_block, int n_polymuls, int threads, double* t_dpf,
                      double* t_ntt);
 
+/* One whole (i,j) block of one party's expansion on the host: all t^2 keys
+ * of block blk (keyed DPF + convert + scatter into the block's g) and
+ * n_polymuls length-N step-4 products, from one task queue on `threads`
+ * threads.  *seconds: wall time. */
+int orc_bench_block(const orc_shape* s, int party, const orc_blk* roots, const orc_blk* cws,
+                    const uint64_t* cw_out, const uint64_t* a, int blk, int n_polymuls,
+                    int threads, double* seconds);
+
 /* mt19937_64 (reference fixtures use std::mt19937_64). */
 void orc_mt64_fill(uint64_t seed, uint64_t* out, size_t n);
 

@@ -34,20 +34,13 @@ sys.path.insert(0, os.path.join(os.path.dirname(HERE), "pcg-square_b200"))
 import oracle_lib as O  # noqa: E402
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--N", type=int, default=1 << 20)
-    ap.add_argument("--c", type=int, default=4)
-    ap.add_argument("--t", type=int, default=16)
-    ap.add_argument("--iters", type=int, default=3)
-    ap.add_argument("--seed", type=int, default=1000)
-    args = ap.parse_args()
-    import pcg_b200 as L
-
+def run(L, N=1 << 20, c=4, t=16, iters=3, seed=1000):
+    """Times the plain path (one warm-up iteration, then `iters`) and checks
+    its g against the library's fused g'; returns the result dict, or None
+    when oracle/_ref/libref_gpu.so is not built."""
     R = O.ref_gpu()
     if R is None:
-        raise SystemExit("oracle/_ref/libref_gpu.so not built")
-    N, c, t = args.N, args.c, args.t
+        return None
     s = O.shape(N, c, t)
     B, n, levels = t * t, s.n, s.levels
     D = 1 << n
@@ -56,7 +49,7 @@ def main():
     K = e.K
     d_r0, d_r1 = L.DeviceBuffer(16 * K), L.DeviceBuffer(16 * K)
     d_cws, d_cwo = L.DeviceBuffer(16 * K * levels * e.nk), L.DeviceBuffer(8 * K)
-    e.deal_keys_device(args.seed, d_r0.ptr, d_r1.ptr, d_cws.ptr, d_cwo.ptr)
+    e.deal_keys_device(seed, d_r0.ptr, d_r1.ptr, d_cws.ptr, d_cwo.ptr)
     roots = d_r0.download(np.uint64, 2 * K).reshape(K, 2)
     cws = d_cws.download(np.uint64, 2 * K * levels).reshape(K, levels, 2)
     cwo = d_cwo.download(np.uint64, K)
@@ -72,7 +65,7 @@ def main():
     dz = np.zeros((B * levels, 2), np.uint64)
     timings = []
     g_blocks = {}
-    for it in range(args.iters + 1):
+    for it in range(iters + 1):
         st = {"dpf": 0.0, "sums": 0.0, "scatter": 0.0, "ntt": 0.0}
         w0 = time.perf_counter()
         for blk in range(c * c):
@@ -125,11 +118,26 @@ def main():
             ok &= bool((fused[q] == np.asarray(want, dtype=np.uint64)).all())
             q += 1
     mean = {k: float(np.mean([x[k] for x in timings])) for k in timings[0]}
-    out = {"path": "plain per-stage GPU (reference kernels, serial arm)", "N": N, "c": c, "t": t,
-           "B_per_block": B, "n": n, "iters": args.iters,
-           "ms": {k: 1e3 * v for k, v in mean.items()},
-           "corr_per_s": N / mean["wall"], "g_bit_exact_vs_fused": ok,
-           "device": L.device_name()}
+    e.close()
+    return {"path": "plain per-stage GPU (reference kernels, serial arm)", "N": N, "c": c, "t": t,
+            "B_per_block": B, "n": n, "iters": iters,
+            "ms": {k: 1e3 * v for k, v in mean.items()},
+            "corr_per_s": N / mean["wall"], "g_bit_exact_vs_fused": ok,
+            "device": L.device_name()}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--N", type=int, default=1 << 20)
+    ap.add_argument("--c", type=int, default=4)
+    ap.add_argument("--t", type=int, default=16)
+    ap.add_argument("--iters", type=int, default=3)
+    ap.add_argument("--seed", type=int, default=1000)
+    args = ap.parse_args()
+    import pcg_b200 as L
+    out = run(L, args.N, args.c, args.t, args.iters, args.seed)
+    if out is None:
+        raise SystemExit("oracle/_ref/libref_gpu.so not built")
     print(json.dumps(out), flush=True)
 
 

@@ -53,11 +53,12 @@ void note_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_o
 
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
-// Returns G int-ops/s; *ms = probe duration.
-double arx_probe(float* ms_out) {
+// G int-ops/s of each of `reps` launches of `iters` double-round iterations
+// (after one short warm-up launch), in launch order.
+void arx_probe_samples(int reps, int iters, double* gops) {
     cudaStream_t st = default_stream();
     const int sms = sm_count();
-    const int blocks = sms * 8, threads = 256, iters = 4096;
+    const int blocks = sms * 8, threads = 256;
     uint32_t* sink =
         static_cast<uint32_t*>(pool_alloc(sizeof(uint32_t) * static_cast<size_t>(blocks) * threads, st));
     arx_probe_kernel<<<blocks, threads, 0, st>>>(1, 64, sink);  // warm-up
@@ -65,8 +66,8 @@ double arx_probe(float* ms_out) {
     cudaEvent_t e0, e1;
     PCGB_CK(cudaEventCreate(&e0));
     PCGB_CK(cudaEventCreate(&e1));
-    float ms = 0;
-    for (int rep = 0; rep < 3; ++rep) {   // the fastest of three launches
+    const double ops = static_cast<double>(blocks) * threads * iters * 2 /*states*/ * 8 * 12;
+    for (int rep = 0; rep < reps; ++rep) {
         PCGB_CK(cudaEventRecord(e0, st));
         arx_probe_kernel<<<blocks, threads, 0, st>>>(2 + rep, iters, sink);
         PCGB_POST_LAUNCH();
@@ -74,14 +75,24 @@ double arx_probe(float* ms_out) {
         PCGB_CK(cudaEventSynchronize(e1));
         float t = 0;
         PCGB_CK(cudaEventElapsedTime(&t, e0, e1));
-        ms = rep == 0 ? t : std::min(ms, t);
+        gops[rep] = ops / (t * 1e-3) / 1e9;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     PCGB_CK(cudaFreeAsync(sink, st));
-    if (ms_out) *ms_out = ms;
-    const double ops = static_cast<double>(blocks) * threads * iters * 2 /*states*/ * 8 * 12;
-    return ops / (ms * 1e-3) / 1e9;
+}
+
+// Returns G int-ops/s of the fastest of three launches; *ms = its duration.
+double arx_probe(float* ms_out) {
+    constexpr int iters = 4096;
+    double g[3];
+    arx_probe_samples(3, iters, g);
+    const double best = std::max(g[0], std::max(g[1], g[2]));
+    if (ms_out) {
+        const double ops = static_cast<double>(sm_count()) * 8 * 256 * iters * 2 * 8 * 12;
+        *ms_out = static_cast<float>(ops / (best * 1e9) * 1e3);
+    }
+    return best;
 }
 
 }  // namespace pcgb

@@ -69,6 +69,7 @@ void server_run_trace(pcgb_server* s, const pcgb_request* reqs, int n, pcgb_resu
 void server_destroy(pcgb_server* s, int timeout_ms);
 void server_stats(pcgb_server* s, int* pending, int* in_flight, size_t* bytes, int* plans);
 double arx_probe(float* ms_out);
+void arx_probe_samples(int reps, int iters, double* gops);
 
 namespace {
 thread_local std::string g_last_error;
@@ -287,6 +288,14 @@ int pcgb_arx_peak(double* gops, float* ms) {
     return guarded([&] {
         const double g = pcgb::arx_probe(ms);
         if (gops) *gops = g;
+    });
+}
+
+int pcgb_arx_peak_samples(int reps, int iters, double* gops) {
+    return guarded([&] {
+        if (reps < 1 || iters < 1 || !gops)
+            pcgb::fail(PCGB_EINVAL, "arx_peak_samples: reps and iters must be positive");
+        pcgb::arx_probe_samples(reps, iters, gops);
     });
 }
 

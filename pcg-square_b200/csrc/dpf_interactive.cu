@@ -401,15 +401,17 @@ Blk* run_levels(Pool& pl, int B, int n, const Blk* roots, const Blk* dltsft,
             PCGB_POST_LAUNCH();
         }
         const size_t sz = static_cast<size_t>(1) << (W * i);
-        const bool rep = PRG == PCGB_PRG_AES && sz >= kRepMinParents;
-        const size_t per_cta = static_cast<size_t>(kTPB) * (rep ? kRepParentsPerThread : 1);
-        const dim3 grid(static_cast<unsigned>((sz + per_cta - 1) / per_cta), static_cast<unsigned>(B));
         if (!hash_next && conv) {
-            last_level_convert_kernel<W><<<grid, kTPB, 0, st>>>(cur, H, my, pl.peer, sz, D, HS,
-                                                                conv->conv, conv->partials);
+            // One parent per thread: the grid the fold's `parts` assumes.
+            const dim3 cgrid(static_cast<unsigned>((sz + kTPB - 1) / kTPB), static_cast<unsigned>(B));
+            last_level_convert_kernel<W><<<cgrid, kTPB, 0, st>>>(cur, H, my, pl.peer, sz, D, HS,
+                                                                 conv->conv, conv->partials);
             PCGB_POST_LAUNCH();
             return nullptr;
         }
+        const bool rep = PRG == PCGB_PRG_AES && sz >= kRepMinParents;
+        const size_t per_cta = static_cast<size_t>(kTPB) * (rep ? kRepParentsPerThread : 1);
+        const dim3 grid(static_cast<unsigned>((sz + per_cta - 1) / per_cta), static_cast<unsigned>(B));
         if constexpr (PRG == PCGB_PRG_AES) {
             if (rep) {
                 const size_t smem_rep = 32 * NK * sizeof(Blk) + sizeof(AesRepSm);

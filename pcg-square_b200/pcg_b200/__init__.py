@@ -143,6 +143,7 @@ def _load():
         "pcgb_expander_stage_times": ([_vp, C.POINTER(C.c_float), C.c_int], C.c_int),
         "pcgb_launch_count": ([], C.c_ulonglong),
         "pcgb_arx_peak": ([C.POINTER(C.c_double), C.POINTER(C.c_float)], C.c_int),
+        "pcgb_arx_peak_samples": ([C.c_int, C.c_int, C.POINTER(C.c_double)], C.c_int),
         "pcgb_event_create": ([C.POINTER(_vp)], C.c_int),
         "pcgb_event_destroy": ([_vp], C.c_int),
         "pcgb_event_record": ([_vp, _vp], C.c_int),
@@ -301,6 +302,13 @@ def arx_peak():
     g, ms = C.c_double(), C.c_float()
     _check(lib.pcgb_arx_peak(C.byref(g), C.byref(ms)))
     return g.value, ms.value
+
+
+def arx_peak_samples(reps=15, iters=16384):
+    """G int-ops/s of each of `reps` launches of the ARX probe."""
+    out = (C.c_double * reps)()
+    _check(lib.pcgb_arx_peak_samples(reps, iters, out))
+    return list(out)
 
 
 def default_stream():

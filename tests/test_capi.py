@@ -40,6 +40,26 @@ def test_exports_pcg_cuda_compat_symbols():
         assert name in out, name
 
 
+@pytest.mark.parametrize("driver", ["test_poly_mul_cuda", "dpf_real_bench", "e2e_full_bench"])
+def test_reference_drivers_resolve_every_pcg_cuda_symbol(driver):
+    """The reference's own drivers, compiled unchanged (oracle/Makefile
+    `drivers`), import only pcg_cuda:: symbols the library defines, and load
+    the in-tree library."""
+    path = os.path.join(ROOT, "oracle", "_ref", "drivers", driver)
+    if not os.path.exists(path):
+        pytest.skip("reference drivers not built (needs the reference tree)")
+    nm = lambda *a: subprocess.run(["nm", "-D", *a], capture_output=True, text=True,
+                                   check=True).stdout
+    need = {l.split()[-1] for l in nm("--undefined-only", path).splitlines()
+            if "pcg_cuda" in l}
+    have = {l.split()[-1] for l in nm("--defined-only", LIB).splitlines()}
+    assert need, "driver imports no pcg_cuda symbol"
+    assert need <= have, sorted(need - have)
+    ldd = subprocess.run(["ldd", path], capture_output=True, text=True, check=True).stdout
+    line = next(l for l in ldd.splitlines() if "libpcg_b200.so" in l)
+    assert os.path.realpath(line.split("=>")[1].split("(")[0].strip()) == os.path.realpath(LIB)
+
+
 def test_host_side_calls_without_device():
     import pcg_b200 as L
     if L.is_cuda_available():

@@ -100,12 +100,14 @@ def test_dpf_real_bench_golden_checksums(pcg, n, B, t, want):
 
 @pytest.mark.parametrize("prg", [O.PRG_CHACHA8, O.PRG_AES])
 @pytest.mark.parametrize("n,w,B", [(1, 1, 3), (10, 1, 5), (10, 2, 5), (9, 3, 4), (8, 4, 6),
-                                   (12, 1, 300)])
+                                   (12, 1, 300), (13, 1, 4), (14, 2, 3), (16, 4, 2)])
 def test_interactive_fused_convert_matches_two_calls(pcg, prg, n, w, B):
     """pcgb_dpf_batch_full_eval_convert_device (last level fused with the
     sums pass, no leaves stored) gives the converted words and sums of
     dpf_gpu_batch_full_eval_device + pcgb_dpf_out_convert_device, and the
-    oracle's sums, with a real per-level exchange."""
+    oracle's sums, with a real per-level exchange.  (13,1), (14,2) and (16,4)
+    have 4096 last-level parents, where the AES expand levels walk 8 parents
+    per thread and the fused last level must still take one each."""
     nk, L = (1 << w) - 1, n // w
     rks = O.aes_tree_round_keys(np.arange(16, dtype=np.uint8), nk) if prg == O.PRG_AES else None
     rng = np.random.default_rng(31 * n + w + B)

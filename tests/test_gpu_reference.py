@@ -20,11 +20,18 @@ def ref():
     return R
 
 
-@pytest.mark.parametrize("prg", [O.PRG_CHACHA8, O.PRG_AES])
-@pytest.mark.parametrize("n,w", [(12, 1), (12, 2), (12, 4)])
-def test_interactive_leaves_match_reference_kernels(pcg, ref, prg, n, w):
+CASES = [(prg, n, w, 16) for prg in (O.PRG_CHACHA8, O.PRG_AES) for n, w in
+         ((12, 1), (12, 2), (12, 4))]
+# Levels of 4096+ parents: the AES level kernel stages the per-lane
+# replicated T-table and walks 8 parents per thread (grid-stride).
+CASES += [(O.PRG_AES, 14, 1, 5), (O.PRG_AES, 14, 2, 3), (O.PRG_AES, 16, 4, 2),
+          (O.PRG_AES, 16, 1, 3)]
+
+
+@pytest.mark.parametrize("prg,n,w,B", CASES)
+def test_interactive_leaves_match_reference_kernels(pcg, ref, prg, n, w, B):
     rng = np.random.default_rng(n + 10 * w + prg)
-    B, nk = 16, (1 << w) - 1
+    nk = (1 << w) - 1
     rks = O.aes_tree_round_keys(rng.integers(0, 256, 16, dtype=np.uint8), nk) \
         if prg == O.PRG_AES else None
     roots = rng.integers(0, 2**64 - 1, (B, 2), dtype=np.uint64)

@@ -46,6 +46,27 @@ def test_noalloc_sums_match_existing_entry_point(pcg):
         assert (got_c == want_c).all() and (got_t == want_t).all(), (B, n)
 
 
+def test_noalloc_sums_with_fewer_partials_than_the_allocating_path(pcg):
+    """B = 4096 instances of 2^16 leaves: the allocating path uses 32 partials
+    per instance, more than the static array holds for this B (16 each), so
+    the allocation-free call runs fewer CTAs with more leaves per thread.
+    The 4 GiB of leaves come from the keyed evaluator on the device.  Then a
+    small call again, which must not see the large call's partials."""
+    rng = np.random.default_rng(77)
+    for B, n in ((4096, 16), (5, 10)):
+        D = 1 << n
+        roots = rng.integers(0, 2**64 - 1, (B, 2), dtype=np.uint64, endpoint=True)
+        cws = rng.integers(0, 2**64 - 1, (B * n, 2), dtype=np.uint64, endpoint=True)
+        d_r, d_c = pcg.to_device(roots), pcg.to_device(cws)
+        d_leaves = pcg.DeviceBuffer(16 * B * D)
+        pcg.dpf_keyed_full_eval_device(B, n, 1, pcg.PRG_CHACHA8, d_r.ptr, d_c.ptr, d_leaves.ptr)
+        pcg.synchronize()
+        got_c, got_t = _sums_noalloc(pcg, d_leaves.ptr, B, D)
+        want_c, want_t = _sums_existing(pcg, d_leaves.ptr, B, D)
+        assert (got_c == want_c).all() and (got_t == want_t).all(), (B, n)
+        d_leaves.free()
+
+
 def test_noalloc_rejects_sizes_beyond_the_static_scratch(pcg):
     d = pcg.DeviceBuffer(16 * 64)
     out = pcg.DeviceBuffer(8)
