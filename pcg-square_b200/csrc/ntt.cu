@@ -313,8 +313,10 @@ __device__ __forceinline__ void row_fwd_body(uint64_t* d, size_t tile,
 // g_q = g + q*N, img_q = img + q*N; img_q in the permuted evaluation order,
 // Montgomery-scaled so that the Montgomery product gives the plain one.
 // g rows come from the column pass; out is in [0, p) and may alias g (a CTA
-// reads all its rows before its first store).
-template <int L, int V>
+// reads all its rows before its first store).  ONE (Q == 1, a plain
+// product): the product stays in the transform's registers, with no
+// separate accumulator live across the forward phases.
+template <int L, int V, bool ONE>
 __device__ __forceinline__ void row_mac_body(const uint64_t* g, const uint64_t* __restrict__ img,
                                              int Q, size_t N, size_t tile,
                                              const ulonglong2* __restrict__ tw,
@@ -326,19 +328,28 @@ __device__ __forceinline__ void row_mac_body(const uint64_t* g, const uint64_t* 
     const size_t base = (tile * V + v) * Geo<L>::n;
     const SmemLay<1> lay{sm + v * Geo<L>::PAD};
     uint64_t acc[E];
+    if constexpr (ONE) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) acc[e] = 0;
-    for (int q = 0; q < Q; ++q) {
-        const uint64_t* gr = g + q * N + base;
-        const uint64_t* im = img + q * N + base;
-        uint64_t x[E];
+        for (int e = 0; e < E; ++e) acc[e] = g[base + eidx<L, 0>(t, e)];
+        forward_all<L>(acc, t, tw, lay);
 #pragma unroll
-        for (int e = 0; e < E; ++e) x[e] = gr[eidx<L, 0>(t, e)];
-        forward_all<L>(x, t, tw, lay);
+        for (int e = 0; e < E; ++e)
+            acc[e] = mont_lazy(acc[e], __ldg(img + base + perm_pos<L>(eidx<L, LP>(t, e))));
+    } else {
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const uint64_t m = mont_lazy(x[e], __ldg(im + perm_pos<L>(eidx<L, LP>(t, e))));
-            acc[e] = csub(acc[e] + m, k2P);
+        for (int e = 0; e < E; ++e) acc[e] = 0;
+        for (int q = 0; q < Q; ++q) {
+            const uint64_t* gr = g + q * N + base;
+            const uint64_t* im = img + q * N + base;
+            uint64_t x[E];
+#pragma unroll
+            for (int e = 0; e < E; ++e) x[e] = gr[eidx<L, 0>(t, e)];
+            forward_all<L>(x, t, tw, lay);
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const uint64_t m = mont_lazy(x[e], __ldg(im + perm_pos<L>(eidx<L, LP>(t, e))));
+                acc[e] = csub(acc[e] + m, k2P);
+            }
         }
     }
     inverse_all<L>(acc, t, twi, lay);
@@ -377,7 +388,7 @@ __global__ void __launch_bounds__(row_threads<L>()) row_fwd_kernel(
 }
 
 // Instance b reads g and img at b*Q*N and writes out at b*N.
-template <int L>
+template <int L, bool ONE>
 __global__ void __launch_bounds__(row_threads<L>()) row_mac_inv_kernel(
     const uint64_t* g, const uint64_t* __restrict__ img, int Q, int l1,
     const ulonglong2* __restrict__ tw, const ulonglong2* __restrict__ twi,
@@ -385,8 +396,8 @@ __global__ void __launch_bounds__(row_threads<L>()) row_mac_inv_kernel(
     extern __shared__ uint64_t sm[];
     const size_t N = size_t{1} << (L + l1);
     const size_t b = blockIdx.y;
-    row_mac_body<L, row_V<L>()>(g + b * Q * N, img + b * Q * N, Q, N, blockIdx.x, tw, twi, Wi,
-                                out + b * N, sm);
+    row_mac_body<L, row_V<L>(), ONE>(g + b * Q * N, img + b * Q * N, Q, N, blockIdx.x, tw, twi,
+                                     Wi, out + b * N, sm);
 }
 
 // ---- mixed-length kernels --------------------------------------------------------
@@ -465,7 +476,7 @@ __global__ void __launch_bounds__(kMixedRowThreads) mixed_row_mac_kernel(
     const MixedPoly& p = polys[j.poly];
     const size_t N = size_t{1} << (p.l1 + p.l2);
 #define PCGB_CALL(LL) \
-    row_mac_body<LL, mixed_V<LL>()>(p.c, p.A, 1, N, j.tile, p.tw2, p.tw2i, p.WiR, p.c, sm)
+    row_mac_body<LL, mixed_V<LL>(), true>(p.c, p.A, 1, N, j.tile, p.tw2, p.tw2i, p.WiR, p.c, sm)
     PCGB_MIXED_SWITCH(p.l2, PCGB_CALL)
 #undef PCGB_CALL
 }
@@ -673,9 +684,16 @@ template <int L>
 void row_mac_l(const NttPlan& pl, const uint64_t* g, const uint64_t* img, int Q, int batch,
                const uint64_t* Wi, uint64_t* out, cudaStream_t st) {
     constexpr size_t sm = row_smem<L>();
-    g_optin(row_mac_inv_kernel<L>, sm);
-    row_mac_inv_kernel<L><<<dim3(pl.n1 / row_V<L>(), batch), row_threads<L>(), sm, st>>>(
-        g, img, Q, pl.l1, pl.tw2, pl.tw2i, Wi, out);
+    const dim3 grid(pl.n1 / row_V<L>(), batch);
+    if (Q == 1) {
+        g_optin(row_mac_inv_kernel<L, true>, sm);
+        row_mac_inv_kernel<L, true><<<grid, row_threads<L>(), sm, st>>>(g, img, Q, pl.l1, pl.tw2,
+                                                                        pl.tw2i, Wi, out);
+    } else {
+        g_optin(row_mac_inv_kernel<L, false>, sm);
+        row_mac_inv_kernel<L, false><<<grid, row_threads<L>(), sm, st>>>(g, img, Q, pl.l1, pl.tw2,
+                                                                         pl.tw2i, Wi, out);
+    }
     PCGB_POST_LAUNCH();
 }
 
