@@ -329,6 +329,21 @@ int pcgb_reduce_mod_p(uint64_t* d, const uint64_t* s, size_t count, void* stream
 int pcgb_expand_device(pcgb_expander* e, int party, const pcgb_blk* d_roots,
                        const pcgb_blk* d_cws, const uint64_t* d_cw_out, const uint64_t* d_pos,
                        const uint64_t* d_val, uint64_t* d_x, uint64_t* d_z, void* stream);
+/* Several expansions of different shapes as one batch (no reference
+ * counterpart; the batching form of GPU_baseline/e2e_full_bench.cu's
+ * expansion loop): request i runs expander e[i] for party[i] on the
+ * device-resident inputs of pcgb_expand_device.  One launch per top-walk
+ * stage, one fused leaf launch, one x launch and three NTT launches cover the
+ * whole batch.  The expanders must share w, the ChaCha8 PRG and the leaf
+ * shape (leaves per thread; set with pcgb_expander_set_leaf_shape), be
+ * unsharded, and have N in 2^14 .. 2^20; each request's x, z equal its
+ * pcgb_expand_device outputs.  Each request's scratch comes from the
+ * library's stream-ordered pool on `stream`. */
+int pcgb_expand_batch_device(int count, pcgb_expander* const* e, const int* party,
+                             const pcgb_blk* const* d_roots, const pcgb_blk* const* d_cws,
+                             const uint64_t* const* d_cw_out, const uint64_t* const* d_pos,
+                             const uint64_t* const* d_val, uint64_t* const* d_x,
+                             uint64_t* const* d_z, void* stream);
 /* Same with host buffers (copies in and out included). */
 int pcgb_expand_host(pcgb_expander* e, int party, const pcgb_blk* roots, const pcgb_blk* cws,
                      const uint64_t* cw_out, const uint64_t* pos, const uint64_t* val,
@@ -422,10 +437,14 @@ int pcgb_deal_keys_device(pcgb_expander* e, uint64_t seed, pcgb_blk* d_roots0,
 /* ---- native: serving ------------------------------------------------------
  * Continuous batching of expansion requests of mixed (N, c, t) on one GPU:
  * requests wait in a FIFO and are admitted onto one of n_streams streams as
- * soon as a stream is free, fewer than max_in_flight are running and the
- * request's HBM footprint (keys, noise, outputs, expansion workspace) fits
- * mem_budget (0 = half of the free memory) next to what is in flight, so
- * their kernels overlap on the device.  Each request deals fresh keys and
+ * soon as a stream is free, fewer than max_in_flight requests are running and
+ * the request's HBM footprint (keys, noise, outputs, expansion workspace)
+ * fits mem_budget (0 = half of the free memory) next to what is in flight,
+ * so their kernels overlap on the device.  Large requests (c^2 N > 2^20) run
+ * one at a time.  When max_in_flight exceeds n_streams, up to 32 queued
+ * small requests with N in 2^14 .. 2^20, of any shapes, are admitted
+ * together onto one stream as one batch (pcgb_expand_batch_device: one
+ * launch per stage for all of them).  Each request deals fresh keys and
  * noise on the GPU from its seed (w = 1, ChaCha8), expands one party against
  * the shape's resident plan (a_i images from a_seed), and reports order-
  * independent digests of x and z (pcgb_digest_device).  n_streams = 1 with

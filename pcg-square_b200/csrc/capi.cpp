@@ -755,6 +755,38 @@ int pcgb_expand_device(pcgb_expander* e, int party, const pcgb_blk* d_roots, con
     });
 }
 
+int pcgb_expand_batch_device(int count, pcgb_expander* const* e, const int* party,
+                             const pcgb_blk* const* d_roots, const pcgb_blk* const* d_cws,
+                             const uint64_t* const* d_cw_out, const uint64_t* const* d_pos,
+                             const uint64_t* const* d_val, uint64_t* const* d_x,
+                             uint64_t* const* d_z, void* stream) {
+    return guarded([&] {
+        if (count < 0) pcgb::fail(PCGB_EINVAL, "expand batch: negative count");
+        if (count == 0) return;
+        if (!e || !party || !d_roots || !d_cws || !d_cw_out || !d_pos || !d_val || !d_x || !d_z)
+            pcgb::fail(PCGB_EINVAL, "expand batch: null array");
+        for (int i = 0; i < count; ++i)
+            if (!e[i]) pcgb::fail(PCGB_EINVAL, "expand batch: null expander");
+        cudaStream_t st = pcgb::as_stream(stream);
+        std::vector<size_t> off(count + 1, 0);
+        for (int i = 0; i < count; ++i)
+            off[i + 1] = off[i] + ((pcgb::workspace_bytes(e[i]) + 255) & ~size_t{255});
+        char* base = static_cast<char*>(pcgb::pool_alloc(off[count], st));
+        std::vector<pcgb::Workspace> ws(count);
+        for (int i = 0; i < count; ++i) ws[i] = pcgb::workspace_carve(e[i], base + off[i]);
+        try {
+            pcgb::expand_batch_ws(count, e, ws.data(), party,
+                                  reinterpret_cast<const Blk* const*>(d_roots),
+                                  reinterpret_cast<const Blk* const*>(d_cws), d_cw_out, d_pos,
+                                  d_val, d_x, d_z, st);
+        } catch (...) {
+            cudaFreeAsync(base, st);
+            throw;
+        }
+        PCGB_CK(cudaFreeAsync(base, st));
+    });
+}
+
 int pcgb_expand_host_async(pcgb_expander* e, int party, const pcgb_blk* roots,
                            const pcgb_blk* cws, const uint64_t* cw_out, const uint64_t* pos,
                            const uint64_t* val, uint64_t* x, uint64_t* z) {

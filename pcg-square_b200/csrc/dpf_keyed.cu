@@ -47,41 +47,53 @@ void keyed_expand_tops(int K, int n, int w, int prg, const Blk* roots, const Blk
         keyed_tops_chacha(K, levels, w, roots, cws, nullptr, nullptr, to_level, out, scratch, st);
 }
 
-// Stage plan of a multi-group evaluation: every group walks its own
-// geometric stages (tops_stages) with its own ping-pong scratch; launch s
-// carries stage s of every group that has one, so the whole batch takes as
-// many launches as its deepest plan has stages.
-void keyed_full_eval_multi(int groups, const int* K, const int* n, int w, int prg,
-                           const Blk* const* roots, const Blk* const* cws, const uint32_t* d_rk,
-                           Blk* const* leaves, cudaStream_t st) {
+// Stage plan of a multi-group walk: every group walks its own geometric
+// stages (tops_stages) down to its own target level with its own ping-pong
+// scratch; launch s carries stage s of every group that has one, so the
+// whole batch takes as many launches as its deepest plan has stages.
+// scratch[g] (2 * keyed_tops_scratch_nodes-sized halves) may be null, in
+// which case the scratch comes from the library's pool.
+void keyed_tops_multi(int groups, const int* K, const int* n, const int* to_level, int w, int prg,
+                      const Blk* const* roots, const Blk* const* cws, const uint32_t* d_rk,
+                      Blk* const* out, Blk* const* scratch, cudaStream_t st) {
     if (groups <= 0) return;
-    if (!K || !n || !roots || !cws || !leaves) fail(PCGB_EINVAL, "keyed eval multi: null array");
+    if (!K || !n || !to_level || !roots || !cws || !out)
+        fail(PCGB_EINVAL, "keyed eval multi: null array");
     if (w < 1 || w > 4) fail(PCGB_EINVAL, "keyed eval multi: w must be in [1,4]");
     if (prg == PCGB_PRG_AES && !d_rk) fail(PCGB_EINVAL, "keyed eval multi: AES needs round keys");
     struct Plan {
         std::vector<int> b;
-        size_t half = 0, off = 0;
+        size_t half = 0;
+        Blk* base = nullptr;
         int levels = 0;
     };
     std::vector<Plan> plan(groups);
-    size_t scratch_nodes = 0;
+    size_t pool_nodes = 0;
     size_t stages = 0;
     for (int g = 0; g < groups; ++g) {
         if (K[g] < 0) fail(PCGB_EINVAL, "keyed eval multi: negative key count");
         if (K[g] == 0) continue;
         if (n[g] < 1 || n[g] > 30 || n[g] % w) fail(PCGB_EINVAL, "keyed eval multi: bad (n, w)");
-        if (!roots[g] || !cws[g] || !leaves[g]) fail(PCGB_EINVAL, "keyed eval multi: null group buffer");
+        if (to_level[g] < 0 || to_level[g] > n[g] / w)
+            fail(PCGB_EINVAL, "keyed eval multi: bad target level");
+        if (!roots[g] || !cws[g] || !out[g]) fail(PCGB_EINVAL, "keyed eval multi: null group buffer");
         Plan& P = plan[g];
         P.levels = n[g] / w;
-        P.b = tops_stages(K[g], w, P.levels);
+        P.b = tops_stages(K[g], w, to_level[g]);
         if (P.b.size() > 2) P.half = static_cast<size_t>(K[g]) << (w * P.b[P.b.size() - 2]);
-        P.off = scratch_nodes;
-        scratch_nodes += 2 * P.half;
+        if (scratch && scratch[g]) P.base = scratch[g];
+        else pool_nodes += 2 * P.half;
         stages = std::max(stages, P.b.size() - 1);
     }
     if (stages == 0) return;
-    Blk* scratch = scratch_nodes ? static_cast<Blk*>(pool_alloc(scratch_nodes * sizeof(Blk), st))
-                                 : nullptr;
+    Blk* pool = pool_nodes ? static_cast<Blk*>(pool_alloc(pool_nodes * sizeof(Blk), st)) : nullptr;
+    size_t o = 0;
+    for (int g = 0; g < groups; ++g) {
+        Plan& P = plan[g];
+        if (K[g] == 0 || P.base || P.half == 0) continue;
+        P.base = pool + o;
+        o += 2 * P.half;
+    }
     TopsJob* d_jobs = static_cast<TopsJob*>(pool_alloc(groups * sizeof(TopsJob), st));
     try {
         for (size_t s = 0; s < stages; ++s) {
@@ -90,10 +102,9 @@ void keyed_full_eval_multi(int groups, const int* K, const int* n, int w, int pr
             for (int g = 0; g < groups; ++g) {
                 const Plan& P = plan[g];
                 if (K[g] == 0 || s + 1 >= P.b.size()) continue;
-                Blk* base = scratch ? scratch + P.off : nullptr;
                 TopsJob J;
-                J.src = s == 0 ? roots[g] : base + ((s - 1) % 2) * P.half;
-                J.dst = (s + 2 == P.b.size()) ? leaves[g] : base + (s % 2) * P.half;
+                J.src = s == 0 ? roots[g] : P.base + ((s - 1) % 2) * P.half;
+                J.dst = (s + 2 == P.b.size()) ? out[g] : P.base + (s % 2) * P.half;
                 J.cws = cws[g];
                 J.first = total;
                 J.K = K[g];
@@ -109,12 +120,24 @@ void keyed_full_eval_multi(int groups, const int* K, const int* n, int w, int pr
                 keyed_tops_multi_chacha(w, jobs, d_jobs, total, st);
         }
     } catch (...) {
-        if (scratch) cudaFreeAsync(scratch, st);
+        if (pool) cudaFreeAsync(pool, st);
         cudaFreeAsync(d_jobs, st);
         throw;
     }
-    if (scratch) PCGB_CK(cudaFreeAsync(scratch, st));
+    if (pool) PCGB_CK(cudaFreeAsync(pool, st));
     PCGB_CK(cudaFreeAsync(d_jobs, st));
+}
+
+// Full-domain evaluation of key groups of different domains: the multi-group
+// walk down to every group's last level.
+void keyed_full_eval_multi(int groups, const int* K, const int* n, int w, int prg,
+                           const Blk* const* roots, const Blk* const* cws, const uint32_t* d_rk,
+                           Blk* const* leaves, cudaStream_t st) {
+    if (groups <= 0) return;
+    if (!n) fail(PCGB_EINVAL, "keyed eval multi: null array");
+    std::vector<int> to(groups);
+    for (int g = 0; g < groups; ++g) to[g] = (w >= 1 && w <= 4) ? n[g] / w : 0;
+    keyed_tops_multi(groups, K, n, to.data(), w, prg, roots, cws, d_rk, leaves, nullptr, st);
 }
 
 // Gather plan: for pair q = (i <= j) and output bin r, the key halves of

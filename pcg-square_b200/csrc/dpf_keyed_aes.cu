@@ -24,6 +24,11 @@ void keyed_tops_multi_aes(int w, const std::vector<TopsJob>& jobs, TopsJob* d_jo
     tops_multi_for_prg<kPrgAes>(w, jobs, d_jobs, total, te, rk, st);
 }
 
+void keyed_leaf_multi_aes(int w, int sl, const LeafJob* d_jobs, int njobs, unsigned ctas, int tpb,
+                          size_t smem, const uint32_t* te, const uint32_t* rk, cudaStream_t st) {
+    leaf_multi_for_prg<kPrgAes>(w, sl, d_jobs, njobs, ctas, tpb, smem, te, rk, st);
+}
+
 size_t keyed_aes_smem_bytes_aes() { return sizeof(AesSmem); }
 
 }  // namespace pcgb

@@ -24,6 +24,11 @@ void keyed_tops_multi_chacha(int w, const std::vector<TopsJob>& jobs, TopsJob* d
     tops_multi_for_prg<kPrgChaCha>(w, jobs, d_jobs, total, nullptr, nullptr, st);
 }
 
+void keyed_leaf_multi_chacha(int w, int sl, const LeafJob* d_jobs, int njobs, unsigned ctas, int tpb,
+                          size_t smem, const uint32_t* te, const uint32_t* rk, cudaStream_t st) {
+    leaf_multi_for_prg<kPrgChaCha>(w, sl, d_jobs, njobs, ctas, tpb, smem, te, rk, st);
+}
+
 size_t keyed_aes_smem_bytes_chacha() { return sizeof(AesSmem); }
 
 }  // namespace pcgb

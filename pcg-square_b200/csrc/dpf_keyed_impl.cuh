@@ -308,26 +308,23 @@ struct DfsM {
     }
 };
 
+// One CTA's tile of the fused leaf kernel: output bin r of launched pair
+// z, tile bx.  acc_s is the CTA's dynamic shared memory (blockDim.x rows of
+// S + 1 128-bit accumulators).
 template <int W, int SL, int PRG>
-__global__ void __launch_bounds__(256) leaf_gather_kernel(
+__device__ __forceinline__ void leaf_gather_tile(
     const Blk* __restrict__ F, const Blk* __restrict__ cws, const uint64_t* __restrict__ cw_out,
     const uint32_t* __restrict__ off, const uint32_t* __restrict__ entries,
     const uint16_t* __restrict__ q_order, const uint16_t* __restrict__ q_slot, int t, int levels,
-    int hl, size_t bin, int N,
-    int party, const uint32_t* __restrict__ aes_te, const uint32_t* __restrict__ aes_rk,
-    uint64_t* __restrict__ gq) {
+    int hl, size_t bin, int N, int party, uint64_t* __restrict__ gq, unsigned bx, int r, int z,
+    ulonglong2* acc_s, const AesSmem* aes_s) {
     constexpr int M = 1 << W, NK = M - 1;
     constexpr int S = 1 << (W * SL);
     constexpr int STRIDE = S + 1;  // padded accumulator rows: conflict-free
-    extern __shared__ __align__(16) ulonglong2 acc_s[];
-    AesSmem& aes_s = *reinterpret_cast<AesSmem*>(acc_s + blockDim.x * STRIDE);
-    if constexpr (PRG == kPrgAes) load_aes_smem(aes_s, aes_te, aes_rk, NK);
-
-    const int r = blockIdx.y;
-    const int q = q_order[blockIdx.z];
-    const int slot = q_slot[blockIdx.z];
+    const int q = q_order[z];
+    const int slot = q_slot[z];
     const size_t tile = static_cast<size_t>(blockDim.x) * S;
-    const size_t o = static_cast<size_t>(blockIdx.x) * tile + static_cast<size_t>(threadIdx.x) * S;
+    const size_t o = static_cast<size_t>(bx) * tile + static_cast<size_t>(threadIdx.x) * S;
     ulonglong2* acc = acc_s + threadIdx.x * STRIDE;
 #pragma unroll
     for (int u = 0; u < S; ++u) acc[u] = make_ulonglong2(0, 0);
@@ -344,15 +341,52 @@ __global__ void __launch_bounds__(256) leaf_gather_kernel(
         c.cwo = __ldg(cw_out + key);
         const Blk node = ldblk(F + key * per_key + (half * bin + o) / S);
         const Blk* kcw = cws + (key * levels + hl) * NK;
-        if constexpr (W == 1) Dfs1<SL, PRG>::run(node, kcw, &aes_s, 0, c);
-        else DfsM<W, SL, PRG>::run(node, kcw, &aes_s, 0, c);
+        if constexpr (W == 1) Dfs1<SL, PRG>::run(node, kcw, aes_s, 0, c);
+        else DfsM<W, SL, PRG>::run(node, kcw, aes_s, 0, c);
     }
     __syncthreads();
     // Coalesced write-out of the CTA's tile.
     uint64_t* dst = gq + static_cast<size_t>(slot) * N + static_cast<size_t>(r) * bin +
-                    static_cast<size_t>(blockIdx.x) * tile;
+                    static_cast<size_t>(bx) * tile;
     for (size_t e = threadIdx.x; e < tile; e += blockDim.x)
         dst[e] = acc_mod_p(acc_s[(e / S) * STRIDE + (e % S)]);
+}
+
+template <int W, int SL, int PRG>
+__global__ void __launch_bounds__(256) leaf_gather_kernel(
+    const Blk* __restrict__ F, const Blk* __restrict__ cws, const uint64_t* __restrict__ cw_out,
+    const uint32_t* __restrict__ off, const uint32_t* __restrict__ entries,
+    const uint16_t* __restrict__ q_order, const uint16_t* __restrict__ q_slot, int t, int levels,
+    int hl, size_t bin, int N,
+    int party, const uint32_t* __restrict__ aes_te, const uint32_t* __restrict__ aes_rk,
+    uint64_t* __restrict__ gq) {
+    constexpr int NK = (1 << W) - 1, S = 1 << (W * SL);
+    extern __shared__ __align__(16) ulonglong2 acc_s[];
+    AesSmem& aes_s = *reinterpret_cast<AesSmem*>(acc_s + blockDim.x * (S + 1));
+    if constexpr (PRG == kPrgAes) load_aes_smem(aes_s, aes_te, aes_rk, NK);
+    leaf_gather_tile<W, SL, PRG>(F, cws, cw_out, off, entries, q_order, q_slot, t, levels, hl, bin,
+                                 N, party, gq, blockIdx.x, blockIdx.y, blockIdx.z, acc_s, &aes_s);
+}
+
+// The fused leaf kernel over several expansions (one job each, same w, sl,
+// PRG and CTA size): CTA b belongs to the job whose CTA range holds b, and
+// runs that job's tile (bx, r, z) = its local index in x-fastest order.
+template <int W, int SL, int PRG>
+__global__ void __launch_bounds__(256) leaf_gather_multi_kernel(
+    const LeafJob* __restrict__ jobs, int njobs, const uint32_t* __restrict__ aes_te,
+    const uint32_t* __restrict__ aes_rk) {
+    constexpr int NK = (1 << W) - 1, S = 1 << (W * SL);
+    extern __shared__ __align__(16) ulonglong2 acc_s[];
+    AesSmem& aes_s = *reinterpret_cast<AesSmem*>(acc_s + blockDim.x * (S + 1));
+    if constexpr (PRG == kPrgAes) load_aes_smem(aes_s, aes_te, aes_rk, NK);
+    int k = 0;
+    while (k + 1 < njobs && jobs[k + 1].first <= blockIdx.x) ++k;
+    const LeafJob& J = jobs[k];
+    const unsigned local = blockIdx.x - J.first;
+    const unsigned bx = local % J.gx, r = (local / J.gx) % J.gy, z = local / (J.gx * J.gy);
+    leaf_gather_tile<W, SL, PRG>(J.F, J.cws, J.cw_out, J.off, J.entries, J.q_order, J.q_slot, J.t,
+                                 J.levels, J.hl, J.bin, J.N, J.party, J.gq, bx,
+                                 static_cast<int>(r), static_cast<int>(z), acc_s, &aes_s);
 }
 
 template <int W, int PRG>
@@ -496,6 +530,32 @@ void leaf_one(const LeafLaunch& L) {
                                          L.q_slot, L.t,
                                          L.levels, L.hl, L.bin, L.N, L.party, L.te, L.rk, L.gq);
     PCGB_POST_LAUNCH();
+}
+
+template <int W, int SL, int PRG>
+void leaf_multi_one(const LeafJob* d_jobs, int njobs, unsigned ctas, int tpb, size_t smem,
+                    const uint32_t* te, const uint32_t* rk, cudaStream_t st) {
+    auto kern = leaf_gather_multi_kernel<W, SL, PRG>;
+    if (smem > 48 * 1024)
+        PCGB_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+    kern<<<ctas, tpb, smem, st>>>(d_jobs, njobs, te, rk);
+    PCGB_POST_LAUNCH();
+}
+
+template <int PRG>
+void leaf_multi_for_prg(int w, int sl, const LeafJob* d_jobs, int njobs, unsigned ctas, int tpb,
+                        size_t smem, const uint32_t* te, const uint32_t* rk, cudaStream_t st) {
+    switch (w * 8 + sl) {
+#define PCGB_LM(W_, SL_)                                                              \
+    case W_ * 8 + SL_:                                                                \
+        leaf_multi_one<W_, SL_, PRG>(d_jobs, njobs, ctas, tpb, smem, te, rk, st); \
+        break;
+        PCGB_LM(1, 4) PCGB_LM(1, 3) PCGB_LM(1, 2) PCGB_LM(1, 1)
+        PCGB_LM(2, 2) PCGB_LM(2, 1) PCGB_LM(3, 1) PCGB_LM(4, 1)
+#undef PCGB_LM
+        default: fail(PCGB_EINVAL, "unsupported (w, sl) for the leaf kernel");
+    }
 }
 
 template <int PRG>

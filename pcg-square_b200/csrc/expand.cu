@@ -38,17 +38,18 @@ namespace {
 // when p < pos_ik, plus sum_k [p == pos_0k] val_0k when a_0 = 1 (i0 = 1).
 // aR holds a_i0 .. a_{c-1} times 2^64 mod p, so one Montgomery product
 // gives a_i * val.
-__global__ void x_kernel(const uint64_t* __restrict__ pos, const uint64_t* __restrict__ val,
-                         const uint64_t* __restrict__ aR, int c, int t, int i0, size_t N,
-                         uint64_t* __restrict__ x) {
-    extern __shared__ uint64_t nz[];  // [c*t] positions then [c*t] values
+__device__ __forceinline__ void x_body(const uint64_t* __restrict__ pos,
+                                       const uint64_t* __restrict__ val,
+                                       const uint64_t* __restrict__ aR, int c, int t, int i0,
+                                       size_t N, uint64_t* __restrict__ x, unsigned block,
+                                       uint64_t* nz /* [c*t] positions then [c*t] values */) {
     const int ct = c * t;
     for (int i = threadIdx.x; i < ct; i += blockDim.x) {
         nz[i] = pos[i] % N;
         nz[ct + i] = reduce_p(val[i]);
     }
     __syncthreads();
-    const size_t p = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t p = static_cast<size_t>(block) * blockDim.x + threadIdx.x;
     if (p >= N) return;
     uint64_t acc = 0;
     if (i0 == 1)
@@ -65,6 +66,57 @@ __global__ void x_kernel(const uint64_t* __restrict__ pos, const uint64_t* __res
         }
     }
     x[p] = acc;
+}
+
+__global__ void x_kernel(const uint64_t* __restrict__ pos, const uint64_t* __restrict__ val,
+                         const uint64_t* __restrict__ aR, int c, int t, int i0, size_t N,
+                         uint64_t* __restrict__ x) {
+    extern __shared__ uint64_t nz[];
+    x_body(pos, val, aR, c, t, i0, N, x, blockIdx.x, nz);
+}
+
+// x of several expansions in one launch: CTA b runs block b - first of the
+// job whose CTA range holds b.
+struct XJob {
+    const uint64_t* pos;
+    const uint64_t* val;
+    const uint64_t* aR;
+    uint64_t* x;
+    size_t N;
+    int c, t, i0;
+    unsigned first;
+};
+__global__ void x_multi_kernel(const XJob* __restrict__ jobs, int njobs) {
+    extern __shared__ uint64_t nz[];
+    int k = 0;
+    while (k + 1 < njobs && jobs[k + 1].first <= blockIdx.x) ++k;
+    const XJob& J = jobs[k];
+    x_body(J.pos, J.val, J.aR, J.c, J.t, J.i0, J.N, J.x, blockIdx.x - J.first, nz);
+}
+
+// Digests of several vectors in one launch: job k covers CTAs
+// [k * per, (k + 1) * per); every output word must be zeroed first.
+struct DigestJob {
+    const uint64_t* v;
+    size_t n;
+    unsigned long long* out;
+};
+__global__ void digest_multi_kernel(const DigestJob* __restrict__ jobs, unsigned per) {
+    __shared__ unsigned long long part[32];
+    const DigestJob J = jobs[blockIdx.x / per];
+    const unsigned b = blockIdx.x % per;
+    unsigned long long acc = 0;
+    for (size_t i = static_cast<size_t>(b) * blockDim.x + threadIdx.x; i < J.n;
+         i += static_cast<size_t>(per) * blockDim.x)
+        acc += mix64(J.v[i] ^ (i * 0x9e3779b97f4a7c15ULL));
+    for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long s = 0;
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += part[w];
+        atomicAdd(J.out, s);
+    }
 }
 
 // d[i] = mont(s[i], k): multiply by a constant given in Montgomery form.
@@ -311,6 +363,122 @@ void expand_device_ws(pcgb_expander* e, const Workspace& ws, int party, const Bl
     if (e->gp.Qs > 0) ntt_mac_inverse(*e->ntt, ws.g, e->d_img, e->gp.Qs, z, st);
     else PCGB_CK(cudaMemsetAsync(z, 0, sizeof(uint64_t) * NN, st));   // a shard with no pairs
     if (ev) PCGB_CK(cudaEventRecord(ev[4], st));
+}
+
+// Expansions of different shapes as one batch (ChaCha8, one w and one leaf
+// depth sl for all): one launch per top-walk stage, one fused leaf launch,
+// one x launch and three NTT launches for the whole batch, each CTA finding
+// its expansion in a job table.  Outputs equal expand_device_ws's, request by
+// request.  All job tables travel in one copy from pinned or pageable host
+// memory on `st`.
+void expand_batch_ws(int count, pcgb_expander* const* e, const Workspace* ws, const int* party,
+                     const Blk* const* roots, const Blk* const* cws,
+                     const uint64_t* const* cw_out, const uint64_t* const* pos,
+                     const uint64_t* const* val, uint64_t* const* x, uint64_t* const* z,
+                     cudaStream_t st) {
+    if (count <= 0) return;
+    const int w = e[0]->w, sl = e[0]->gp.sl, S = e[0]->gp.S;
+    for (int i = 0; i < count; ++i) {
+        const pcgb_expander* E = e[i];
+        if (!E || !ws[i].F || !ws[i].g) fail(PCGB_EINVAL, "expand batch: null expander or workspace");
+        if (E->prg != PCGB_PRG_CHACHA8) fail(PCGB_EINVAL, "expand batch: ChaCha8 expanders only");
+        if (E->w != w || E->gp.sl != sl)
+            fail(PCGB_EINVAL, "expand batch: every expander needs the same w and leaf shape");
+        if (E->gp.world != 1) fail(PCGB_EINVAL, "expand batch: sharded expanders are not batched");
+        if (!ntt_mac_multi_ok(ilog2(E->N))) fail(PCGB_EINVAL, "expand batch: N must be 2^14 .. 2^20");
+        if (party[i] != 0 && party[i] != 1) fail(PCGB_EINVAL, "expand: party must be 0 or 1");
+        if (!roots[i] || !cws[i] || !cw_out[i] || !pos[i] || !val[i] || !x[i] || !z[i])
+            fail(PCGB_EINVAL, "expand: null pointer");
+    }
+    // Stage 1: the top-level walks, each to its expander's frontier level.
+    {
+        std::vector<int> K(count), n(count), hl(count);
+        std::vector<const Blk*> r(count), c(count);
+        std::vector<Blk*> out(count), scr(count);
+        for (int i = 0; i < count; ++i) {
+            K[i] = e[i]->K; n[i] = e[i]->n; hl[i] = e[i]->gp.hl;
+            r[i] = roots[i];
+            c[i] = cws[i]; out[i] = ws[i].F; scr[i] = ws[i].tops;
+        }
+        keyed_tops_multi(count, K.data(), n.data(), hl.data(), w, PCGB_PRG_CHACHA8, r.data(),
+                         c.data(), nullptr, out.data(), scr.data(), st);
+    }
+    // Job tables of the leaf and x launches.
+    int tpb = 256;
+    for (int i = 0; i < count; ++i) {
+        const size_t bin = static_cast<size_t>(e[i]->N) / e[i]->t;
+        int tp = e[i]->gp.tpb > 0 ? e[i]->gp.tpb : 256;
+        while (tp > 1 && static_cast<size_t>(tp) * S > bin) tp >>= 1;
+        if (static_cast<size_t>(tp) * S > bin) fail(PCGB_EINVAL, "bin smaller than one tile");
+        tpb = std::min(tpb, tp);
+    }
+    std::vector<LeafJob> leaf(count);
+    std::vector<XJob> xj(count);
+    unsigned leaf_ctas = 0, x_ctas = 0;
+    size_t x_smem = 0;
+    for (int i = 0; i < count; ++i) {
+        const pcgb_expander* E = e[i];
+        LeafJob& L = leaf[i];
+        L.F = ws[i].F; L.cws = cws[i]; L.cw_out = cw_out[i];
+        L.off = E->gp.d_off; L.entries = E->gp.d_entries;
+        L.q_order = E->gp.d_qorder; L.q_slot = E->gp.d_qslot; L.gq = ws[i].g;
+        L.bin = static_cast<size_t>(E->N) / E->t;
+        L.t = E->t; L.levels = E->levels; L.hl = E->gp.hl; L.N = E->N; L.party = party[i];
+        L.gx = static_cast<unsigned>(L.bin / (static_cast<size_t>(tpb) * S));
+        L.gy = static_cast<unsigned>(E->t);
+        L.first = leaf_ctas;
+        leaf_ctas += L.gx * L.gy * static_cast<unsigned>(E->gp.Qs);
+        XJob& X = xj[i];
+        X.pos = pos[i]; X.val = val[i]; X.aR = E->d_aR; X.x = x[i];
+        X.N = static_cast<size_t>(E->N); X.c = E->c; X.t = E->t; X.i0 = E->i0;
+        X.first = x_ctas;
+        x_ctas += blocks_for(X.N, 256);
+        x_smem = std::max(x_smem, sizeof(uint64_t) * 2 * static_cast<size_t>(E->c) * E->t);
+    }
+    const size_t b_leaf = sizeof(LeafJob) * count;
+    const size_t o_x = (b_leaf + 255) & ~size_t{255};
+    const size_t total = o_x + sizeof(XJob) * count;
+    std::vector<char> host(total);
+    std::memcpy(host.data(), leaf.data(), b_leaf);
+    std::memcpy(host.data() + o_x, xj.data(), sizeof(XJob) * count);
+    char* tab = static_cast<char*>(pool_alloc(total, st));
+    PCGB_CK(cudaMemcpyAsync(tab, host.data(), total, cudaMemcpyHostToDevice, st));
+    // Stage 2: the fused leaf kernel over every expansion's tiles.
+    const size_t leaf_smem = static_cast<size_t>(tpb) * (S + 1) * 2 * sizeof(uint64_t);
+    keyed_leaf_multi_chacha(w, sl, reinterpret_cast<const LeafJob*>(tab), count, leaf_ctas, tpb,
+                            leaf_smem, nullptr, nullptr, st);
+    // Stage 3: the sparse x products.
+    x_multi_kernel<<<x_ctas, 256, x_smem, st>>>(reinterpret_cast<const XJob*>(tab + o_x), count);
+    PCGB_POST_LAUNCH();
+    // Stage 4: NTT multiply-accumulate and inverse, all lengths at once.
+    std::vector<uint64_t*> g(count), zz(count);
+    std::vector<const uint64_t*> img(count);
+    std::vector<int> Q(count), lg(count);
+    for (int i = 0; i < count; ++i) {
+        g[i] = ws[i].g; img[i] = e[i]->d_img; Q[i] = e[i]->gp.Qs; zz[i] = z[i];
+        lg[i] = ilog2(e[i]->N);
+    }
+    ntt_mac_inverse_multi(count, g.data(), img.data(), Q.data(), zz.data(), lg.data(), st);
+    PCGB_CK(cudaFreeAsync(tab, st));
+}
+
+// out[i] (device words, zeroed here) = digest of v[i][0 .. n[i]), one launch.
+void digest_multi_device(int count, const uint64_t* const* v, const size_t* n, uint64_t* const* out,
+                         cudaStream_t st) {
+    if (count <= 0) return;
+    std::vector<DigestJob> jobs(count);
+    size_t longest = 1;
+    for (int i = 0; i < count; ++i) {
+        jobs[i] = DigestJob{v[i], n[i], reinterpret_cast<unsigned long long*>(out[i])};
+        longest = std::max(longest, n[i]);
+    }
+    const unsigned per = static_cast<unsigned>(std::min<size_t>((longest + 255) / 256, 256));
+    DigestJob* d = static_cast<DigestJob*>(pool_alloc(sizeof(DigestJob) * count, st));
+    PCGB_CK(cudaMemcpyAsync(d, jobs.data(), sizeof(DigestJob) * count, cudaMemcpyHostToDevice, st));
+    for (int i = 0; i < count; ++i) PCGB_CK(cudaMemsetAsync(out[i], 0, sizeof(uint64_t), st));
+    digest_multi_kernel<<<per * static_cast<unsigned>(count), 256, 0, st>>>(d, per);
+    PCGB_POST_LAUNCH();
+    PCGB_CK(cudaFreeAsync(d, st));
 }
 
 // The expander's own workspace, allocated on first use (plans held by the

@@ -48,6 +48,7 @@
 #include "pcgb_internal.h"
 
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -492,6 +493,76 @@ __global__ void __launch_bounds__(kMixedColThreads, 2) mixed_col_inv_kernel(
 }
 #undef PCGB_MIXED_SWITCH
 
+// ---- multi-request multiply-accumulate ------------------------------------
+// The step-4 transforms of several expansions of different lengths
+// 2^14 .. 2^20 (sub-lengths 2^7 .. 2^10) in three launches: the column pass
+// of every request's Q g' buffers, the Q-way multiply-accumulate row pass
+// with its inverse, and the inverse column pass into each request's z.  The
+// CTA shapes are the mixed kernels' (512 column threads, 64 row threads,
+// the same shared memory at every sub-length down to 2^7).
+struct MacReq {
+    uint64_t* g;                 // Q*N words, column-transformed in place
+    const uint64_t* img;         // Q*N, Montgomery-scaled evaluation images
+    uint64_t* z;                 // N
+    const ulonglong2* tw1;
+    const ulonglong2* tw1i;
+    const ulonglong2* tw2;
+    const ulonglong2* tw2i;
+    const uint64_t* W;
+    const uint64_t* Wi;
+    int Q, l1, l2;
+};
+struct MacCta {
+    uint32_t req, q, tile;
+};
+constexpr int kMacLmin = 7;
+static_assert(sizeof(uint64_t) * Geo<7>::PAD * mixed_C<7>() == kMixedColSmem &&
+              sizeof(uint64_t) * Geo<7>::PAD * mixed_V<7>() == kMixedRowSmem,
+              "sub-length 2^7 fits the mixed CTA shapes");
+
+#define PCGB_MAC_SWITCH(LEN, CALL) \
+    switch (LEN) {                  \
+        case 7: CALL(7); break;     \
+        case 8: CALL(8); break;     \
+        case 9: CALL(9); break;     \
+        case 10: CALL(10); break;   \
+        default: break;             \
+    }
+
+__global__ void __launch_bounds__(kMixedColThreads, 2) mac_col_fwd_kernel(
+    const MacReq* __restrict__ reqs, const MacCta* __restrict__ ctas) {
+    extern __shared__ uint64_t sm[];
+    const MacCta j = ctas[blockIdx.x];
+    const MacReq& r = reqs[j.req];
+    uint64_t* d = r.g + (static_cast<size_t>(j.q) << (r.l1 + r.l2));
+#define PCGB_CALL(LL) col_fwd_body<LL, mixed_C<LL>(), false>(d, d, r.l2, j.tile, r.tw1, r.W, sm)
+    PCGB_MAC_SWITCH(r.l1, PCGB_CALL)
+#undef PCGB_CALL
+}
+
+__global__ void __launch_bounds__(kMixedRowThreads) mac_row_kernel(
+    const MacReq* __restrict__ reqs, const MacCta* __restrict__ ctas) {
+    extern __shared__ uint64_t sm[];
+    const MacCta j = ctas[blockIdx.x];
+    const MacReq& r = reqs[j.req];
+    const size_t N = size_t{1} << (r.l1 + r.l2);
+#define PCGB_CALL(LL) \
+    row_mac_body<LL, mixed_V<LL>(), false>(r.g, r.img, r.Q, N, j.tile, r.tw2, r.tw2i, r.Wi, r.z, sm)
+    PCGB_MAC_SWITCH(r.l2, PCGB_CALL)
+#undef PCGB_CALL
+}
+
+__global__ void __launch_bounds__(kMixedColThreads, 2) mac_col_inv_kernel(
+    const MacReq* __restrict__ reqs, const MacCta* __restrict__ ctas) {
+    extern __shared__ uint64_t sm[];
+    const MacCta j = ctas[blockIdx.x];
+    const MacReq& r = reqs[j.req];
+#define PCGB_CALL(LL) col_inv_body<LL, mixed_C<LL>()>(r.z, r.l2, j.tile, r.tw1i, sm)
+    PCGB_MAC_SWITCH(r.l1, PCGB_CALL)
+#undef PCGB_CALL
+}
+#undef PCGB_MAC_SWITCH
+
 // Twiddle tables: W[k*n2 + j2] = psi^(j2*(2*brev(k)+1-n1)) (times R), and
 // Wi = psi^-(...) * N^-1 (times R).  powR[b] = psi^(2^b) * R mod p.
 __global__ void twiddle_kernel(uint64_t* W, uint64_t* Wi, int l1, int l2,
@@ -862,6 +933,74 @@ void ntt_mac_inverse(const NttPlan& pl, uint64_t* g, const uint64_t* img, int Q,
     col_fwd(pl, g, g, Q, false, st);
     row_mac(pl, g, img, Q, 1, pl.Wi, acc, st);
     col_inv(pl, acc, 1, st);
+}
+
+bool ntt_mac_multi_ok(int logN) { return logN >= 2 * kMacLmin && logN <= 2 * kMixedLmax; }
+
+void ntt_mac_inverse_multi(int count, uint64_t* const* g, const uint64_t* const* img, const int* Q,
+                           uint64_t* const* z, const int* logN, cudaStream_t st) {
+    if (count <= 0) return;
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i) {
+        if (!ntt_mac_multi_ok(logN[i])) fail(PCGB_EINVAL, "multi MAC: N must be 2^14 .. 2^20");
+        if (Q[i] < 1 || !g[i] || !img[i] || !z[i]) fail(PCGB_EINVAL, "multi MAC: bad request");
+        order[i] = i;
+    }
+    // Most work first, so the last CTAs of each pass are short ones.
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return (static_cast<uint64_t>(Q[x]) << logN[x]) > (static_cast<uint64_t>(Q[y]) << logN[y]);
+    });
+    std::vector<MacReq> reqs(count);
+    std::vector<MacCta> colf, row, coli;
+    for (int k = 0; k < count; ++k) {
+        const int i = order[k];
+        const NttPlan& pl = ntt_plan(logN[i]);
+        MacReq& m = reqs[k];
+        m.g = g[i]; m.img = img[i]; m.z = z[i];
+        m.tw1 = pl.tw1; m.tw1i = pl.tw1i; m.tw2 = pl.tw2; m.tw2i = pl.tw2i;
+        m.W = pl.W; m.Wi = pl.Wi;
+        m.Q = Q[i]; m.l1 = pl.l1; m.l2 = pl.l2;
+        int C = 0, V = 0;
+        by_len(pl.l1, [&](auto L) {
+            if constexpr (decltype(L)::value >= kMacLmin && decltype(L)::value <= kMixedLmax)
+                C = mixed_C<decltype(L)::value>();
+        });
+        by_len(pl.l2, [&](auto L) {
+            if constexpr (decltype(L)::value >= kMacLmin && decltype(L)::value <= kMixedLmax)
+                V = mixed_V<decltype(L)::value>();
+        });
+        const uint32_t kk = static_cast<uint32_t>(k);
+        for (uint32_t q = 0; q < static_cast<uint32_t>(m.Q); ++q)
+            for (uint32_t tl = 0; tl < static_cast<uint32_t>(pl.n2 / C); ++tl) colf.push_back({kk, q, tl});
+        for (uint32_t tl = 0; tl < static_cast<uint32_t>(pl.n1 / V); ++tl) row.push_back({kk, 0, tl});
+        for (uint32_t tl = 0; tl < static_cast<uint32_t>(pl.n2 / C); ++tl) coli.push_back({kk, 0, tl});
+    }
+    const size_t b_req = sizeof(MacReq) * reqs.size();
+    const size_t o_colf = (b_req + 255) & ~size_t{255};
+    const size_t o_row = (o_colf + sizeof(MacCta) * colf.size() + 255) & ~size_t{255};
+    const size_t o_coli = (o_row + sizeof(MacCta) * row.size() + 255) & ~size_t{255};
+    const size_t total = o_coli + sizeof(MacCta) * coli.size();
+    std::vector<char> host(total);
+    std::memcpy(host.data(), reqs.data(), b_req);
+    std::memcpy(host.data() + o_colf, colf.data(), sizeof(MacCta) * colf.size());
+    std::memcpy(host.data() + o_row, row.data(), sizeof(MacCta) * row.size());
+    std::memcpy(host.data() + o_coli, coli.data(), sizeof(MacCta) * coli.size());
+    char* tab = static_cast<char*>(pool_alloc(total, st));
+    PCGB_CK(cudaMemcpyAsync(tab, host.data(), total, cudaMemcpyHostToDevice, st));
+    const MacReq* d_req = reinterpret_cast<const MacReq*>(tab);
+    g_optin(mac_col_fwd_kernel, kMixedColSmem);
+    g_optin(mac_row_kernel, kMixedRowSmem);
+    g_optin(mac_col_inv_kernel, kMixedColSmem);
+    mac_col_fwd_kernel<<<static_cast<unsigned>(colf.size()), kMixedColThreads, kMixedColSmem, st>>>(
+        d_req, reinterpret_cast<const MacCta*>(tab + o_colf));
+    PCGB_POST_LAUNCH();
+    mac_row_kernel<<<static_cast<unsigned>(row.size()), kMixedRowThreads, kMixedRowSmem, st>>>(
+        d_req, reinterpret_cast<const MacCta*>(tab + o_row));
+    PCGB_POST_LAUNCH();
+    mac_col_inv_kernel<<<static_cast<unsigned>(coli.size()), kMixedColThreads, kMixedColSmem, st>>>(
+        d_req, reinterpret_cast<const MacCta*>(tab + o_coli));
+    PCGB_POST_LAUNCH();
+    PCGB_CK(cudaFreeAsync(tab, st));
 }
 
 void pointwise_mul(uint64_t* c, const uint64_t* a, const uint64_t* b, size_t count, int mode,

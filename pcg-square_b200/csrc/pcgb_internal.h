@@ -79,6 +79,13 @@ struct TopsJob {
     unsigned long long first;   // first global thread index of this job
     int K, src_lvl, nlev, levels;
 };
+// Top-level walk of `groups` key groups of different domains (same w and
+// PRG), each to its own level to_level[g] into out[g]: one launch per stage
+// for all groups.  scratch[g] holds keyed_tops_scratch_nodes(K[g], w,
+// to_level[g]) nodes, or is null (scratch from the pool); scratch may be null.
+void keyed_tops_multi(int groups, const int* K, const int* n, const int* to_level, int w, int prg,
+                      const Blk* const* roots, const Blk* const* cws, const uint32_t* d_rk,
+                      Blk* const* out, Blk* const* scratch, cudaStream_t st);
 // Full-domain evaluation of `groups` key groups of different domains (same
 // w and PRG): one launch per top-walk stage for all groups.
 void keyed_full_eval_multi(int groups, const int* K, const int* n, int w, int prg,
@@ -150,12 +157,31 @@ struct LeafLaunch {
     uint64_t* gq = nullptr;
 };
 
+// One expansion's part of a multi-expansion leaf launch: its LeafLaunch
+// fields plus its CTA range [first, first + gx*gy*gz) in the shared grid.
+struct LeafJob {
+    const Blk* F;
+    const Blk* cws;
+    const uint64_t* cw_out;
+    const uint32_t* off;
+    const uint32_t* entries;
+    const uint16_t* q_order;
+    const uint16_t* q_slot;
+    uint64_t* gq;
+    size_t bin;
+    int t, levels, hl, N, party;
+    unsigned gx, gy, first;
+};
+
 // Per-PRG instantiations (dpf_keyed_chacha.cu / dpf_keyed_aes.cu).
 #define PCGB_KEYED_DECL(NAME)                                                                   \
     void keyed_tops_##NAME(int K, int levels, int w, const Blk* roots, const Blk* cws,          \
                            const uint32_t* te, const uint32_t* rk, int to_level, Blk* out,     \
                            Blk* scratch, cudaStream_t st);                                     \
     void keyed_leaf_##NAME(int w, int sl, const LeafLaunch& L);                                 \
+    void keyed_leaf_multi_##NAME(int w, int sl, const LeafJob* d_jobs, int njobs, unsigned ctas, \
+                                 int tpb, size_t smem, const uint32_t* te, const uint32_t* rk,  \
+                                 cudaStream_t st);                                              \
     void keyed_deal_##NAME(int w, unsigned grid, size_t smem, uint64_t seed, int c, int t,      \
                            int n, uint64_t bin, Blk* roots0, Blk* roots1, Blk* cws,            \
                            uint64_t* cw_out, const uint32_t* te, const uint32_t* rk,           \
@@ -204,6 +230,16 @@ Workspace workspace_carve(const pcgb_expander* e, void* base);
 void expand_device_ws(pcgb_expander* e, const Workspace& ws, int party, const Blk* roots,
                       const Blk* cws, const uint64_t* cw_out, const uint64_t* pos,
                       const uint64_t* val, uint64_t* x, uint64_t* z, cudaStream_t st);
+// Several expansions of different shapes as one batch (ChaCha8, the same w
+// and leaf shape for all; N in 2^14 .. 2^20): one launch per stage for the
+// whole batch; each request's outputs equal expand_device_ws's.
+void expand_batch_ws(int count, pcgb_expander* const* e, const Workspace* ws, const int* party,
+                     const Blk* const* roots, const Blk* const* cws,
+                     const uint64_t* const* cw_out, const uint64_t* const* pos,
+                     const uint64_t* const* val, uint64_t* const* x, uint64_t* const* z,
+                     cudaStream_t st);
+void digest_multi_device(int count, const uint64_t* const* v, const size_t* n, uint64_t* const* out,
+                         cudaStream_t st);
 void deal_keys_device(pcgb_expander* e, uint64_t seed, Blk* r0, Blk* r1, Blk* cws, uint64_t* cwo,
                       cudaStream_t st);
 void noise_device(int N, int c, int t, uint64_t seed, int party, uint64_t* pos, uint64_t* val,
@@ -244,6 +280,11 @@ void poly_mul_device_mixed(int count, uint64_t* const* c, const uint64_t* const*
 // place); img in Montgomery-scaled evaluation layout.
 void ntt_mac_inverse(const NttPlan& pl, uint64_t* g, const uint64_t* img, int Q, uint64_t* acc,
                      cudaStream_t st);
+// The same for `count` requests of different lengths N_i = 2^logN[i] in
+// 2^14 .. 2^20 (Q[i] buffers each), three launches for all of them.
+bool ntt_mac_multi_ok(int logN);
+void ntt_mac_inverse_multi(int count, uint64_t* const* g, const uint64_t* const* img, const int* Q,
+                           uint64_t* const* z, const int* logN, cudaStream_t st);
 // Pointwise c[i] = a[i]*b[i]*R mod p over `count` words (R = 2^64): turns
 // an evaluation vector into its Montgomery-scaled form when b = R^2 scaled.
 void pointwise_mul(uint64_t* c, const uint64_t* a, const uint64_t* b, size_t count, int mode,

@@ -122,6 +122,8 @@ def _load():
         "pcgb_expander_info": ([_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                 C.POINTER(C.c_size_t)], C.c_int),
         "pcgb_expand_device": ([_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
+        "pcgb_expand_batch_device": ([C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+                                     C.c_int),
         "pcgb_expand_host": ([_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
         "pcgb_expand_g_device": ([_vp, C.c_int, _vp, _vp, _vp, _vp, _vp], C.c_int),
         "pcgb_expander_set_profiling": ([_vp, C.c_int], C.c_int),
@@ -743,6 +745,19 @@ class Expander:
         return [tuple(ms[4 * i: 4 * i + 4]) for i in range(r)]
 
 
+def expand_batch_device(requests, stream=None):
+    """Several expansions as one batch (pcgb_expand_batch_device).
+    requests: list of (Expander, party, d_roots, d_cws, d_cw_out, d_pos, d_val,
+    d_x, d_z), the pointers device addresses (ints)."""
+    n = len(requests)
+    if n == 0:
+        return
+    col = lambda k: (C.c_void_p * n)(*[r[k] for r in requests])
+    _check(lib.pcgb_expand_batch_device(n, (C.c_void_p * n)(*[r[0].h for r in requests]),
+                                        (C.c_int * n)(*[r[1] for r in requests]), col(2), col(3),
+                                        col(4), col(5), col(6), col(7), col(8), stream))
+
+
 def digest_device(d_v, n, stream=None):
     """Order-independent 64-bit digest of n device words (bit-exactness checks)."""
     out = DeviceBuffer(8)
@@ -752,12 +767,14 @@ def digest_device(d_v, n, stream=None):
 
 
 class Server:
-    """Continuous-batching expansion server on the current device."""
+    """Continuous-batching expansion server on the current device.
+    max_in_flight (default 8 x n_streams) above n_streams lets small
+    requests of mixed shapes run as batches (pcgb_server_create)."""
 
     def __init__(self, n_streams=4, mem_budget=0, max_in_flight=None, a_seed=7):
         h = C.c_void_p()
         _check(lib.pcgb_server_create(C.byref(h), n_streams, mem_budget,
-                                      max_in_flight or n_streams, a_seed))
+                                      max_in_flight or 8 * n_streams, a_seed))
         self.h = h.value
 
     def prepare(self, N, c, t):

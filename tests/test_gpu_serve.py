@@ -108,3 +108,25 @@ def test_large_requests_run_one_at_a_time_and_small_ones_pass(pcg):
     assert rb[1].start_s >= rb[0].done_s - 1e-6
     assert rs.start_s < rb[0].done_s
     srv.close()
+
+
+def test_queued_small_requests_run_as_batches(pcg):
+    """Small requests of mixed shapes (N in 2^14 .. 2^18) queued together run
+    as batches: the same digests as one at a time, in far fewer launches."""
+    shapes = [(1 << 14, 2, 8), (1 << 16, 4, 16), (1 << 14, 4, 32), (1 << 18, 2, 8),
+              (1 << 16, 2, 32), (1 << 14, 2, 16)]
+    trace = [(*shapes[i % len(shapes)], i & 1, 700 + i, 0.0) for i in range(24)]
+    runs = {}
+    for name, kw in (("batched", dict(n_streams=1, max_in_flight=32)),
+                     ("alone", dict(n_streams=1, max_in_flight=1))):
+        srv = pcg.Server(a_seed=A_SEED, **kw)
+        for shp in shapes:
+            srv.prepare(*shp)
+        srv.run_trace(trace[:6])          # warm: plans, pool
+        before = pcg.launch_count()
+        res = srv.run_trace(trace, timeout_s=300)
+        runs[name] = ([(r.digest_x, r.digest_z) for r in res], pcg.launch_count() - before)
+        assert all(r.status == 0 for r in res)
+        srv.close()
+    assert runs["batched"][0] == runs["alone"][0]
+    assert runs["batched"][1] * 2 < runs["alone"][1]
