@@ -131,6 +131,8 @@ def parse():
                     help="skip the batched 16 x 2^20 poly-mul measurement")
     ap.add_argument("--no-graph", dest="graph", action="store_false",
                     help="time direct launches instead of CUDA-graph replays")
+    ap.add_argument("--arx-variants", action="store_true",
+                    help="only the ARX probe with quarter-round adds moved to the FMA pipe")
     ap.add_argument("--polymul-only", action="store_true",
                     help="only the batched poly-mul measurement (profiler captures)")
     ap.add_argument("--serve-requests", type=int, default=1000,
@@ -516,7 +518,8 @@ def run_ours(args, d):
     Q = e.Q
     ntt_bytes = 8 * N * (4 * Q + 3)
     roofline_ntt = {"bound": "hbm", "achieved": ntt_bytes / (ntt_ms * 1e-3) / 1e9 if ntt_ms else None,
-                    "peak": hbm_peak(), "unit": "GB/s", "bytes_per_step": ntt_bytes,
+                    "peak": hbm_peak(), "peak_source": hbm_peak_source()[1], "unit": "GB/s",
+                    "bytes_per_step": ntt_bytes,
                     "stage_ms": ntt_ms}
     if roofline_ntt["achieved"]:
         roofline_ntt["frac"] = roofline_ntt["achieved"] / roofline_ntt["peak"]
@@ -593,6 +596,23 @@ def run_ours(args, d):
     e.close()
 
 
+def run_arx_variants(L):
+    """The ARX probe (two ChaCha8 states per thread, every SM full) with a
+    chosen set of the quarter round's four adds issued as multiply-adds on
+    the FMA pipe; median T int-ops/s of 7 launches per variant."""
+    masks = [("none", 0x00000000), ("1 of 8 (add 0, every other QR)", 0x10101010),
+             ("add 0 (1/4)", 0x11111111), ("add 1 (1/4)", 0x22222222),
+             ("adds 0,1 (1/2)", 0x33333333), ("adds 0,2 (1/2)", 0x55555555),
+             ("3 of 8 (adds 0,2 / 0)", 0x15151515), ("3 of 4", 0x77777777),
+             ("all 4", 0xFFFFFFFF)]
+    out = []
+    for name, m in masks:
+        g = L.arx_peak_variant(m)
+        out.append({"adds_on_fma": name, "mask": f"{m:08x}",
+                    "tops_median": float(np.median(g)) / 1e3})
+    return out
+
+
 def run_polymul(L, batch=16, logN=20, steps=10, warmup=3, seed=11):
     """Batched negacyclic product c = a*b mod (X^N + 1, p), 16 x 2^20 words of
     seeded uniform [0, p) inputs, through pcgb_poly_mul_device (forward column
@@ -619,7 +639,8 @@ def run_polymul(L, batch=16, logN=20, steps=10, warmup=3, seed=11):
     out = {"workload": f"{batch} x 2^{logN} negacyclic products, uniform [0,p) inputs",
            "ms_median": med, "ms_min": float(min(ms)),
            "roofline": {"bound": "hbm", "achieved": nbytes / (med * 1e-3) / 1e9,
-                        "peak": hbm_peak(), "unit": "GB/s", "bytes": nbytes}}
+                        "peak": hbm_peak(), "peak_source": hbm_peak_source()[1],
+                        "unit": "GB/s", "bytes": nbytes}}
     out["roofline"]["frac"] = out["roofline"]["achieved"] / out["roofline"]["peak"]
 
     # Mixed lengths in one call (five launches for the batch): 6 x 2^20,
@@ -741,10 +762,18 @@ LEAF_WRITE_BYTES_PER_WORD = 14.8e6 / (10 * 2 ** 18)
 
 
 def hbm_peak():
+    """HBM copy bandwidth in GB/s: the measured figure of this pool's B200s
+    (MEASURED_PEAKS.json) when present, else the pool's earlier measured
+    fallback of 6650 GB/s."""
+    return hbm_peak_source()[0]
+
+
+def hbm_peak_source():
     try:
-        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+        return (float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]),
+                "MEASURED_PEAKS.json hbm_gbs (measured)")
     except Exception:
-        return 6650.0   # fallback figure for this pool
+        return 6650.0, "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"
 
 
 def main():
@@ -753,6 +782,10 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, d)
+        elif args.arx_variants:
+            import pcg_b200 as L
+            if d.rank == 0:
+                print(json.dumps({"arx_variants": run_arx_variants(L)}), flush=True)
         elif args.polymul_only:
             import pcg_b200 as L
             if d.rank == 0:

@@ -94,6 +94,12 @@ int pcgb_arx_peak(double* gops, float* ms);
  * (4096 iterations take about 9 ms on B200); gops[r] = G int-ops/s of launch
  * r, so the caller can report the probe's spread. */
 int pcgb_arx_peak_samples(int reps, int iters, double* gops);
+/* Pipe-balance variants of the probe: the quarter-round adds selected by
+ * add_mask (bit 4q + k = add k of quarter round q of a double round) are
+ * issued as multiply-adds, moving them from the integer ALU to the FMA pipe.
+ * Masks with an instance: 0, 0x10101010, 0x11111111, 0x22222222,
+ * 0x33333333, 0x55555555, 0x15151515, 0x77777777, 0xFFFFFFFF. */
+int pcgb_arx_peak_variant(uint32_t add_mask, int reps, int iters, double* gops);
 /* CUDA events on the library's streams (device-side timing). */
 int pcgb_event_create(void** ev);
 int pcgb_event_destroy(void* ev);

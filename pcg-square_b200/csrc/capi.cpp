@@ -70,6 +70,7 @@ void server_destroy(pcgb_server* s, int timeout_ms);
 void server_stats(pcgb_server* s, int* pending, int* in_flight, size_t* bytes, int* plans);
 double arx_probe(float* ms_out);
 void arx_probe_samples(int reps, int iters, double* gops);
+bool arx_probe_variant(uint32_t mask, int reps, int iters, double* gops);
 
 namespace {
 thread_local std::string g_last_error;
@@ -296,6 +297,15 @@ int pcgb_arx_peak_samples(int reps, int iters, double* gops) {
         if (reps < 1 || iters < 1 || !gops)
             pcgb::fail(PCGB_EINVAL, "arx_peak_samples: reps and iters must be positive");
         pcgb::arx_probe_samples(reps, iters, gops);
+    });
+}
+
+int pcgb_arx_peak_variant(uint32_t add_mask, int reps, int iters, double* gops) {
+    return guarded([&] {
+        if (reps < 1 || iters < 1 || !gops)
+            pcgb::fail(PCGB_EINVAL, "arx_peak_variant: reps and iters must be positive");
+        if (!pcgb::arx_probe_variant(add_mask, reps, iters, gops))
+            pcgb::fail(PCGB_EINVAL, "arx_peak_variant: no probe instance for this add mask");
     });
 }
 

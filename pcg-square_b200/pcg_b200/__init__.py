@@ -146,6 +146,7 @@ def _load():
         "pcgb_launch_count": ([], C.c_ulonglong),
         "pcgb_arx_peak": ([C.POINTER(C.c_double), C.POINTER(C.c_float)], C.c_int),
         "pcgb_arx_peak_samples": ([C.c_int, C.c_int, C.POINTER(C.c_double)], C.c_int),
+        "pcgb_arx_peak_variant": ([C.c_uint32, C.c_int, C.c_int, C.POINTER(C.c_double)], C.c_int),
         "pcgb_event_create": ([C.POINTER(_vp)], C.c_int),
         "pcgb_event_destroy": ([_vp], C.c_int),
         "pcgb_event_record": ([_vp, _vp], C.c_int),
@@ -310,6 +311,14 @@ def arx_peak_samples(reps=15, iters=16384):
     """G int-ops/s of each of `reps` launches of the ARX probe."""
     out = (C.c_double * reps)()
     _check(lib.pcgb_arx_peak_samples(reps, iters, out))
+    return list(out)
+
+
+def arx_peak_variant(add_mask, reps=7, iters=16384):
+    """G int-ops/s of `reps` launches of the probe with the quarter-round
+    adds of add_mask issued on the FMA pipe (pcgb_arx_peak_variant)."""
+    out = (C.c_double * reps)()
+    _check(lib.pcgb_arx_peak_variant(add_mask, reps, iters, out))
     return list(out)
 
 

@@ -127,20 +127,35 @@ def device_words(ptr, nwords):
 
 
 class DeviceChannel(Channel):
-    """Exchange for parties on separate GPUs: torch.distributed over NCCL,
-    the messages sent from and received into device memory (the CW shares
-    and Beaver openings never visit the host).  Needs one GPU per party;
-    this pool runs one GPU per job, so it is not exercised on a GPU pair
-    here (the library side is, through a one-GPU loopback)."""
+    """Exchange that keeps the messages in device memory: gen_and_expand
+    hands it the per-level CW shares and the Beaver openings as device
+    pointers (pcgb_dpf_batch_full_eval_convert_device_dx), so they never
+    visit the host.  Over NCCL (one GPU per party) the words go device to
+    device.  Backends without device send/recv (gloo) stage each message
+    through host memory (`stage`, default: on unless the backend is NCCL);
+    that is how two processes sharing one GPU run this same code path.
+    `exchange` (host arrays in and out) serves the callers that work on
+    host arrays, the GMW circuits of `preprocess`."""
+
+    def __init__(self, party, peer_rank=None, stage=None):
+        super().__init__(party, peer_rank)
+        self.stage = (self.dist.get_backend() != "nccl") if stage is None else stage
 
     def exchange_device(self, d_my, d_peer, nwords):
         my, peer = device_words(d_my, nwords), device_words(d_peer, nwords)
-        if self.party == 0:
-            self.dist.send(my, self.peer)
-            self.dist.recv(peer, self.peer)
+        if self.stage:
+            self.torch.cuda.current_stream().synchronize()
+            t_my, t_peer = my.cpu(), self.torch.empty(nwords, dtype=self.torch.int64)
         else:
-            self.dist.recv(peer, self.peer)
-            self.dist.send(my, self.peer)
+            t_my, t_peer = my, peer
+        if self.party == 0:
+            self.dist.send(t_my, self.peer)
+            self.dist.recv(t_peer, self.peer)
+        else:
+            self.dist.recv(t_peer, self.peer)
+            self.dist.send(t_my, self.peer)
+        if self.stage:
+            peer.copy_(t_peer)
         self.torch.cuda.current_stream().synchronize()
         self.messages += 1
         self.bytes += 8 * nwords

@@ -64,7 +64,7 @@ def dealer(N, c, t, seed):
                 rs=rs_, a=O.public_a(s, 7))
 
 
-def _party(party, port, N, c, t, mat, q, batched):
+def _party(party, port, N, c, t, mat, q, batched, device_channel=False):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     import datetime
     import torch.distributed as dist
@@ -78,7 +78,10 @@ def _party(party, port, N, c, t, mat, q, batched):
             roots=mat["roots"][party], dltsft=mat["dlt"][party], beta=mat["beta"][party],
             r=mat["r"][party], s=mat["s"][party], rs=mat["rs"][party],
             pos=mat["noise"][party][0], val=mat["noise"][party][1])
-        chan = twoparty.Channel(party)
+        # DeviceChannel: messages stay in device memory up to the transport
+        # (gloo here, staged through the host; NCCL moves them device to
+        # device when each party has its own GPU).
+        chan = twoparty.DeviceChannel(party) if device_channel else twoparty.Channel(party)
         d_x, d_z = twoparty.gen_and_expand(party, chan, e, m, batched=batched)
         L.synchronize()
         q.put((party, d_x.download(np.uint64, N), d_z.download(np.uint64, N), chan.messages))
@@ -88,14 +91,16 @@ def _party(party, port, N, c, t, mat, q, batched):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("N,c,t,batched", [(1 << 12, 2, 4, False), (1 << 12, 2, 4, True),
-                                           (1 << 13, 2, 8, True)])
-def test_two_processes_match_the_fused_expansion(pcg, N, c, t, batched):
+@pytest.mark.parametrize("N,c,t,batched,device_channel",
+                         [(1 << 12, 2, 4, False, False), (1 << 12, 2, 4, True, False),
+                          (1 << 13, 2, 8, True, False), (1 << 13, 2, 8, True, True),
+                          (1 << 12, 2, 4, False, True)])
+def test_two_processes_match_the_fused_expansion(pcg, N, c, t, batched, device_channel):
     mat = dealer(N, c, t, 5150 + N)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_party, args=(p, port, N, c, t, mat, q, batched))
+    procs = [ctx.Process(target=_party, args=(p, port, N, c, t, mat, q, batched, device_channel))
              for p in (0, 1)]
     for p in procs:
         p.start()
