@@ -29,6 +29,11 @@ void keyed_leaf_multi_chacha(int w, int sl, const LeafJob* d_jobs, int njobs, un
     leaf_multi_for_prg<kPrgChaCha>(w, sl, d_jobs, njobs, ctas, tpb, smem, te, rk, st);
 }
 
+void deal_multi_chacha_launch(int w, const DealJob* d_jobs, int njobs, unsigned ctas, uint64_t r2,
+                              cudaStream_t st) {
+    deal_multi_for_chacha(w, d_jobs, njobs, ctas, r2, st);
+}
+
 size_t keyed_aes_smem_bytes_chacha() { return sizeof(AesSmem); }
 
 }  // namespace pcgb

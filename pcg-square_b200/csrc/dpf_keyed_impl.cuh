@@ -416,17 +416,13 @@ void tops_dispatch(int K, int levels, const Blk* roots, const Blk* cws, const ui
     }
 }
 
+// Key `id` of an expansion's dealer (below): roots of both parties, the
+// per-level CWs and the output CW.
 template <int W, int PRG>
-__global__ void deal_kernel(uint64_t seed, int c, int t, int n, uint64_t bin, Blk* roots0,
-                            Blk* roots1, Blk* cws, uint64_t* cw_out, const uint32_t* aes_te,
-                            const uint32_t* aes_rk, uint64_t r2) {
+__device__ __forceinline__ void deal_one(int id, uint64_t seed, int c, int t, int n, uint64_t bin,
+                                         Blk* roots0, Blk* roots1, Blk* cws, uint64_t* cw_out,
+                                         const AesSmem* aes_s, uint64_t r2) {
     constexpr int M = 1 << W, NK = M - 1;
-    extern __shared__ __align__(16) uint64_t deal_dsm[];
-    AesSmem& aes_s = *reinterpret_cast<AesSmem*>(deal_dsm);
-    if constexpr (PRG == kPrgAes) load_aes_smem(aes_s, aes_te, aes_rk, NK);
-    const int K = c * c * t * t;
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= K) return;
     const int blk = id / (t * t), rr = id % (t * t);
     const int ii = blk / c, jj = blk % c, kk = rr / t, ll = rr % t;
     const uint64_t alpha = synth_offset(seed, 0, static_cast<uint64_t>(ii) * t + kk, bin) +
@@ -444,8 +440,8 @@ __global__ void deal_kernel(uint64_t seed, int c, int t, int n, uint64_t bin, Bl
     for (int i = 0; i < levels; ++i) {
         const int digit = static_cast<int>((alpha >> (n - W * (i + 1))) & NK);
         Blk h0[NK], h1[NK];
-        hash_raw<W, PRG>(p0, &aes_s, h0);
-        hash_raw<W, PRG>(p1, &aes_s, h1);
+        hash_raw<W, PRG>(p0, aes_s, h0);
+        hash_raw<W, PRG>(p1, aes_s, h1);
         Blk cwf{0, 0}, cwd{0, 0};
         Blk x0{p0.lo, p0.hi}, x1{p1.lo, p1.hi};
         Blk n0{0, 0}, n1{0, 0};
@@ -472,6 +468,33 @@ __global__ void deal_kernel(uint64_t seed, int c, int t, int n, uint64_t bin, Bl
     const uint64_t Bv = add_p(sub_p(C1, C0), beta);
     const int A = static_cast<int>(p0.lo & 1) - static_cast<int>(p1.lo & 1);
     cw_out[id] = A == 1 ? Bv : (A == -1 ? neg_p(Bv) : 0);
+}
+
+template <int W, int PRG>
+__global__ void deal_kernel(uint64_t seed, int c, int t, int n, uint64_t bin, Blk* roots0,
+                            Blk* roots1, Blk* cws, uint64_t* cw_out, const uint32_t* aes_te,
+                            const uint32_t* aes_rk, uint64_t r2) {
+    constexpr int NK = (1 << W) - 1;
+    extern __shared__ __align__(16) uint64_t deal_dsm[];
+    AesSmem& aes_s = *reinterpret_cast<AesSmem*>(deal_dsm);
+    if constexpr (PRG == kPrgAes) load_aes_smem(aes_s, aes_te, aes_rk, NK);
+    const int K = c * c * t * t;
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= K) return;
+    deal_one<W, PRG>(id, seed, c, t, n, bin, roots0, roots1, cws, cw_out, &aes_s, r2);
+}
+
+// The dealer of several expansions (ChaCha8, one w) in one launch: CTA b
+// deals keys of the job whose CTA range holds b.
+template <int W>
+__global__ void deal_multi_kernel(const DealJob* __restrict__ jobs, int njobs, uint64_t r2) {
+    int k = 0;
+    while (k + 1 < njobs && jobs[k + 1].first <= blockIdx.x) ++k;
+    const DealJob& J = jobs[k];
+    const int id = static_cast<int>((blockIdx.x - J.first) * blockDim.x + threadIdx.x);
+    if (id >= J.c * J.c * J.t * J.t) return;
+    deal_one<W, kPrgChaCha>(id, J.seed, J.c, J.t, J.n, J.bin, J.roots0, J.roots1, J.cws,
+                            J.cw_out, nullptr, r2);
 }
 
 
@@ -571,6 +594,18 @@ void leaf_for_prg(int w, int sl, const LeafLaunch& L) {
         case 4 * 8 + 1: leaf_one<4, 1, PRG>(L); break;
         default: fail(PCGB_EINVAL, "unsupported (w, sl) for the leaf kernel");
     }
+}
+
+inline void deal_multi_for_chacha(int w, const DealJob* d_jobs, int njobs, unsigned ctas, uint64_t r2,
+                           cudaStream_t st) {
+    switch (w) {
+        case 1: deal_multi_kernel<1><<<ctas, 128, 0, st>>>(d_jobs, njobs, r2); break;
+        case 2: deal_multi_kernel<2><<<ctas, 128, 0, st>>>(d_jobs, njobs, r2); break;
+        case 3: deal_multi_kernel<3><<<ctas, 128, 0, st>>>(d_jobs, njobs, r2); break;
+        case 4: deal_multi_kernel<4><<<ctas, 128, 0, st>>>(d_jobs, njobs, r2); break;
+        default: fail(PCGB_EINVAL, "w must be in [1,4]");
+    }
+    PCGB_POST_LAUNCH();
 }
 
 template <int PRG>

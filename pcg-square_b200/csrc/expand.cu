@@ -158,6 +158,22 @@ __global__ void noise_kernel(uint64_t seed, int party, int ct, uint64_t bin, int
     val[i] = synth_value(seed, party, i);
 }
 
+// Noise of several requests in one launch, one CTA each.
+struct NoiseJob {
+    uint64_t seed;
+    uint64_t bin;
+    uint64_t* pos;
+    uint64_t* val;
+    int party, ct, t;
+};
+__global__ void noise_multi_kernel(const NoiseJob* __restrict__ jobs) {
+    const NoiseJob J = jobs[blockIdx.x];
+    for (int i = threadIdx.x; i < J.ct; i += blockDim.x) {
+        J.pos[i] = static_cast<uint64_t>(i % J.t) * J.bin + synth_offset(J.seed, J.party, i, J.bin);
+        J.val[i] = synth_value(J.seed, J.party, i);
+    }
+}
+
 // Order-independent 64-bit fingerprint of a word vector: sum (mod 2^64) of
 // mix(v[i] ^ i*phi).  Used to compare outputs across runs without moving
 // them to the host.
@@ -459,6 +475,41 @@ void expand_batch_ws(int count, pcgb_expander* const* e, const Workspace* ws, co
         lg[i] = ilog2(e[i]->N);
     }
     ntt_mac_inverse_multi(count, g.data(), img.data(), Q.data(), zz.data(), lg.data(), st);
+    PCGB_CK(cudaFreeAsync(tab, st));
+}
+
+// Keys and noise of several requests (ChaCha8 expanders of one w), one
+// dealer launch and one noise launch for all: request i gets
+// deal_keys_device(e[i], seed[i], ...) and noise_device(..., party[i], ...).
+void deal_noise_multi_device(int count, pcgb_expander* const* e, const uint64_t* seed,
+                             const int* party, Blk* const* r0, Blk* const* r1, Blk* const* cws,
+                             uint64_t* const* cwo, uint64_t* const* pos, uint64_t* const* val,
+                             cudaStream_t st) {
+    if (count <= 0) return;
+    const int w = e[0]->w;
+    std::vector<DealJob> deal(count);
+    std::vector<NoiseJob> noise(count);
+    unsigned ctas = 0;
+    for (int i = 0; i < count; ++i) {
+        const pcgb_expander* E = e[i];
+        if (E->prg != PCGB_PRG_CHACHA8 || E->w != w)
+            fail(PCGB_EINVAL, "deal batch: ChaCha8 expanders of one w only");
+        const uint64_t bin = static_cast<uint64_t>(E->N / E->t);
+        deal[i] = DealJob{seed[i], r0[i], r1[i], cws[i], cwo[i], bin, E->c, E->t, E->n, ctas};
+        ctas += static_cast<unsigned>((E->K + 127) / 128);
+        noise[i] = NoiseJob{seed[i], bin, pos[i], val[i], party[i], E->c * E->t, E->t};
+    }
+    const size_t b_deal = sizeof(DealJob) * count;
+    const size_t o_noise = (b_deal + 255) & ~size_t{255};
+    const size_t total = o_noise + sizeof(NoiseJob) * count;
+    std::vector<char> host(total);
+    std::memcpy(host.data(), deal.data(), b_deal);
+    std::memcpy(host.data() + o_noise, noise.data(), sizeof(NoiseJob) * count);
+    char* tab = static_cast<char*>(pool_alloc(total, st));
+    PCGB_CK(cudaMemcpyAsync(tab, host.data(), total, cudaMemcpyHostToDevice, st));
+    deal_multi_chacha_launch(w, reinterpret_cast<const DealJob*>(tab), count, ctas, r2_mod_p(), st);
+    noise_multi_kernel<<<count, 128, 0, st>>>(reinterpret_cast<const NoiseJob*>(tab + o_noise));
+    PCGB_POST_LAUNCH();
     PCGB_CK(cudaFreeAsync(tab, st));
 }
 

@@ -361,6 +361,32 @@ __device__ __forceinline__ void row_mac_body(const uint64_t* g, const uint64_t* 
     }
 }
 
+// Pointwise product and inverse row pass on rows [tile*V, tile*V + V) of a
+// transform already in the permuted evaluation order (row_fwd_body's
+// output): out row = Wi (.) INTT( d row (.) img row ), in place.  Each
+// thread loads the permuted positions of its last-phase registers, so the
+// inverse starts where the fused forward would have ended.
+template <int L, int V>
+__device__ __forceinline__ void row_pmul_inv_body(uint64_t* d, const uint64_t* __restrict__ img,
+                                                  size_t tile, const ulonglong2* __restrict__ twi,
+                                                  const uint64_t* __restrict__ Wi, uint64_t* sm) {
+    constexpr int E = Geo<L>::E, T = Geo<L>::T, LP = last_phase(L);
+    const int t = threadIdx.x % T, v = threadIdx.x / T;
+    const size_t base = (tile * V + v) * Geo<L>::n;
+    uint64_t x[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const size_t i = base + perm_pos<L>(eidx<L, LP>(t, e));
+        x[e] = mont_lazy(d[i], __ldg(img + i));
+    }
+    inverse_all<L>(x, t, twi, SmemLay<1>{sm + v * Geo<L>::PAD});
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const size_t i = base + eidx<L, 0>(t, e);
+        d[i] = csub(mont_lazy(x[e], __ldg(Wi + i)), kPm);
+    }
+}
+
 // ---- per-length kernels: grid = (tiles, batch) ---------------------------------
 
 template <int L, bool REDUCE>
@@ -386,6 +412,15 @@ __global__ void __launch_bounds__(row_threads<L>()) row_fwd_kernel(
     extern __shared__ uint64_t sm[];
     row_fwd_body<L, row_V<L>()>(d + (static_cast<size_t>(blockIdx.y) << (L + l1)), blockIdx.x,
                                 tw, sm);
+}
+
+template <int L>
+__global__ void __launch_bounds__(row_threads<L>()) row_pmul_inv_kernel(
+    uint64_t* d, const uint64_t* __restrict__ img, int l1, const ulonglong2* __restrict__ twi,
+    const uint64_t* __restrict__ Wi) {
+    extern __shared__ uint64_t sm[];
+    const size_t off = static_cast<size_t>(blockIdx.y) << (L + l1);
+    row_pmul_inv_body<L, row_V<L>()>(d + off, img + off, blockIdx.x, twi, Wi, sm);
 }
 
 // Instance b reads g and img at b*Q*N and writes out at b*N.
@@ -752,6 +787,16 @@ void row_fwd_l(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
 }
 
 template <int L>
+void row_pmul_inv_l(const NttPlan& pl, uint64_t* d, const uint64_t* img, int batch,
+                    const uint64_t* Wi, cudaStream_t st) {
+    constexpr size_t sm = row_smem<L>();
+    g_optin(row_pmul_inv_kernel<L>, sm);
+    row_pmul_inv_kernel<L><<<dim3(pl.n1 / row_V<L>(), batch), row_threads<L>(), sm, st>>>(
+        d, img, pl.l1, pl.tw2i, Wi);
+    PCGB_POST_LAUNCH();
+}
+
+template <int L>
 void row_mac_l(const NttPlan& pl, const uint64_t* g, const uint64_t* img, int Q, int batch,
                const uint64_t* Wi, uint64_t* out, cudaStream_t st) {
     constexpr size_t sm = row_smem<L>();
@@ -798,6 +843,10 @@ void col_inv(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
 }
 void row_fwd(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
     by_len(pl.l2, [&](auto L) { row_fwd_l<decltype(L)::value>(pl, d, batch, st); });
+}
+void row_pmul_inv(const NttPlan& pl, uint64_t* d, const uint64_t* img, int batch,
+                  const uint64_t* Wi, cudaStream_t st) {
+    by_len(pl.l2, [&](auto L) { row_pmul_inv_l<decltype(L)::value>(pl, d, img, batch, Wi, st); });
 }
 void row_mac(const NttPlan& pl, const uint64_t* g, const uint64_t* img, int Q, int batch,
              const uint64_t* Wi, uint64_t* out, cudaStream_t st) {
@@ -850,12 +899,16 @@ void ntt_forward(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
 void poly_mul_device(const NttPlan& pl, uint64_t* c, const uint64_t* a, const uint64_t* b,
                      int batch, uint64_t* scratch, cudaStream_t st) {
     const uint64_t* wir = wi_times_r(const_cast<NttPlan&>(pl), st);
-    // A = NTT(a) in scratch; c = column pass of b; c = INTT(NTT(c) (.) A).
+    // A = NTT(a) in scratch; c = NTT(b); c = INTT(c (.) A): the forward row
+    // pass of c and the pointwise product + inverse row pass are separate
+    // launches (each needs about 70 registers a thread where the fused
+    // pass needs 96, so more CTAs fit on an SM).
     // a is read before c is first written, so c may alias a or b.
     col_fwd(pl, a, scratch, batch, true, st);
     row_fwd(pl, scratch, batch, st);
     col_fwd(pl, b, c, batch, true, st);
-    row_mac(pl, c, scratch, 1, batch, wir, c, st);
+    row_fwd(pl, c, batch, st);
+    row_pmul_inv(pl, c, scratch, batch, wir, st);
     col_inv(pl, c, batch, st);
 }
 

@@ -173,6 +173,20 @@ struct LeafJob {
     unsigned gx, gy, first;
 };
 
+// One expansion's part of a multi-expansion dealer launch (ChaCha8).
+struct DealJob {
+    uint64_t seed;
+    Blk* roots0;
+    Blk* roots1;
+    Blk* cws;
+    uint64_t* cw_out;
+    uint64_t bin;
+    int c, t, n;
+    unsigned first;   // first CTA (128 threads, one key each)
+};
+void deal_multi_chacha_launch(int w, const DealJob* d_jobs, int njobs, unsigned ctas, uint64_t r2,
+                              cudaStream_t st);
+
 // Per-PRG instantiations (dpf_keyed_chacha.cu / dpf_keyed_aes.cu).
 #define PCGB_KEYED_DECL(NAME)                                                                   \
     void keyed_tops_##NAME(int K, int levels, int w, const Blk* roots, const Blk* cws,          \
@@ -238,6 +252,10 @@ void expand_batch_ws(int count, pcgb_expander* const* e, const Workspace* ws, co
                      const uint64_t* const* cw_out, const uint64_t* const* pos,
                      const uint64_t* const* val, uint64_t* const* x, uint64_t* const* z,
                      cudaStream_t st);
+void deal_noise_multi_device(int count, pcgb_expander* const* e, const uint64_t* seed,
+                             const int* party, Blk* const* r0, Blk* const* r1, Blk* const* cws,
+                             uint64_t* const* cwo, uint64_t* const* pos, uint64_t* const* val,
+                             cudaStream_t st);
 void digest_multi_device(int count, const uint64_t* const* v, const size_t* n, uint64_t* const* out,
                          cudaStream_t st);
 void deal_keys_device(pcgb_expander* e, uint64_t seed, Blk* r0, Blk* r1, Blk* cws, uint64_t* cwo,

@@ -194,7 +194,7 @@ struct ReqMem {
     Workspace ws;
 };
 
-ReqMem carve_request(pcgb_expander* e, const Req* r, cudaStream_t st) {
+ReqMem carve_request(pcgb_expander* e, const Req* r, cudaStream_t st, bool deal) {
     int K = 0, levels = 0, nk = 0;
     size_t wsb = 0;
     expander_info(e, &K, &levels, &nk, &wsb);
@@ -215,9 +215,10 @@ ReqMem carve_request(pcgb_expander* e, const Req* r, cudaStream_t st) {
     m.x = reinterpret_cast<uint64_t*>(take(16 * N));
     m.z = m.x + N;
     m.ws = workspace_carve(e, take(wsb));
-    // Fresh keys (both parties' roots) and this party's noise.
-    deal_keys_device(e, r->r.seed, m.roots, m.roots + K, m.cws, m.cwo, st);
-    noise_device(r->r.N, r->r.c, r->r.t, r->r.seed, r->r.party, m.pos, m.val, st);
+    if (deal) {   // fresh keys (both parties' roots) and this party's noise
+        deal_keys_device(e, r->r.seed, m.roots, m.roots + K, m.cws, m.cwo, st);
+        noise_device(r->r.N, r->r.c, r->r.t, r->r.seed, r->r.party, m.pos, m.val, st);
+    }
     return m;
 }
 
@@ -232,9 +233,25 @@ void launch(pcgb_server* s, const std::vector<Req*>& rs) {
     std::vector<ReqMem> mem(n);
     for (int i = 0; i < n; ++i) {
         es[i] = get_plan(s, rs[i]->r.N, rs[i]->r.c, rs[i]->r.t);
-        mem[i] = carve_request(es[i], rs[i], st);
+        mem[i] = carve_request(es[i], rs[i], st, !batch);
     }
     if (batch) {
+        // Keys and noise of the whole batch: one dealer and one noise launch.
+        std::vector<uint64_t> seed(n);
+        std::vector<int> pty(n);
+        std::vector<Blk*> r0(n), r1(n), kc(n);
+        std::vector<uint64_t*> co(n), ps(n), vl(n);
+        for (int i = 0; i < n; ++i) {
+            int K = 0, levels = 0, nk = 0;
+            size_t wsb = 0;
+            expander_info(es[i], &K, &levels, &nk, &wsb);
+            seed[i] = rs[i]->r.seed;
+            pty[i] = rs[i]->r.party;
+            r0[i] = mem[i].roots; r1[i] = mem[i].roots + K; kc[i] = mem[i].cws;
+            co[i] = mem[i].cwo; ps[i] = mem[i].pos; vl[i] = mem[i].val;
+        }
+        deal_noise_multi_device(n, es.data(), seed.data(), pty.data(), r0.data(), r1.data(),
+                                kc.data(), co.data(), ps.data(), vl.data(), st);
         std::vector<Workspace> ws(n);
         std::vector<int> party(n);
         std::vector<const Blk*> roots(n), cws(n);
