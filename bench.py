@@ -642,6 +642,13 @@ def run_polymul(L, batch=16, logN=20, steps=10, warmup=3, seed=11):
                         "peak": hbm_peak(), "peak_source": hbm_peak_source()[1],
                         "unit": "GB/s", "bytes": nbytes}}
     out["roofline"]["frac"] = out["roofline"]["achieved"] / out["roofline"]["peak"]
+    # Per-pass accounting (8 B read + 8 B written per word in each of the two
+    # passes of the three transforms, pointwise fused): 96 B per element.
+    out["roofline"]["bytes_per_pass_accounting"] = 96 * batch * N
+    out["roofline"]["frac_per_pass_accounting"] = (96 * batch * N / (med * 1e-3) / 1e9 /
+                                                   out["roofline"]["peak"])
+    out["roofline"]["bound_by"] = ("64-bit integer multiplies (FMA-heavy pipe, math-pipe "
+                                   "throttle the top stall; profiles/ntt_polymul_16x2e20.txt)")
 
     # Mixed lengths in one call (five launches for the batch): 6 x 2^20,
     # 5 x 2^18, 5 x 2^16, interleaved, through pcgb_poly_mul_device_multi.
