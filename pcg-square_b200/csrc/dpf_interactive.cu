@@ -16,6 +16,7 @@
 // Leaves come out in the reference layout: instance b, leaf d at [b*D + d].
 #include "pcgb_internal.h"
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -31,21 +32,16 @@ namespace {
 
 constexpr int kTPB = 128;
 
-// The compact four-table AES: these kernels run one short pass per node, so
-// staging the per-lane replicated table (32 KB per CTA) would cost as much
-// as the bank conflicts it removes.
+// The compact four-table AES for the shallow levels: these kernels run one
+// short pass per node, so staging a bank-conflict-free table would cost as
+// much as the conflicts it removes.
 struct AesSm {
     uint32_t te[1024];
     uint32_t rk[15 * 44];
 };
-// The per-lane replicated Te0 (bank-conflict-free, aes128.cuh) for the deep
-// levels, where a CTA walks enough parents to pay for its 32 KB fill.
-struct AesRepSm {
-    uint32_t te_rep[kAesRepWords];
-    uint32_t rk[15 * 44];
-};
-constexpr size_t kRepMinParents = 4096;   // per instance, to use AesRepSm
-constexpr int kRepParentsPerThread = 8;
+// Levels with at least this many parents per instance hash with the
+// PRMT-addressed table instead (expand_level_prmt_kernel).
+constexpr size_t kRepMinParents = 4096;
 
 // H_0..H_{nk-1} of one node.
 template <int W, int PRG>
@@ -133,10 +129,9 @@ __global__ void __launch_bounds__(kTPB) hash_roots_kernel(const Blk* __restrict_
 
 // Expand level i (frontier size sz, hashes H) with CW = my ^ peer; write the
 // children to nxt; when hash_next, hash the children into Hn and reduce
-// their columns into my_next.  grid = (x, B); the CTAs of an instance
-// stride over its sz parents (one each, or several with REP).  REP (AES
-// only): hash with the replicated table staged once per CTA.
-template <int W, int PRG, bool REP>
+// their columns into my_next.  grid = (x, B); thread x*kTPB + t of an
+// instance expands its parent x*kTPB + t.
+template <int W, int PRG>
 __global__ void __launch_bounds__(kTPB) expand_level_kernel(
     const Blk* __restrict__ cur, const Blk* __restrict__ H, const Blk* __restrict__ my,
     const Blk* __restrict__ peer, Blk* __restrict__ nxt, Blk* __restrict__ Hn,
@@ -145,18 +140,8 @@ __global__ void __launch_bounds__(kTPB) expand_level_kernel(
     constexpr int M = 1 << W, NK = M - 1;
     extern __shared__ __align__(16) unsigned char smraw[];
     Blk* red = reinterpret_cast<Blk*>(smraw);
-    const AesSm* a = nullptr;
-    const AesRepSm* arep = nullptr;
-    if constexpr (REP) {
-        AesRepSm& rs = *reinterpret_cast<AesRepSm*>(smraw + 32 * NK * sizeof(Blk));
-        aes_fill_rep(rs.te_rep, te);
-        for (int i = threadIdx.x; i < NK * 44; i += blockDim.x) rs.rk[i] = rk[i];
-        __syncthreads();
-        arep = &rs;
-    } else {
-        AesSm& aes = *reinterpret_cast<AesSm*>(smraw + 32 * NK * sizeof(Blk));
-        a = stage_aes<PRG>(aes, te, rk, NK);
-    }
+    AesSm& aes = *reinterpret_cast<AesSm*>(smraw + 32 * NK * sizeof(Blk));
+    const AesSm* a = stage_aes<PRG>(aes, te, rk, NK);
     const int b = blockIdx.y;
     Blk cw[NK];
     Blk cwf{0, 0};
@@ -189,14 +174,7 @@ __global__ void __launch_bounds__(kTPB) expand_level_kernel(
         if (hash_next) {
             auto hash_child = [&](int k) {
                 Blk h[NK];
-                if constexpr (REP) {
-#pragma unroll 1
-                    for (int q = 0; q < NK; ++q)
-                        aes_ccr_rep(arep->te_rep, arep->rk + 44 * q, kids[k].lo, kids[k].hi,
-                                    h[q].lo, h[q].hi);
-                } else {
-                    hash_node<W, PRG>(kids[k], a, h);
-                }
+                hash_node<W, PRG>(kids[k], a, h);
                 Blk* hd = Hn + static_cast<size_t>(b) * HS + (j * M + k) * NK;
 #pragma unroll
                 for (int kk = 0; kk < NK; ++kk) {
@@ -219,12 +197,80 @@ __global__ void __launch_bounds__(kTPB) expand_level_kernel(
         }
     };
     const size_t j0 = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if constexpr (REP) {
-        for (size_t j = j0; j < sz; j += static_cast<size_t>(gridDim.x) * blockDim.x) parent(j);
-    } else if (j0 < sz) {
-        parent(j0);
-    }
+    if (j0 < sz) parent(j0);
     if (hash_next) cta_xor_reduce<NK>(acc, my_next + static_cast<size_t>(b) * NK, red);
+}
+
+// AES levels of kRepMinParents or more parents per instance with the
+// PRMT-addressed table (aes128.cuh): one 768-thread CTA per SM, filled
+// once, walking (instance, chunk) tiles of kPrmtChunk parents; per tile the
+// same work as expand_level_kernel, then the CTA's XOR reduction into the
+// instance's my_next.
+constexpr int kPrmtTPB = 768;   // no register spills (at most 80 a thread)
+constexpr size_t kPrmtChunk = 4096;
+
+template <int W>
+__global__ void __launch_bounds__(kPrmtTPB) expand_level_prmt_kernel(
+    const Blk* __restrict__ cur, const Blk* __restrict__ H, const Blk* __restrict__ my,
+    const Blk* __restrict__ peer, Blk* __restrict__ nxt, Blk* __restrict__ Hn,
+    Blk* __restrict__ my_next, size_t sz, size_t D, size_t HS, int hash_next, int B,
+    const uint32_t* te, const uint32_t* rk) {
+    constexpr int M = 1 << W, NK = M - 1;
+    extern __shared__ __align__(16) unsigned char prmt_dsm[];
+    __shared__ AesPrmtKeys keys;
+    __shared__ Blk red[32 * NK];
+    const AesPrmt A = aes_prmt_setup<NK>(prmt_dsm, keys, te, rk);
+    const size_t chunks = (sz + kPrmtChunk - 1) / kPrmtChunk;
+    const size_t tiles = static_cast<size_t>(B) * chunks;
+    for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const size_t b = tile / chunks, x = tile % chunks;
+        Blk cw[NK];
+        Blk cwf{0, 0};
+#pragma unroll
+        for (int k = 0; k < NK; ++k) {
+            const Blk m0 = my[b * NK + k], p0 = peer[b * NK + k];
+            cw[k] = Blk{m0.lo ^ p0.lo, m0.hi ^ p0.hi};
+            cwf.lo ^= cw[k].lo;
+            cwf.hi ^= cw[k].hi;
+        }
+        Blk acc[NK];
+#pragma unroll
+        for (int k = 0; k < NK; ++k) acc[k] = Blk{0, 0};
+        const size_t j1 = (x + 1) * kPrmtChunk < sz ? (x + 1) * kPrmtChunk : sz;
+        for (size_t j = x * kPrmtChunk + threadIdx.x; j < j1; j += blockDim.x) {
+            const Blk p = cur[b * D + j];
+            const bool t = (p.lo & 1) != 0;
+            Blk kids[M];
+            uint64_t xl = 0, xh = 0;
+#pragma unroll
+            for (int k = 0; k < NK; ++k) {
+                const Blk h = H[b * HS + j * NK + k];
+                xl ^= h.lo;
+                xh ^= h.hi;
+                kids[k] = Blk{h.lo ^ (t ? cw[k].lo : 0), h.hi ^ (t ? cw[k].hi : 0)};
+            }
+            kids[NK] = Blk{xl ^ p.lo ^ (t ? cwf.lo : 0), xh ^ p.hi ^ (t ? cwf.hi : 0)};
+            Blk* dst = nxt + b * D + j * M;
+#pragma unroll
+            for (int k = 0; k < M; ++k) dst[k] = kids[k];
+            if (hash_next) {
+#pragma unroll 1
+                for (int k = 0; k < M; ++k) {
+                    Blk* hd = Hn + b * HS + (j * M + k) * NK;
+#pragma unroll 1
+                    for (int q = 0; q < NK; ++q) {
+                        Blk h;
+                        aes_ccr_prmt(A, q, kids[k].lo, kids[k].hi, h.lo, h.hi);
+                        hd[q] = h;
+                        acc[q].lo ^= h.lo;
+                        acc[q].hi ^= h.hi;
+                    }
+                }
+            }
+        }
+        if (hash_next) cta_xor_reduce<NK>(acc, my_next + b * NK, red);
+        __syncthreads();   // red is reused by the next tile
+    }
 }
 
 // Last level fused with the output layer's first pass (the two-party
@@ -410,19 +456,23 @@ Blk* run_levels(Pool& pl, int B, int n, const Blk* roots, const Blk* dltsft,
             return nullptr;
         }
         const bool rep = PRG == PCGB_PRG_AES && sz >= kRepMinParents;
-        const size_t per_cta = static_cast<size_t>(kTPB) * (rep ? kRepParentsPerThread : 1);
-        const dim3 grid(static_cast<unsigned>((sz + per_cta - 1) / per_cta), static_cast<unsigned>(B));
+        const dim3 grid(static_cast<unsigned>((sz + kTPB - 1) / kTPB), static_cast<unsigned>(B));
         if constexpr (PRG == PCGB_PRG_AES) {
             if (rep) {
-                const size_t smem_rep = 32 * NK * sizeof(Blk) + sizeof(AesRepSm);
-                expand_level_kernel<W, PRG, true><<<grid, kTPB, smem_rep, st>>>(
-                    cur, H, my, pl.peer, nxt, Hn, myn, sz, D, HS, hash_next, te, pl.rk);
+                PCGB_CK(cudaFuncSetAttribute(expand_level_prmt_kernel<W>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(kAesPrmtSmemBytes)));
+                const size_t tiles = static_cast<size_t>(B) * ((sz + kPrmtChunk - 1) / kPrmtChunk);
+                const unsigned pgrid = static_cast<unsigned>(
+                    std::min<size_t>(tiles, static_cast<size_t>(sm_count())));
+                expand_level_prmt_kernel<W><<<pgrid, kPrmtTPB, kAesPrmtSmemBytes, st>>>(
+                    cur, H, my, pl.peer, nxt, Hn, myn, sz, D, HS, hash_next, B, te, pl.rk);
             } else {
-                expand_level_kernel<W, PRG, false><<<grid, kTPB, smem, st>>>(
+                expand_level_kernel<W, PRG><<<grid, kTPB, smem, st>>>(
                     cur, H, my, pl.peer, nxt, Hn, myn, sz, D, HS, hash_next, te, pl.rk);
             }
         } else {
-            expand_level_kernel<W, PRG, false><<<grid, kTPB, smem, st>>>(
+            expand_level_kernel<W, PRG><<<grid, kTPB, smem, st>>>(
                 cur, H, my, pl.peer, nxt, Hn, myn, sz, D, HS, hash_next, te, pl.rk);
         }
         PCGB_POST_LAUNCH();

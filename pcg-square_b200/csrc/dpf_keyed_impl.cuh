@@ -65,10 +65,21 @@ __device__ __forceinline__ void stblk(Blk* p, const Blk& b) {
     *reinterpret_cast<ulonglong2*>(p) = make_ulonglong2(b.lo, b.hi);
 }
 
+// AES CCR hash H_k of one node, with the replicated table (AesSmem) or the
+// PRMT-addressed one (AesPrmt).
+__device__ __forceinline__ void aes_node(const AesSmem* a, int k, uint64_t lo, uint64_t hi,
+                                         uint64_t& olo, uint64_t& ohi) {
+    aes_ccr_rep(a->te_rep, a->rk + 44 * k, lo, hi, olo, ohi);
+}
+__device__ __forceinline__ void aes_node(const AesPrmt* a, int k, uint64_t lo, uint64_t hi,
+                                         uint64_t& olo, uint64_t& ohi) {
+    aes_ccr_prmt(*a, k, lo, hi, olo, ohi);
+}
+
 // m children of `p` under the level CWs cw[0..nk) (global, broadcast).
-template <int W, int PRG>
+template <int W, int PRG, class A>
 __device__ __forceinline__ void children(const Blk& p, const Blk* __restrict__ cw,
-                                         const AesSmem* aes, Blk (&kids)[1 << W]) {
+                                         const A* aes, Blk (&kids)[1 << W]) {
     constexpr int M = 1 << W, NK = M - 1;
     const bool t = (p.lo & 1) != 0;
     uint64_t hxl = 0, hxh = 0, cfl = 0, cfh = 0;
@@ -94,7 +105,7 @@ __device__ __forceinline__ void children(const Blk& p, const Blk* __restrict__ c
 #pragma unroll 1
         for (int k = 0; k < NK; ++k) {
             uint64_t hl, hh;
-            aes_ccr_rep(aes->te_rep, aes->rk + 44 * k, p.lo, p.hi, hl, hh);
+            aes_node(aes, k, p.lo, p.hi, hl, hh);
             const Blk cv = ldblk(cw + k);
             cfl ^= cv.lo; cfh ^= cv.hi;
             hxl ^= hl; hxh ^= hh;
@@ -105,8 +116,8 @@ __device__ __forceinline__ void children(const Blk& p, const Blk* __restrict__ c
 }
 
 // Raw tree hashes H_0..H_{nk-1} of one node (no correction words).
-template <int W, int PRG>
-__device__ __forceinline__ void hash_raw(const Blk& p, const AesSmem* aes, Blk (&h)[(1 << W) - 1]) {
+template <int W, int PRG, class A>
+__device__ __forceinline__ void hash_raw(const Blk& p, const A* aes, Blk (&h)[(1 << W) - 1]) {
     constexpr int NK = (1 << W) - 1;
     if constexpr (PRG == kPrgChaCha) {
 #pragma unroll
@@ -123,21 +134,19 @@ __device__ __forceinline__ void hash_raw(const Blk& p, const AesSmem* aes, Blk (
         }
     } else {
 #pragma unroll 1
-        for (int k = 0; k < NK; ++k)
-            aes_ccr_rep(aes->te_rep, aes->rk + 44 * k, p.lo, p.hi, h[k].lo, h[k].hi);
+        for (int k = 0; k < NK; ++k) aes_node(aes, k, p.lo, p.hi, h[k].lo, h[k].hi);
     }
 }
 
 // ---------------------------------------------------------------------------
 // expand_tops: depth-first expansion of `nlev` levels below each source node.
 // Thread `id` (< K * m^src_lvl) expands source node id: key id / m^src_lvl.
-template <int W, int PRG>
+template <int W, int PRG, class A>
 __device__ __forceinline__ void tops_walk(const Blk* __restrict__ src, size_t id, int src_lvl,
                                           int nlev, int levels, const Blk* __restrict__ cws,
-                                          const AesSmem* aes, Blk* __restrict__ dst) {
+                                          const A* aes, Blk* __restrict__ dst) {
     constexpr int M = 1 << W, NK = M - 1;
     constexpr int MAXD = tops_max_depth<W>();
-    const AesSmem& aes_s = *aes;
     const size_t per_key_src = static_cast<size_t>(1) << (W * src_lvl);
     const size_t key = id / per_key_src;
     const size_t j = id % per_key_src;
@@ -150,7 +159,7 @@ __device__ __forceinline__ void tops_walk(const Blk* __restrict__ src, size_t id
     // stack[d][k]: children at relative depth d+1; pos[d]: next child index.
     Blk stack[MAXD][M];
     int pos[MAXD];
-    children<W, PRG>(root, kcw + static_cast<size_t>(src_lvl) * NK, &aes_s, stack[0]);
+    children<W, PRG>(root, kcw + static_cast<size_t>(src_lvl) * NK, aes, stack[0]);
     pos[0] = 0;
     int d = 0;
     size_t emitted = 0;
@@ -169,8 +178,8 @@ __device__ __forceinline__ void tops_walk(const Blk* __restrict__ src, size_t id
             continue;
         }
         Blk kids[M];
-        children<W, PRG>(stack[d][pos[d]], kcw + static_cast<size_t>(src_lvl + d + 1) * NK,
-                         &aes_s, kids);
+        children<W, PRG>(stack[d][pos[d]], kcw + static_cast<size_t>(src_lvl + d + 1) * NK, aes,
+                         kids);
 #pragma unroll
         for (int k = 0; k < M; ++k) stack[d + 1][k] = kids[k];
         ++d;
@@ -211,6 +220,52 @@ __global__ void __launch_bounds__(128) expand_tops_multi_kernel(
         const TopsJob J = jobs[j];
         tops_walk<W, PRG>(J.src, g - J.first, J.src_lvl, J.nlev, J.levels, J.cws, &aes_s, J.dst);
     }
+}
+
+// AES top-level walks with the PRMT-addressed tables (aes128.cuh): the 64 KB
+// table region takes most of an SM's shared memory, so these run one
+// 1024-thread CTA per SM, each thread walking source nodes grid-stride (the
+// table is filled once per CTA, not once per 128 threads).
+constexpr int kAesPrmtThreads = 1024;
+
+template <int W>
+__global__ void __launch_bounds__(kAesPrmtThreads) expand_tops_prmt_kernel(
+    const Blk* __restrict__ src, int K, int src_lvl, int nlev, int levels,
+    const Blk* __restrict__ cws, const uint32_t* __restrict__ aes_te,
+    const uint32_t* __restrict__ aes_rk, Blk* __restrict__ dst) {
+    constexpr int NK = (1 << W) - 1;
+    extern __shared__ __align__(16) unsigned char prmt_dsm[];
+    __shared__ AesPrmtKeys keys;
+    const AesPrmt A = aes_prmt_setup<NK>(prmt_dsm, keys, aes_te, aes_rk);
+    const size_t total = static_cast<size_t>(K) << (W * src_lvl);
+    for (size_t id = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; id < total;
+         id += static_cast<size_t>(gridDim.x) * blockDim.x)
+        tops_walk<W, kPrgAes>(src, id, src_lvl, nlev, levels, cws, &A, dst);
+}
+
+template <int W>
+__global__ void __launch_bounds__(kAesPrmtThreads) expand_tops_multi_prmt_kernel(
+    const TopsJob* __restrict__ jobs, int njobs, unsigned long long total,
+    const uint32_t* __restrict__ aes_te, const uint32_t* __restrict__ aes_rk) {
+    constexpr int NK = (1 << W) - 1;
+    extern __shared__ __align__(16) unsigned char prmt_dsm[];
+    __shared__ AesPrmtKeys keys;
+    const AesPrmt A = aes_prmt_setup<NK>(prmt_dsm, keys, aes_te, aes_rk);
+    for (unsigned long long g = static_cast<unsigned long long>(blockIdx.x) * blockDim.x +
+                                threadIdx.x;
+         g < total; g += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        int j = 0;
+        while (j + 1 < njobs && jobs[j + 1].first <= g) ++j;
+        const TopsJob J = jobs[j];
+        tops_walk<W, kPrgAes>(J.src, g - J.first, J.src_lvl, J.nlev, J.levels, J.cws, &A, J.dst);
+    }
+}
+
+// Grid of a PRMT kernel over `threads` work items: at most one CTA per SM.
+inline unsigned aes_prmt_grid(unsigned long long threads) {
+    const unsigned long long need = (threads + kAesPrmtThreads - 1) / kAesPrmtThreads;
+    const unsigned long long sms = static_cast<unsigned long long>(sm_count());
+    return static_cast<unsigned>(need < sms ? (need ? need : 1) : sms);
 }
 
 // ---------------------------------------------------------------------------
@@ -394,10 +449,17 @@ void launch_tops(const Blk* src, int K, int src_lvl, int nlev, int levels, const
                  const uint32_t* te, const uint32_t* rk, Blk* dst, cudaStream_t st) {
     if (nlev < 0 || nlev >= tops_max_depth<W>()) fail(PCGB_EINVAL, "keyed expansion deeper than the DFS stack");
     const size_t threads = static_cast<size_t>(K) << (W * src_lvl);
-    const int TPB = 128;
-    const size_t smem = PRG == kPrgAes ? sizeof(AesSmem) : 0;
-    expand_tops_kernel<W, PRG><<<static_cast<unsigned>((threads + TPB - 1) / TPB), TPB, smem, st>>>(
-        src, K, src_lvl, nlev, levels, cws, te, rk, dst);
+    if constexpr (PRG == kPrgAes) {
+        PCGB_CK(cudaFuncSetAttribute(expand_tops_prmt_kernel<W>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kAesPrmtSmemBytes)));
+        expand_tops_prmt_kernel<W><<<aes_prmt_grid(threads), kAesPrmtThreads, kAesPrmtSmemBytes,
+                                     st>>>(src, K, src_lvl, nlev, levels, cws, te, rk, dst);
+    } else {
+        const int TPB = 128;
+        expand_tops_kernel<W, PRG><<<static_cast<unsigned>((threads + TPB - 1) / TPB), TPB, 0,
+                                     st>>>(src, K, src_lvl, nlev, levels, cws, te, rk, dst);
+    }
     PCGB_POST_LAUNCH();
 }
 
@@ -520,13 +582,21 @@ void tops_multi_launch(const std::vector<TopsJob>& jobs, TopsJob* d_jobs,
             fail(PCGB_EINVAL, "keyed expansion deeper than the DFS stack");
     PCGB_CK(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(TopsJob),
                             cudaMemcpyHostToDevice, st));
-    const int TPB = 128;
-    const size_t smem = PRG == kPrgAes ? sizeof(AesSmem) : 0;
-    const unsigned long long blocks = (total + TPB - 1) / TPB;
-    const unsigned long long cap = static_cast<unsigned long long>(sm_count()) * 8;  // persistent
-    expand_tops_multi_kernel<W, PRG><<<static_cast<unsigned>(blocks < cap ? blocks : cap), TPB,
-                                      smem, st>>>(d_jobs, static_cast<int>(jobs.size()), total,
-                                                  te, rk);
+    if constexpr (PRG == kPrgAes) {
+        PCGB_CK(cudaFuncSetAttribute(expand_tops_multi_prmt_kernel<W>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kAesPrmtSmemBytes)));
+        expand_tops_multi_prmt_kernel<W><<<aes_prmt_grid(total), kAesPrmtThreads,
+                                           kAesPrmtSmemBytes, st>>>(
+            d_jobs, static_cast<int>(jobs.size()), total, te, rk);
+    } else {
+        const int TPB = 128;
+        const unsigned long long blocks = (total + TPB - 1) / TPB;
+        const unsigned long long cap = static_cast<unsigned long long>(sm_count()) * 8;
+        expand_tops_multi_kernel<W, PRG><<<static_cast<unsigned>(blocks < cap ? blocks : cap),
+                                           TPB, 0, st>>>(d_jobs, static_cast<int>(jobs.size()),
+                                                         total, te, rk);
+    }
     PCGB_POST_LAUNCH();
 }
 
