@@ -254,16 +254,27 @@ __global__ void __launch_bounds__(kPrmtTPB) expand_level_prmt_kernel(
 #pragma unroll
             for (int k = 0; k < M; ++k) dst[k] = kids[k];
             if (hash_next) {
+                if constexpr (W == 1) {
+                    // Both children's hashes in flight at once.
+                    Blk h0, h1;
+                    aes_ccr_prmt(A, 0, kids[0].lo, kids[0].hi, h0.lo, h0.hi);
+                    aes_ccr_prmt(A, 0, kids[1].lo, kids[1].hi, h1.lo, h1.hi);
+                    Hn[b * HS + j * 2] = h0;
+                    Hn[b * HS + j * 2 + 1] = h1;
+                    acc[0].lo ^= h0.lo ^ h1.lo;
+                    acc[0].hi ^= h0.hi ^ h1.hi;
+                } else {
 #pragma unroll 1
-                for (int k = 0; k < M; ++k) {
-                    Blk* hd = Hn + b * HS + (j * M + k) * NK;
+                    for (int k = 0; k < M; ++k) {
+                        Blk* hd = Hn + b * HS + (j * M + k) * NK;
 #pragma unroll 1
-                    for (int q = 0; q < NK; ++q) {
-                        Blk h;
-                        aes_ccr_prmt(A, q, kids[k].lo, kids[k].hi, h.lo, h.hi);
-                        hd[q] = h;
-                        acc[q].lo ^= h.lo;
-                        acc[q].hi ^= h.hi;
+                        for (int q = 0; q < NK; ++q) {
+                            Blk h;
+                            aes_ccr_prmt(A, q, kids[k].lo, kids[k].hi, h.lo, h.hi);
+                            hd[q] = h;
+                            acc[q].lo ^= h.lo;
+                            acc[q].hi ^= h.hi;
+                        }
                     }
                 }
             }
@@ -455,7 +466,8 @@ Blk* run_levels(Pool& pl, int B, int n, const Blk* roots, const Blk* dltsft,
             PCGB_POST_LAUNCH();
             return nullptr;
         }
-        const bool rep = PRG == PCGB_PRG_AES && sz >= kRepMinParents;
+        // The last level only writes leaves (no hashing): the plain kernel.
+        const bool rep = PRG == PCGB_PRG_AES && sz >= kRepMinParents && hash_next;
         const dim3 grid(static_cast<unsigned>((sz + kTPB - 1) / kTPB), static_cast<unsigned>(B));
         if constexpr (PRG == PCGB_PRG_AES) {
             if (rep) {
