@@ -261,6 +261,11 @@ __global__ void __launch_bounds__(kAesPrmtThreads) expand_tops_multi_prmt_kernel
     }
 }
 
+// Work items of one full wave of PRMT CTAs (one per SM).
+inline unsigned long long aes_prmt_wave() {
+    return static_cast<unsigned long long>(sm_count()) * kAesPrmtThreads;
+}
+
 // Grid of a PRMT kernel over `threads` work items: at most one CTA per SM.
 inline unsigned aes_prmt_grid(unsigned long long threads) {
     const unsigned long long need = (threads + kAesPrmtThreads - 1) / kAesPrmtThreads;
@@ -450,16 +455,23 @@ void launch_tops(const Blk* src, int K, int src_lvl, int nlev, int levels, const
     if (nlev < 0 || nlev >= tops_max_depth<W>()) fail(PCGB_EINVAL, "keyed expansion deeper than the DFS stack");
     const size_t threads = static_cast<size_t>(K) << (W * src_lvl);
     if constexpr (PRG == kPrgAes) {
-        PCGB_CK(cudaFuncSetAttribute(expand_tops_prmt_kernel<W>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(kAesPrmtSmemBytes)));
-        expand_tops_prmt_kernel<W><<<aes_prmt_grid(threads), kAesPrmtThreads, kAesPrmtSmemBytes,
-                                     st>>>(src, K, src_lvl, nlev, levels, cws, te, rk, dst);
-    } else {
-        const int TPB = 128;
-        expand_tops_kernel<W, PRG><<<static_cast<unsigned>((threads + TPB - 1) / TPB), TPB, 0,
-                                     st>>>(src, K, src_lvl, nlev, levels, cws, te, rk, dst);
+        // A stage with fewer threads than one wave of PRMT CTAs keeps the
+        // replicated table in small CTAs, spread over every SM.
+        if (threads >= aes_prmt_wave()) {
+            PCGB_CK(cudaFuncSetAttribute(expand_tops_prmt_kernel<W>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kAesPrmtSmemBytes)));
+            expand_tops_prmt_kernel<W><<<aes_prmt_grid(threads), kAesPrmtThreads,
+                                         kAesPrmtSmemBytes, st>>>(src, K, src_lvl, nlev, levels,
+                                                                  cws, te, rk, dst);
+            PCGB_POST_LAUNCH();
+            return;
+        }
     }
+    const int TPB = 128;
+    const size_t smem = PRG == kPrgAes ? sizeof(AesSmem) : 0;
+    expand_tops_kernel<W, PRG><<<static_cast<unsigned>((threads + TPB - 1) / TPB), TPB, smem,
+                                 st>>>(src, K, src_lvl, nlev, levels, cws, te, rk, dst);
     PCGB_POST_LAUNCH();
 }
 
@@ -583,20 +595,24 @@ void tops_multi_launch(const std::vector<TopsJob>& jobs, TopsJob* d_jobs,
     PCGB_CK(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(TopsJob),
                             cudaMemcpyHostToDevice, st));
     if constexpr (PRG == kPrgAes) {
-        PCGB_CK(cudaFuncSetAttribute(expand_tops_multi_prmt_kernel<W>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(kAesPrmtSmemBytes)));
-        expand_tops_multi_prmt_kernel<W><<<aes_prmt_grid(total), kAesPrmtThreads,
-                                           kAesPrmtSmemBytes, st>>>(
-            d_jobs, static_cast<int>(jobs.size()), total, te, rk);
-    } else {
-        const int TPB = 128;
-        const unsigned long long blocks = (total + TPB - 1) / TPB;
-        const unsigned long long cap = static_cast<unsigned long long>(sm_count()) * 8;
-        expand_tops_multi_kernel<W, PRG><<<static_cast<unsigned>(blocks < cap ? blocks : cap),
-                                           TPB, 0, st>>>(d_jobs, static_cast<int>(jobs.size()),
-                                                         total, te, rk);
+        if (total >= aes_prmt_wave()) {   // as launch_tops
+            PCGB_CK(cudaFuncSetAttribute(expand_tops_multi_prmt_kernel<W>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kAesPrmtSmemBytes)));
+            expand_tops_multi_prmt_kernel<W><<<aes_prmt_grid(total), kAesPrmtThreads,
+                                               kAesPrmtSmemBytes, st>>>(
+                d_jobs, static_cast<int>(jobs.size()), total, te, rk);
+            PCGB_POST_LAUNCH();
+            return;
+        }
     }
+    const int TPB = 128;
+    const size_t smem = PRG == kPrgAes ? sizeof(AesSmem) : 0;
+    const unsigned long long blocks = (total + TPB - 1) / TPB;
+    const unsigned long long cap = static_cast<unsigned long long>(sm_count()) * 8;  // persistent
+    expand_tops_multi_kernel<W, PRG><<<static_cast<unsigned>(blocks < cap ? blocks : cap), TPB,
+                                       smem, st>>>(d_jobs, static_cast<int>(jobs.size()), total,
+                                                   te, rk);
     PCGB_POST_LAUNCH();
 }
 
