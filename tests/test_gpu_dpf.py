@@ -180,6 +180,8 @@ MULTI_CASES = [
     (O.PRG_CHACHA8, 1, [(64, 10), (7, 12), (300, 8), (1, 16), (0, 9), (2048, 12)]),
     (O.PRG_CHACHA8, 2, [(100, 10), (16, 12), (1, 4)]),
     (O.PRG_AES, 1, [(64, 10), (9, 12), (0, 6), (33, 7)]),
+    # A final stage of 2^19+ threads: the PRMT-addressed AES walk.
+    (O.PRG_AES, 1, [(4096, 10), (2048, 12), (3, 8)]),
 ]
 
 
@@ -226,3 +228,38 @@ def test_keyed_multi_rejects_bad_groups(pcg):
         pcg.dpf_keyed_full_eval_multi_device([(-1, 6, d.ptr, d.ptr, d.ptr)], 1, pcg.PRG_CHACHA8)
     with pytest.raises(pcg.PcgError, match="round keys"):
         pcg.dpf_keyed_full_eval_multi_device([(4, 6, d.ptr, d.ptr, d.ptr)], 1, pcg.PRG_AES)
+
+
+@pytest.mark.parametrize("prg", [O.PRG_CHACHA8, O.PRG_AES])
+@pytest.mark.parametrize("n,w,K", [(10, 1, 9), (14, 1, 5), (14, 2, 4), (16, 4, 3)])
+def test_point_function_property(pcg, prg, n, w, K):
+    """The reference's half_tree_dpf test (CPU_baseline/test/half_tree_dpf.cpp:80-94):
+    the two parties' leaves XOR to Delta at alpha and to zero everywhere else,
+    for the keyed evaluation and for the interactive drop-in with real DltSft
+    shares (levels of 4096+ parents take the PRMT-addressed AES kernel)."""
+    nk, L = (1 << w) - 1, n // w
+    rks = O.aes_tree_round_keys(np.arange(16, dtype=np.uint8), nk) if prg == O.PRG_AES else None
+    k = dealt_keys(n, w, K, 500 + n + w, prg, rks, with_dlt=True)
+    D = 1 << n
+    want = np.zeros((K, D, 2), np.uint64)
+    want[np.arange(K), k["alphas"]] = k["deltas"]
+    d_c = dev(pcg, k["cws"])
+    keyed = []
+    for roots in (k["roots0"], k["roots1"]):
+        d_r, d_l = dev(pcg, roots), pcg.DeviceBuffer(16 * K * D)
+        pcg.dpf_keyed_full_eval_device(K, n, w, prg, d_r.ptr, d_c.ptr, d_l.ptr, round_keys=rks)
+        keyed.append(d_l.download(np.uint64, 2 * K * D).reshape(K, D, 2))
+    assert (keyed[0] ^ keyed[1] == want).all()
+    cw = k["cws"].reshape(K, L, nk, 2)
+    inter = []
+    for party, roots, dlt in ((0, k["roots0"], k["dlt0"]), (1, k["roots1"], k["dlt1"])):
+        level = [0]
+
+        def exchange(my):
+            peer = my.reshape(K, nk, 2) ^ cw[:, level[0]]
+            level[0] += 1
+            return peer.reshape(-1, 2)
+
+        inter.append(pcg.dpf_gpu_batch_full_eval(K, n, w, roots, dlt, round_keys=rks, party=party,
+                                                 exchange=exchange, prg=prg).reshape(K, D, 2))
+    assert (inter[0] ^ inter[1] == want).all()
