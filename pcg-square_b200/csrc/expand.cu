@@ -55,15 +55,32 @@ __device__ __forceinline__ void x_body(const uint64_t* __restrict__ pos,
     if (i0 == 1)
         for (int k = 0; k < t; ++k)
             if (nz[k] == p) acc = add_p(acc, nz[ct + k]);
-    for (int i = i0; i < c; ++i) {
-        const uint64_t* a = aR + static_cast<size_t>(i - i0) * N;
-        for (int k = 0; k < t; ++k) {
-            const uint64_t ps = nz[i * t + k];
-            const bool wrap = p < ps;
-            const size_t idx = wrap ? p + N - ps : p - ps;
-            const uint64_t term = mont_mul(__ldg(a + idx), nz[ct + i * t + k]);
-            acc = wrap ? sub_p(acc, term) : add_p(acc, term);
+    // The (i, k) terms as one flat run q = (i - i0) * t + k (t is a power of
+    // two), eight gathers issued before their products so that eight loads
+    // of the a_i rows are in flight per thread.
+    const int nt = (c - i0) * t, lt = __ffs(t) - 1, q0 = i0 * t;
+    const uint64_t* nv = nz + ct + q0;
+    auto gather = [&](int q, bool& wrap) {
+        const uint64_t ps = nz[q0 + q];
+        wrap = p < ps;
+        return __ldg(aR + static_cast<size_t>(q >> lt) * N + (wrap ? p + N - ps : p - ps));
+    };
+    int q = 0;
+    for (; q + 8 <= nt; q += 8) {
+        uint64_t v[8];
+        bool w[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = gather(q + j, w[j]);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const uint64_t term = mont_mul(v[j], nv[q + j]);
+            acc = w[j] ? sub_p(acc, term) : add_p(acc, term);
         }
+    }
+    for (; q < nt; ++q) {
+        bool w;
+        const uint64_t term = mont_mul(gather(q, w), nv[q]);
+        acc = w ? sub_p(acc, term) : add_p(acc, term);
     }
     x[p] = acc;
 }
