@@ -3,10 +3,16 @@
 // N = n1 * n2 with n1 = 2^floor(logN/2), n2 = 2^ceil(logN/2); coefficient j
 // sits at row j / n2, column j % n2.  With psi a primitive 2N-th root:
 //   column pass: negacyclic NTT of length n1 on every column (root
-//                psi1 = psi^n2), then multiply element (k, j2) by the
-//                twiddle psi^(j2 * (2*i1 + 1 - n1)), i1 = brev(k);
-//   row pass:    negacyclic NTT of length n2 on every row (root psi2 =
-//                psi^n1).
+//                psi1 = psi^n2);
+//   row pass:    multiply element (k, j2) by the twiddle
+//                psi^(j2 * (2*i1 + 1 - n1)), i1 = brev(k), then a
+//                negacyclic NTT of length n2 on every row (root psi2 =
+//                psi^n1).  The row transform's first stage has a single
+//                root w0; it is folded into the twiddles of the row's upper
+//                half, so that stage only adds and subtracts, and each
+//                element costs one Shoup product by a (value, quotient)
+//                pair where a Montgomery twiddle product and half a
+//                butterfly product stood.
 // Element (k, k2) then holds A(psi^(2*(i1 + n1*i2) + 1)) with i1 = brev(k),
 // i2 = brev(k2): the evaluations of a(x) mod x^N + 1.  The row pass stores
 // its outputs in a fixed permuted order (below) that every operand of a
@@ -67,10 +73,12 @@ struct NttPlan {
     ulonglong2* tw1i = nullptr;
     ulonglong2* tw2 = nullptr;    // row roots
     ulonglong2* tw2i = nullptr;
-    uint64_t* W = nullptr;        // [n1][n2] forward twiddle, Montgomery form
-    uint64_t* Wi = nullptr;       // inverse twiddle * N^-1, Montgomery form
-    uint64_t* WiR = nullptr;      // Wi * 2^64: for products of two plain transforms
-    std::mutex mu;                // guards the lazy WiR
+    // [n1][n2] four-step twiddles as Shoup pairs, the row transform's first
+    // (forward) / last (inverse) root folded into the upper half of each row
+    ulonglong2* Wf = nullptr;     // forward twiddle
+    ulonglong2* Wif = nullptr;    // inverse twiddle * N^-1
+    ulonglong2* WiRf = nullptr;   // Wif * 2^64: for products of two plain transforms
+    std::mutex mu;                // guards the lazy WiRf
 };
 
 namespace {
@@ -110,6 +118,21 @@ __device__ __forceinline__ void gs_bfly(uint64_t& X, uint64_t& Y, ulonglong2 w) 
     X = s;
 }
 
+// Butterfly of a stage whose root has been folded into the per-element
+// twiddles (the row pass's first forward stage and last inverse stage):
+// X, Y in [0, 2p) -> X + Y, X - Y in [0, 4p).
+__device__ __forceinline__ void add_sub_bfly(uint64_t& X, uint64_t& Y) {
+    const uint64_t s = X + Y;
+    Y = X - Y + k2P;
+    X = s;
+}
+
+// Shoup product with a per-element twiddle pair (value, quotient).
+__device__ __forceinline__ uint64_t shoup_tw(uint64_t a, const ulonglong2* __restrict__ w) {
+    const ulonglong2 v = __ldg(w);
+    return shoup_lazy(a, v.x, v.y);
+}
+
 // ---- phase geometry ----------------------------------------------------------
 
 template <int L>
@@ -140,7 +163,10 @@ __device__ __forceinline__ int perm_pos(int i) {
     else return i;
 }
 
-template <int L, int P, bool INV>
+// FOLD: stage 0 (a single root) has that root folded into the per-element
+// twiddles the caller applies (before the forward phases, after the inverse
+// ones), so it is a plain add/sub; its inputs are in [0, 2p).
+template <int L, int P, bool INV, bool FOLD>
 __device__ __forceinline__ void run_phase(uint64_t (&x)[Geo<L>::E], int t,
                                           const ulonglong2* __restrict__ tw) {
     constexpr int s0 = 4 * P, r = Geo<L>::r(P), U = Geo<L>::E >> r, ltl = L - s0 - r;
@@ -153,6 +179,12 @@ __device__ __forceinline__ void run_phase(uint64_t (&x)[Geo<L>::E], int t,
             for (int q = 0; q < r; ++q) {
 #pragma unroll
                 for (int sub = 0; sub < (1 << q); ++sub) {
+                    if (FOLD && s0 + q == 0) {
+#pragma unroll
+                        for (int kk = 0; kk < (1 << (r - 1)); ++kk)
+                            add_sub_bfly(x[o + kk], x[o + kk + (1 << (r - 1))]);
+                        continue;
+                    }
                     const ulonglong2 w = __ldg(tw + (1 << (s0 + q)) + (sub << s0) + g);
 #pragma unroll
                     for (int kk = 0; kk < (1 << (r - 1 - q)); ++kk) {
@@ -169,6 +201,12 @@ __device__ __forceinline__ void run_phase(uint64_t (&x)[Geo<L>::E], int t,
                 const int q = r - 1 - qq;
 #pragma unroll
                 for (int sub = 0; sub < (1 << q); ++sub) {
+                    if (FOLD && s0 + q == 0) {
+#pragma unroll
+                        for (int kk = 0; kk < (1 << (r - 1)); ++kk)
+                            add_sub_bfly(x[o + kk], x[o + kk + (1 << (r - 1))]);
+                        continue;
+                    }
                     const ulonglong2 w = __ldg(tw + (1 << (s0 + q)) + (sub << s0) + g);
 #pragma unroll
                     for (int kk = 0; kk < (1 << (r - 1 - q)); ++kk) {
@@ -200,24 +238,24 @@ __device__ __forceinline__ void exchange(uint64_t (&x)[Geo<L>::E], int t, const 
 }
 
 // All forward phases: registers start in phase 0 layout, end in the last.
-template <int L, int P = 0, class Lay>
+template <int L, bool FOLD, int P = 0, class Lay>
 __device__ __forceinline__ void forward_all(uint64_t (&x)[Geo<L>::E], int t,
                                             const ulonglong2* __restrict__ tw, const Lay& lay) {
     if constexpr (P < Geo<L>::NPH) {
         if constexpr (P > 0) exchange<L, P - 1, P>(x, t, lay);
-        run_phase<L, P, false>(x, t, tw);
-        forward_all<L, P + 1>(x, t, tw, lay);
+        run_phase<L, P, false, FOLD>(x, t, tw);
+        forward_all<L, FOLD, P + 1>(x, t, tw, lay);
     }
 }
 
 // All inverse phases: registers start in the last phase layout, end in phase 0.
-template <int L, int P = Geo<L>::NPH - 1, class Lay>
+template <int L, bool FOLD, int P = Geo<L>::NPH - 1, class Lay>
 __device__ __forceinline__ void inverse_all(uint64_t (&x)[Geo<L>::E], int t,
                                             const ulonglong2* __restrict__ twi, const Lay& lay) {
     if constexpr (P >= 0) {
         if constexpr (P < Geo<L>::NPH - 1) exchange<L, P + 1, P>(x, t, lay);
-        run_phase<L, P, true>(x, t, twi);
-        inverse_all<L, P - 1>(x, t, twi, lay);
+        run_phase<L, P, true, FOLD>(x, t, twi);
+        inverse_all<L, FOLD, P - 1>(x, t, twi, lay);
     }
 }
 
@@ -248,14 +286,15 @@ __host__ __device__ constexpr int row_threads() { return Geo<L>::T * row_V<L>();
 // mixed-length kernels (a job table names each CTA's polynomial and tile).
 // Pointers arrive already offset to the polynomial's first word.
 
-// Column pass, forward, then the four-step twiddle, for columns
-// [tile*C, tile*C + C).  src may equal dst (every CTA loads its columns
-// before its first store).  REDUCE maps arbitrary 64-bit inputs into [0, p)
-// first; otherwise inputs must be below 4p.  Outputs in [0, p).
+// Column pass, forward, for columns [tile*C, tile*C + C).  src may equal
+// dst (every CTA loads its columns before its first store).  REDUCE maps
+// arbitrary 64-bit inputs into [0, p) first; otherwise inputs must be below
+// 4p.  Outputs in [0, 4p), without the four-step twiddle: the row pass
+// applies it together with its own first root.
 template <int L, int C, bool REDUCE>
 __device__ __forceinline__ void col_fwd_body(const uint64_t* src, uint64_t* dst, int l2,
                                              size_t tile, const ulonglong2* __restrict__ tw,
-                                             const uint64_t* __restrict__ W, uint64_t* sm) {
+                                             uint64_t* sm) {
     constexpr int E = Geo<L>::E, LP = last_phase(L);
     const int t = threadIdx.x / C, c = threadIdx.x % C;
     const size_t n2 = size_t{1} << l2;
@@ -266,12 +305,9 @@ __device__ __forceinline__ void col_fwd_body(const uint64_t* src, uint64_t* dst,
         const uint64_t v = src[col + eidx<L, 0>(t, e) * n2];
         x[e] = REDUCE ? reduce_p(v) : v;
     }
-    forward_all<L>(x, t, tw, SmemLay<C>{sm + c});
+    forward_all<L, false>(x, t, tw, SmemLay<C>{sm + c});
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const size_t i = eidx<L, LP>(t, e);
-        dst[col + i * n2] = csub(mont_lazy(x[e], __ldg(W + i * n2 + col)), kPm);
-    }
+    for (int e = 0; e < E; ++e) dst[col + eidx<L, LP>(t, e) * n2] = x[e];
 }
 
 // Column pass, inverse, in place (output in natural coefficient order, in
@@ -286,24 +322,30 @@ __device__ __forceinline__ void col_inv_body(uint64_t* d, int l2, size_t tile,
     uint64_t x[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) x[e] = d[col + eidx<L, LP>(t, e) * n2];
-    inverse_all<L>(x, t, twi, SmemLay<C>{sm + c});
+    inverse_all<L, false>(x, t, twi, SmemLay<C>{sm + c});
 #pragma unroll
     for (int e = 0; e < E; ++e) d[col + eidx<L, 0>(t, e) * n2] = csub(x[e], kPm);
 }
 
 // Row pass, forward, in place on rows [tile*V, tile*V + V) (each thread
-// reads and writes the same set of positions); outputs in [0, p) in the
-// permuted order.
+// reads and writes the same set of positions): the four-step twiddle with
+// the row transform's first root folded in (Wf, per element), then the row
+// transform; outputs in [0, p) in the permuted order.
 template <int L, int V>
 __device__ __forceinline__ void row_fwd_body(uint64_t* d, size_t tile,
-                                             const ulonglong2* __restrict__ tw, uint64_t* sm) {
+                                             const ulonglong2* __restrict__ tw,
+                                             const ulonglong2* __restrict__ Wf, uint64_t* sm) {
     constexpr int E = Geo<L>::E, T = Geo<L>::T, LP = last_phase(L);
     const int t = threadIdx.x % T, v = threadIdx.x / T;
-    uint64_t* row = d + (tile * V + v) * Geo<L>::n;
+    const size_t base = (tile * V + v) * Geo<L>::n;
+    uint64_t* row = d + base;
     uint64_t x[E];
 #pragma unroll
-    for (int e = 0; e < E; ++e) x[e] = row[eidx<L, 0>(t, e)];
-    forward_all<L>(x, t, tw, SmemLay<1>{sm + v * Geo<L>::PAD});
+    for (int e = 0; e < E; ++e) {
+        const int i = eidx<L, 0>(t, e);
+        x[e] = shoup_tw(row[i], Wf + base + i);
+    }
+    forward_all<L, true>(x, t, tw, SmemLay<1>{sm + v * Geo<L>::PAD});
 #pragma unroll
     for (int e = 0; e < E; ++e)
         row[perm_pos<L>(eidx<L, LP>(t, e))] = csub(csub(x[e], k2P), kPm);
@@ -313,8 +355,10 @@ __device__ __forceinline__ void row_fwd_body(uint64_t* d, size_t tile,
 //   out row = Wi (.) INTT( sum_q NTT(g_q row) (.) img_q row ),
 // g_q = g + q*N, img_q = img + q*N; img_q in the permuted evaluation order,
 // Montgomery-scaled so that the Montgomery product gives the plain one.
-// g rows come from the column pass; out is in [0, p) and may alias g (a CTA
-// reads all its rows before its first store).  ONE (Q == 1, a plain
+// g rows come from the column pass (Wf, the forward twiddle, is applied
+// here as in row_fwd_body); Wif is the inverse twiddle with the inverse
+// row transform's last root folded in.  out is in [0, p) and may alias g
+// (a CTA reads all its rows before its first store).  ONE (Q == 1, a plain
 // product): the product stays in the transform's registers, with no
 // separate accumulator live across the forward phases.
 template <int L, int V, bool ONE>
@@ -322,7 +366,8 @@ __device__ __forceinline__ void row_mac_body(const uint64_t* g, const uint64_t* 
                                              int Q, size_t N, size_t tile,
                                              const ulonglong2* __restrict__ tw,
                                              const ulonglong2* __restrict__ twi,
-                                             const uint64_t* __restrict__ Wi, uint64_t* out,
+                                             const ulonglong2* __restrict__ Wf,
+                                             const ulonglong2* __restrict__ Wif, uint64_t* out,
                                              uint64_t* sm) {
     constexpr int E = Geo<L>::E, T = Geo<L>::T, LP = last_phase(L);
     const int t = threadIdx.x % T, v = threadIdx.x / T;
@@ -331,8 +376,11 @@ __device__ __forceinline__ void row_mac_body(const uint64_t* g, const uint64_t* 
     uint64_t acc[E];
     if constexpr (ONE) {
 #pragma unroll
-        for (int e = 0; e < E; ++e) acc[e] = g[base + eidx<L, 0>(t, e)];
-        forward_all<L>(acc, t, tw, lay);
+        for (int e = 0; e < E; ++e) {
+            const size_t i = base + eidx<L, 0>(t, e);
+            acc[e] = shoup_tw(g[i], Wf + i);
+        }
+        forward_all<L, true>(acc, t, tw, lay);
 #pragma unroll
         for (int e = 0; e < E; ++e)
             acc[e] = mont_lazy(acc[e], __ldg(img + base + perm_pos<L>(eidx<L, LP>(t, e))));
@@ -344,8 +392,11 @@ __device__ __forceinline__ void row_mac_body(const uint64_t* g, const uint64_t* 
             const uint64_t* im = img + q * N + base;
             uint64_t x[E];
 #pragma unroll
-            for (int e = 0; e < E; ++e) x[e] = gr[eidx<L, 0>(t, e)];
-            forward_all<L>(x, t, tw, lay);
+            for (int e = 0; e < E; ++e) {
+                const int i = eidx<L, 0>(t, e);
+                x[e] = shoup_tw(gr[i], Wf + base + i);
+            }
+            forward_all<L, true>(x, t, tw, lay);
 #pragma unroll
             for (int e = 0; e < E; ++e) {
                 const uint64_t m = mont_lazy(x[e], __ldg(im + perm_pos<L>(eidx<L, LP>(t, e))));
@@ -353,23 +404,26 @@ __device__ __forceinline__ void row_mac_body(const uint64_t* g, const uint64_t* 
             }
         }
     }
-    inverse_all<L>(acc, t, twi, lay);
+    inverse_all<L, true>(acc, t, twi, lay);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const size_t i = base + eidx<L, 0>(t, e);
-        out[i] = csub(mont_lazy(acc[e], __ldg(Wi + i)), kPm);
+        out[i] = csub(shoup_tw(acc[e], Wif + i), kPm);
     }
 }
 
 // Pointwise product and inverse row pass on rows [tile*V, tile*V + V) of a
 // transform already in the permuted evaluation order (row_fwd_body's
-// output): out row = Wi (.) INTT( d row (.) img row ), in place.  Each
-// thread loads the permuted positions of its last-phase registers, so the
-// inverse starts where the fused forward would have ended.
+// output): out row = Wi (.) INTT( d row (.) img row ), in place, Wi given
+// as WiRf (the inverse twiddle times 2^64, which cancels the Montgomery
+// product's 2^-64, with the last root folded in).  Each thread loads the
+// permuted positions of its last-phase registers, so the inverse starts
+// where the fused forward would have ended.
 template <int L, int V>
 __device__ __forceinline__ void row_pmul_inv_body(uint64_t* d, const uint64_t* __restrict__ img,
                                                   size_t tile, const ulonglong2* __restrict__ twi,
-                                                  const uint64_t* __restrict__ Wi, uint64_t* sm) {
+                                                  const ulonglong2* __restrict__ WiRf,
+                                                  uint64_t* sm) {
     constexpr int E = Geo<L>::E, T = Geo<L>::T, LP = last_phase(L);
     const int t = threadIdx.x % T, v = threadIdx.x / T;
     const size_t base = (tile * V + v) * Geo<L>::n;
@@ -379,11 +433,11 @@ __device__ __forceinline__ void row_pmul_inv_body(uint64_t* d, const uint64_t* _
         const size_t i = base + perm_pos<L>(eidx<L, LP>(t, e));
         x[e] = mont_lazy(d[i], __ldg(img + i));
     }
-    inverse_all<L>(x, t, twi, SmemLay<1>{sm + v * Geo<L>::PAD});
+    inverse_all<L, true>(x, t, twi, SmemLay<1>{sm + v * Geo<L>::PAD});
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const size_t i = base + eidx<L, 0>(t, e);
-        d[i] = csub(mont_lazy(x[e], __ldg(Wi + i)), kPm);
+        d[i] = csub(shoup_tw(x[e], WiRf + i), kPm);
     }
 }
 
@@ -391,11 +445,10 @@ __device__ __forceinline__ void row_pmul_inv_body(uint64_t* d, const uint64_t* _
 
 template <int L, bool REDUCE>
 __global__ void __launch_bounds__(col_threads<L>(), 2) col_fwd_kernel(
-    const uint64_t* src, uint64_t* dst, int l2, const ulonglong2* __restrict__ tw,
-    const uint64_t* __restrict__ W) {
+    const uint64_t* src, uint64_t* dst, int l2, const ulonglong2* __restrict__ tw) {
     extern __shared__ uint64_t sm[];
     const size_t off = static_cast<size_t>(blockIdx.y) << (L + l2);
-    col_fwd_body<L, col_C(L), REDUCE>(src + off, dst + off, l2, blockIdx.x, tw, W, sm);
+    col_fwd_body<L, col_C(L), REDUCE>(src + off, dst + off, l2, blockIdx.x, tw, sm);
 }
 
 template <int L>
@@ -408,19 +461,19 @@ __global__ void __launch_bounds__(col_threads<L>(), 2) col_inv_kernel(
 
 template <int L>
 __global__ void __launch_bounds__(row_threads<L>()) row_fwd_kernel(
-    uint64_t* d, int l1, const ulonglong2* __restrict__ tw) {
+    uint64_t* d, int l1, const ulonglong2* __restrict__ tw, const ulonglong2* __restrict__ Wf) {
     extern __shared__ uint64_t sm[];
     row_fwd_body<L, row_V<L>()>(d + (static_cast<size_t>(blockIdx.y) << (L + l1)), blockIdx.x,
-                                tw, sm);
+                                tw, Wf, sm);
 }
 
 template <int L>
 __global__ void __launch_bounds__(row_threads<L>()) row_pmul_inv_kernel(
     uint64_t* d, const uint64_t* __restrict__ img, int l1, const ulonglong2* __restrict__ twi,
-    const uint64_t* __restrict__ Wi) {
+    const ulonglong2* __restrict__ WiRf) {
     extern __shared__ uint64_t sm[];
     const size_t off = static_cast<size_t>(blockIdx.y) << (L + l1);
-    row_pmul_inv_body<L, row_V<L>()>(d + off, img + off, blockIdx.x, twi, Wi, sm);
+    row_pmul_inv_body<L, row_V<L>()>(d + off, img + off, blockIdx.x, twi, WiRf, sm);
 }
 
 // Instance b reads g and img at b*Q*N and writes out at b*N.
@@ -428,12 +481,12 @@ template <int L, bool ONE>
 __global__ void __launch_bounds__(row_threads<L>()) row_mac_inv_kernel(
     const uint64_t* g, const uint64_t* __restrict__ img, int Q, int l1,
     const ulonglong2* __restrict__ tw, const ulonglong2* __restrict__ twi,
-    const uint64_t* __restrict__ Wi, uint64_t* out) {
+    const ulonglong2* __restrict__ Wf, const ulonglong2* __restrict__ Wif, uint64_t* out) {
     extern __shared__ uint64_t sm[];
     const size_t N = size_t{1} << (L + l1);
     const size_t b = blockIdx.y;
     row_mac_body<L, row_V<L>(), ONE>(g + b * Q * N, img + b * Q * N, Q, N, blockIdx.x, tw, twi,
-                                     Wi, out + b * N, sm);
+                                     Wf, Wif, out + b * N, sm);
 }
 
 // ---- mixed-length kernels --------------------------------------------------------
@@ -453,8 +506,8 @@ struct MixedPoly {
     const ulonglong2* tw1i;
     const ulonglong2* tw2;
     const ulonglong2* tw2i;
-    const uint64_t* W;
-    const uint64_t* WiR;
+    const ulonglong2* Wf;
+    const ulonglong2* WiRf;
     int l1, l2;
 };
 struct MixedCta {
@@ -489,7 +542,7 @@ __global__ void __launch_bounds__(kMixedColThreads, 2) mixed_col_fwd_kernel(
     const MixedPoly& p = polys[j.poly];
     const uint64_t* src = which ? p.b : p.a;
     uint64_t* dst = which ? p.c : p.A;
-#define PCGB_CALL(LL) col_fwd_body<LL, mixed_C<LL>(), true>(src, dst, p.l2, j.tile, p.tw1, p.W, sm)
+#define PCGB_CALL(LL) col_fwd_body<LL, mixed_C<LL>(), true>(src, dst, p.l2, j.tile, p.tw1, sm)
     PCGB_MIXED_SWITCH(p.l1, PCGB_CALL)
 #undef PCGB_CALL
 }
@@ -499,7 +552,7 @@ __global__ void __launch_bounds__(kMixedRowThreads) mixed_row_fwd_kernel(
     extern __shared__ uint64_t sm[];
     const MixedCta j = ctas[blockIdx.x];
     const MixedPoly& p = polys[j.poly];
-#define PCGB_CALL(LL) row_fwd_body<LL, mixed_V<LL>()>(p.A, j.tile, p.tw2, sm)
+#define PCGB_CALL(LL) row_fwd_body<LL, mixed_V<LL>()>(p.A, j.tile, p.tw2, p.Wf, sm)
     PCGB_MIXED_SWITCH(p.l2, PCGB_CALL)
 #undef PCGB_CALL
 }
@@ -512,7 +565,8 @@ __global__ void __launch_bounds__(kMixedRowThreads) mixed_row_mac_kernel(
     const MixedPoly& p = polys[j.poly];
     const size_t N = size_t{1} << (p.l1 + p.l2);
 #define PCGB_CALL(LL) \
-    row_mac_body<LL, mixed_V<LL>(), true>(p.c, p.A, 1, N, j.tile, p.tw2, p.tw2i, p.WiR, p.c, sm)
+    row_mac_body<LL, mixed_V<LL>(), true>(p.c, p.A, 1, N, j.tile, p.tw2, p.tw2i, p.Wf, p.WiRf, \
+                                          p.c, sm)
     PCGB_MIXED_SWITCH(p.l2, PCGB_CALL)
 #undef PCGB_CALL
 }
@@ -543,8 +597,8 @@ struct MacReq {
     const ulonglong2* tw1i;
     const ulonglong2* tw2;
     const ulonglong2* tw2i;
-    const uint64_t* W;
-    const uint64_t* Wi;
+    const ulonglong2* Wf;
+    const ulonglong2* Wif;
     int Q, l1, l2;
 };
 struct MacCta {
@@ -570,7 +624,7 @@ __global__ void __launch_bounds__(kMixedColThreads, 2) mac_col_fwd_kernel(
     const MacCta j = ctas[blockIdx.x];
     const MacReq& r = reqs[j.req];
     uint64_t* d = r.g + (static_cast<size_t>(j.q) << (r.l1 + r.l2));
-#define PCGB_CALL(LL) col_fwd_body<LL, mixed_C<LL>(), false>(d, d, r.l2, j.tile, r.tw1, r.W, sm)
+#define PCGB_CALL(LL) col_fwd_body<LL, mixed_C<LL>(), false>(d, d, r.l2, j.tile, r.tw1, sm)
     PCGB_MAC_SWITCH(r.l1, PCGB_CALL)
 #undef PCGB_CALL
 }
@@ -582,7 +636,8 @@ __global__ void __launch_bounds__(kMixedRowThreads) mac_row_kernel(
     const MacReq& r = reqs[j.req];
     const size_t N = size_t{1} << (r.l1 + r.l2);
 #define PCGB_CALL(LL) \
-    row_mac_body<LL, mixed_V<LL>(), false>(r.g, r.img, r.Q, N, j.tile, r.tw2, r.tw2i, r.Wi, r.z, sm)
+    row_mac_body<LL, mixed_V<LL>(), false>(r.g, r.img, r.Q, N, j.tile, r.tw2, r.tw2i, r.Wf, r.Wif, \
+                                           r.z, sm)
     PCGB_MAC_SWITCH(r.l2, PCGB_CALL)
 #undef PCGB_CALL
 }
@@ -598,10 +653,22 @@ __global__ void __launch_bounds__(kMixedColThreads, 2) mac_col_inv_kernel(
 }
 #undef PCGB_MAC_SWITCH
 
-// Twiddle tables: W[k*n2 + j2] = psi^(j2*(2*brev(k)+1-n1)) (times R), and
-// Wi = psi^-(...) * N^-1 (times R).  powR[b] = psi^(2^b) * R mod p.
-__global__ void twiddle_kernel(uint64_t* W, uint64_t* Wi, int l1, int l2,
-                               const uint64_t* __restrict__ powR, uint64_t oneR, uint64_t ninvR) {
+// Shoup pair (v, floor(v * 2^64 / p)) of v < p given in Montgomery form
+// vR = v * 2^64 mod p: the quotient is (v * 2^64 - vR) / p, an exact
+// division, so it equals vR * (-p^-1) mod 2^64.
+__device__ __forceinline__ ulonglong2 shoup_pair_from_mont(uint64_t vR) {
+    return make_ulonglong2(mont_mul(vR, 1), vR * kPNegInv);
+}
+
+// Twiddle tables, element k*n2 + j2 with e = j2*(2*brev(k)+1-n1) mod 2N:
+//   Wf  = psi^e,          times w0 = psi2^(n2/2) for j2 >= n2/2,
+//   Wif = psi^-e * N^-1,  times w0i = psi2^-(n2/2) for j2 >= n2/2,
+// w0 / w0i being the single root of the row transform's first forward /
+// last inverse stage (that stage then only adds and subtracts).
+// powR[b] = psi^(2^b) * R mod p; w0R, w0iR are w0, w0i times R.
+__global__ void twiddle_kernel(ulonglong2* Wf, ulonglong2* Wif, int l1, int l2,
+                               const uint64_t* __restrict__ powR, uint64_t oneR, uint64_t ninvR,
+                               uint64_t w0R, uint64_t w0iR) {
     const size_t N = static_cast<size_t>(1) << (l1 + l2);
     const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= N) return;
@@ -618,8 +685,22 @@ __global__ void twiddle_kernel(uint64_t* W, uint64_t* Wi, int l1, int l2,
         if ((e >> bit) & 1) a = mont_mul(a, powR[bit]);
         if ((ei >> bit) & 1) b = mont_mul(b, powR[bit]);
     }
-    W[idx] = a;                    // psi^e * R
-    Wi[idx] = mont_mul(b, ninvR);  // psi^-e * N^-1 * R
+    b = mont_mul(b, ninvR);        // psi^-e * N^-1 * R
+    if (j2 >= (1u << (l2 - 1))) {
+        a = mont_mul(a, w0R);
+        b = mont_mul(b, w0iR);
+    }
+    Wf[idx] = shoup_pair_from_mont(a);
+    Wif[idx] = shoup_pair_from_mont(b);
+}
+
+// dst = src * 2^64 mod p, Shoup pairs; r2 = 2^128 mod p.
+__global__ void scale_r_kernel(ulonglong2* dst, const ulonglong2* __restrict__ src, size_t n,
+                               uint64_t r2) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t vR = mont_mul(src[i].x, r2);      // v * R: the new value
+    dst[i] = shoup_pair_from_mont(mont_mul(vR, r2));  // from its Montgomery form
 }
 
 // Pointwise products, one word per thread.
@@ -632,12 +713,6 @@ __global__ void pointwise_kernel(uint64_t* c, const uint64_t* a, const uint64_t*
     uint64_t v = mont_mul(a[i], b[i]);
     if (mode == 1) v = mont_mul(v, r2);
     c[i] = v;
-}
-
-// d[i] = s[i] * k * R^-1 (Montgomery product with a constant).
-__global__ void scale_const_kernel(uint64_t* d, const uint64_t* s, size_t n, uint64_t k) {
-    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i < n) d[i] = mont_mul(s[i], k);
 }
 
 __global__ void reduce_kernel(uint64_t* d, const uint64_t* s, size_t n) {
@@ -705,8 +780,8 @@ NttPlan* build_plan(int logN) {
     pl->tw1i = upload_root_table(pow_p_host(psi_inv, pl->n2), pl->l1);
     pl->tw2 = upload_root_table(pow_p_host(psi, pl->n1), pl->l2);
     pl->tw2i = upload_root_table(pow_p_host(psi_inv, pl->n1), pl->l2);
-    PCGB_CK(cudaMalloc(&pl->W, sizeof(uint64_t) * pl->N));
-    PCGB_CK(cudaMalloc(&pl->Wi, sizeof(uint64_t) * pl->N));
+    PCGB_CK(cudaMalloc(&pl->Wf, sizeof(ulonglong2) * pl->N));
+    PCGB_CK(cudaMalloc(&pl->Wif, sizeof(ulonglong2) * pl->N));
     const uint64_t R = r_mod_p();
     std::vector<uint64_t> powR(logN + 2);
     uint64_t pb = psi;
@@ -715,8 +790,11 @@ NttPlan* build_plan(int logN) {
     PCGB_CK(cudaMalloc(&d_pow, sizeof(uint64_t) * powR.size()));
     upload_blocking(d_pow, powR.data(), sizeof(uint64_t) * powR.size());
     const uint64_t ninvR = mul_p_host(pow_p_host(pl->N % kPm, kPm - 2), R);
-    twiddle_kernel<<<static_cast<unsigned>((pl->N + 255) / 256), 256>>>(pl->W, pl->Wi, pl->l1,
-                                                                        pl->l2, d_pow, R, ninvR);
+    // The row transform's stage-0 root: psi2^brev(1) = psi2^(n2/2) = psi^(N/2).
+    const uint64_t w0R = mul_p_host(pow_p_host(psi, pl->N / 2), R);
+    const uint64_t w0iR = mul_p_host(pow_p_host(psi_inv, pl->N / 2), R);
+    twiddle_kernel<<<static_cast<unsigned>((pl->N + 255) / 256), 256>>>(
+        pl->Wf, pl->Wif, pl->l1, pl->l2, d_pow, R, ninvR, w0R, w0iR);
     PCGB_POST_LAUNCH();
     PCGB_CK(cudaDeviceSynchronize());
     cudaFree(d_pow);
@@ -760,10 +838,10 @@ void col_fwd_l(const NttPlan& pl, const uint64_t* src, uint64_t* dst, int batch,
     const dim3 grid(pl.n2 / col_C(L), batch);
     if (reduce) {
         g_optin(col_fwd_kernel<L, true>, sm);
-        col_fwd_kernel<L, true><<<grid, col_threads<L>(), sm, st>>>(src, dst, pl.l2, pl.tw1, pl.W);
+        col_fwd_kernel<L, true><<<grid, col_threads<L>(), sm, st>>>(src, dst, pl.l2, pl.tw1);
     } else {
         g_optin(col_fwd_kernel<L, false>, sm);
-        col_fwd_kernel<L, false><<<grid, col_threads<L>(), sm, st>>>(src, dst, pl.l2, pl.tw1, pl.W);
+        col_fwd_kernel<L, false><<<grid, col_threads<L>(), sm, st>>>(src, dst, pl.l2, pl.tw1);
     }
     PCGB_POST_LAUNCH();
 }
@@ -782,33 +860,33 @@ void row_fwd_l(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
     constexpr size_t sm = row_smem<L>();
     g_optin(row_fwd_kernel<L>, sm);
     row_fwd_kernel<L><<<dim3(pl.n1 / row_V<L>(), batch), row_threads<L>(), sm, st>>>(d, pl.l1,
-                                                                                    pl.tw2);
+                                                                                    pl.tw2, pl.Wf);
     PCGB_POST_LAUNCH();
 }
 
 template <int L>
 void row_pmul_inv_l(const NttPlan& pl, uint64_t* d, const uint64_t* img, int batch,
-                    const uint64_t* Wi, cudaStream_t st) {
+                    const ulonglong2* WiRf, cudaStream_t st) {
     constexpr size_t sm = row_smem<L>();
     g_optin(row_pmul_inv_kernel<L>, sm);
     row_pmul_inv_kernel<L><<<dim3(pl.n1 / row_V<L>(), batch), row_threads<L>(), sm, st>>>(
-        d, img, pl.l1, pl.tw2i, Wi);
+        d, img, pl.l1, pl.tw2i, WiRf);
     PCGB_POST_LAUNCH();
 }
 
 template <int L>
 void row_mac_l(const NttPlan& pl, const uint64_t* g, const uint64_t* img, int Q, int batch,
-               const uint64_t* Wi, uint64_t* out, cudaStream_t st) {
+               const ulonglong2* Wif, uint64_t* out, cudaStream_t st) {
     constexpr size_t sm = row_smem<L>();
     const dim3 grid(pl.n1 / row_V<L>(), batch);
     if (Q == 1) {
         g_optin(row_mac_inv_kernel<L, true>, sm);
         row_mac_inv_kernel<L, true><<<grid, row_threads<L>(), sm, st>>>(g, img, Q, pl.l1, pl.tw2,
-                                                                        pl.tw2i, Wi, out);
+                                                                        pl.tw2i, pl.Wf, Wif, out);
     } else {
         g_optin(row_mac_inv_kernel<L, false>, sm);
         row_mac_inv_kernel<L, false><<<grid, row_threads<L>(), sm, st>>>(g, img, Q, pl.l1, pl.tw2,
-                                                                         pl.tw2i, Wi, out);
+                                                                         pl.tw2i, pl.Wf, Wif, out);
     }
     PCGB_POST_LAUNCH();
 }
@@ -845,25 +923,26 @@ void row_fwd(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
     by_len(pl.l2, [&](auto L) { row_fwd_l<decltype(L)::value>(pl, d, batch, st); });
 }
 void row_pmul_inv(const NttPlan& pl, uint64_t* d, const uint64_t* img, int batch,
-                  const uint64_t* Wi, cudaStream_t st) {
-    by_len(pl.l2, [&](auto L) { row_pmul_inv_l<decltype(L)::value>(pl, d, img, batch, Wi, st); });
+                  const ulonglong2* WiRf, cudaStream_t st) {
+    by_len(pl.l2,
+           [&](auto L) { row_pmul_inv_l<decltype(L)::value>(pl, d, img, batch, WiRf, st); });
 }
 void row_mac(const NttPlan& pl, const uint64_t* g, const uint64_t* img, int Q, int batch,
-             const uint64_t* Wi, uint64_t* out, cudaStream_t st) {
+             const ulonglong2* Wif, uint64_t* out, cudaStream_t st) {
     by_len(pl.l2,
-           [&](auto L) { row_mac_l<decltype(L)::value>(pl, g, img, Q, batch, Wi, out, st); });
+           [&](auto L) { row_mac_l<decltype(L)::value>(pl, g, img, Q, batch, Wif, out, st); });
 }
 
-const uint64_t* wi_times_r(NttPlan& pl, cudaStream_t st) {
+const ulonglong2* wi_times_r(NttPlan& pl, cudaStream_t st) {
     std::lock_guard<std::mutex> lk(pl.mu);
-    if (!pl.WiR) {
-        PCGB_CK(cudaMalloc(&pl.WiR, sizeof(uint64_t) * pl.N));
-        scale_const_kernel<<<static_cast<unsigned>((pl.N + 255) / 256), 256, 0, st>>>(
-            pl.WiR, pl.Wi, pl.N, r2_mod_p());
+    if (!pl.WiRf) {
+        PCGB_CK(cudaMalloc(&pl.WiRf, sizeof(ulonglong2) * pl.N));
+        scale_r_kernel<<<static_cast<unsigned>((pl.N + 255) / 256), 256, 0, st>>>(
+            pl.WiRf, pl.Wif, pl.N, r2_mod_p());
         PCGB_POST_LAUNCH();
         PCGB_CK(cudaStreamSynchronize(st));
     }
-    return pl.WiR;
+    return pl.WiRf;
 }
 
 }  // namespace
@@ -898,7 +977,7 @@ void ntt_forward(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
 
 void poly_mul_device(const NttPlan& pl, uint64_t* c, const uint64_t* a, const uint64_t* b,
                      int batch, uint64_t* scratch, cudaStream_t st) {
-    const uint64_t* wir = wi_times_r(const_cast<NttPlan&>(pl), st);
+    const ulonglong2* wir = wi_times_r(const_cast<NttPlan&>(pl), st);
     // A = NTT(a) in scratch; c = NTT(b); c = INTT(c (.) A): the forward row
     // pass of c and the pointwise product + inverse row pass are separate
     // launches (each needs about 70 registers a thread where the fused
@@ -936,7 +1015,7 @@ void poly_mul_device_mixed(int count, uint64_t* const* c, const uint64_t* const*
         MixedPoly& m = polys[k];
         m.a = a[i]; m.b = b[i]; m.c = c[i]; m.A = scratch + off;
         m.tw1 = pl.tw1; m.tw1i = pl.tw1i; m.tw2 = pl.tw2; m.tw2i = pl.tw2i;
-        m.W = pl.W; m.WiR = wi_times_r(pl, st);
+        m.Wf = pl.Wf; m.WiRf = wi_times_r(pl, st);
         m.l1 = pl.l1; m.l2 = pl.l2;
         off += pl.N;
         int C = 0, V = 0;
@@ -984,7 +1063,7 @@ void poly_mul_device_mixed(int count, uint64_t* const* c, const uint64_t* const*
 void ntt_mac_inverse(const NttPlan& pl, uint64_t* g, const uint64_t* img, int Q, uint64_t* acc,
                      cudaStream_t st) {
     col_fwd(pl, g, g, Q, false, st);
-    row_mac(pl, g, img, Q, 1, pl.Wi, acc, st);
+    row_mac(pl, g, img, Q, 1, pl.Wif, acc, st);
     col_inv(pl, acc, 1, st);
 }
 
@@ -1011,7 +1090,7 @@ void ntt_mac_inverse_multi(int count, uint64_t* const* g, const uint64_t* const*
         MacReq& m = reqs[k];
         m.g = g[i]; m.img = img[i]; m.z = z[i];
         m.tw1 = pl.tw1; m.tw1i = pl.tw1i; m.tw2 = pl.tw2; m.tw2i = pl.tw2i;
-        m.W = pl.W; m.Wi = pl.Wi;
+        m.Wf = pl.Wf; m.Wif = pl.Wif;
         m.Q = Q[i]; m.l1 = pl.l1; m.l2 = pl.l2;
         int C = 0, V = 0;
         by_len(pl.l1, [&](auto L) {
