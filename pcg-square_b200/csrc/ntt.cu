@@ -290,14 +290,15 @@ __host__ __device__ constexpr int row_threads() { return Geo<L>::T * row_V<L>();
 // dst (every CTA loads its columns before its first store).  REDUCE maps
 // arbitrary 64-bit inputs into [0, p) first; otherwise inputs must be below
 // 4p.  Outputs in [0, 4p), without the four-step twiddle: the row pass
-// applies it together with its own first root.
-template <int L, int C, bool REDUCE>
+// applies it together with its own first root.  L2 >= 0 fixes log2(n2) at
+// compile time (element offsets become immediates); -1 takes l2.
+template <int L, int C, bool REDUCE, int L2 = -1>
 __device__ __forceinline__ void col_fwd_body(const uint64_t* src, uint64_t* dst, int l2,
                                              size_t tile, const ulonglong2* __restrict__ tw,
                                              uint64_t* sm) {
     constexpr int E = Geo<L>::E, LP = last_phase(L);
     const int t = threadIdx.x / C, c = threadIdx.x % C;
-    const size_t n2 = size_t{1} << l2;
+    const size_t n2 = size_t{1} << (L2 >= 0 ? L2 : l2);
     const size_t col = tile * C + c;
     uint64_t x[E];
 #pragma unroll
@@ -311,13 +312,13 @@ __device__ __forceinline__ void col_fwd_body(const uint64_t* src, uint64_t* dst,
 }
 
 // Column pass, inverse, in place (output in natural coefficient order, in
-// [0, p)).
-template <int L, int C>
+// [0, p)).  L2 as in col_fwd_body.
+template <int L, int C, int L2 = -1>
 __device__ __forceinline__ void col_inv_body(uint64_t* d, int l2, size_t tile,
                                              const ulonglong2* __restrict__ twi, uint64_t* sm) {
     constexpr int E = Geo<L>::E, LP = last_phase(L);
     const int t = threadIdx.x / C, c = threadIdx.x % C;
-    const size_t n2 = size_t{1} << l2;
+    const size_t n2 = size_t{1} << (L2 >= 0 ? L2 : l2);
     const size_t col = tile * C + c;
     uint64_t x[E];
 #pragma unroll
@@ -443,20 +444,21 @@ __device__ __forceinline__ void row_pmul_inv_body(uint64_t* d, const uint64_t* _
 
 // ---- per-length kernels: grid = (tiles, batch) ---------------------------------
 
-template <int L, bool REDUCE>
+// The column kernels fix the row length: l2 = L + DL (l2 - l1 is 0 or 1).
+template <int L, bool REDUCE, int DL>
 __global__ void __launch_bounds__(col_threads<L>(), 2) col_fwd_kernel(
-    const uint64_t* src, uint64_t* dst, int l2, const ulonglong2* __restrict__ tw) {
+    const uint64_t* src, uint64_t* dst, const ulonglong2* __restrict__ tw) {
     extern __shared__ uint64_t sm[];
-    const size_t off = static_cast<size_t>(blockIdx.y) << (L + l2);
-    col_fwd_body<L, col_C(L), REDUCE>(src + off, dst + off, l2, blockIdx.x, tw, sm);
+    const size_t off = static_cast<size_t>(blockIdx.y) << (2 * L + DL);
+    col_fwd_body<L, col_C(L), REDUCE, L + DL>(src + off, dst + off, L + DL, blockIdx.x, tw, sm);
 }
 
-template <int L>
+template <int L, int DL>
 __global__ void __launch_bounds__(col_threads<L>(), 2) col_inv_kernel(
-    uint64_t* d, int l2, const ulonglong2* __restrict__ twi) {
+    uint64_t* d, const ulonglong2* __restrict__ twi) {
     extern __shared__ uint64_t sm[];
-    col_inv_body<L, col_C(L)>(d + (static_cast<size_t>(blockIdx.y) << (L + l2)), l2, blockIdx.x,
-                              twi, sm);
+    col_inv_body<L, col_C(L), L + DL>(d + (static_cast<size_t>(blockIdx.y) << (2 * L + DL)),
+                                      L + DL, blockIdx.x, twi, sm);
 }
 
 template <int L>
@@ -836,22 +838,24 @@ void col_fwd_l(const NttPlan& pl, const uint64_t* src, uint64_t* dst, int batch,
                cudaStream_t st) {
     constexpr size_t sm = col_smem<L>();
     const dim3 grid(pl.n2 / col_C(L), batch);
-    if (reduce) {
-        g_optin(col_fwd_kernel<L, true>, sm);
-        col_fwd_kernel<L, true><<<grid, col_threads<L>(), sm, st>>>(src, dst, pl.l2, pl.tw1);
-    } else {
-        g_optin(col_fwd_kernel<L, false>, sm);
-        col_fwd_kernel<L, false><<<grid, col_threads<L>(), sm, st>>>(src, dst, pl.l2, pl.tw1);
-    }
+    auto go = [&](auto kernel) {
+        g_optin(kernel, sm);
+        kernel<<<grid, col_threads<L>(), sm, st>>>(src, dst, pl.tw1);
+    };
+    const bool odd = pl.l2 != L;
+    if (reduce) odd ? go(col_fwd_kernel<L, true, 1>) : go(col_fwd_kernel<L, true, 0>);
+    else odd ? go(col_fwd_kernel<L, false, 1>) : go(col_fwd_kernel<L, false, 0>);
     PCGB_POST_LAUNCH();
 }
 
 template <int L>
 void col_inv_l(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
     constexpr size_t sm = col_smem<L>();
-    g_optin(col_inv_kernel<L>, sm);
-    col_inv_kernel<L><<<dim3(pl.n2 / col_C(L), batch), col_threads<L>(), sm, st>>>(d, pl.l2,
-                                                                                  pl.tw1i);
+    auto go = [&](auto kernel) {
+        g_optin(kernel, sm);
+        kernel<<<dim3(pl.n2 / col_C(L), batch), col_threads<L>(), sm, st>>>(d, pl.tw1i);
+    };
+    pl.l2 != L ? go(col_inv_kernel<L, 1>) : go(col_inv_kernel<L, 0>);
     PCGB_POST_LAUNCH();
 }
 
