@@ -535,6 +535,16 @@ static_assert(sizeof(uint64_t) * Geo<8>::PAD * mixed_C<8>() == kMixedColSmem &&
         case 10: CALL(10); break;     \
         default: break;               \
     }
+// Column passes: (l1, l2) pairs, l2 = l1 or l1 + 1, both compile-time.
+#define PCGB_MIXED_COL_SWITCH(P1, P2, CALL)           \
+    switch (2 * (P1) + ((P2) - (P1))) {                \
+        case 16: CALL(8, 8); break;                    \
+        case 17: CALL(8, 9); break;                    \
+        case 18: CALL(9, 9); break;                    \
+        case 19: CALL(9, 10); break;                   \
+        case 20: CALL(10, 10); break;                  \
+        default: break;                                \
+    }
 
 // which = 0: column pass of a into A; which = 1: column pass of b into c.
 __global__ void __launch_bounds__(kMixedColThreads, 2) mixed_col_fwd_kernel(
@@ -544,8 +554,9 @@ __global__ void __launch_bounds__(kMixedColThreads, 2) mixed_col_fwd_kernel(
     const MixedPoly& p = polys[j.poly];
     const uint64_t* src = which ? p.b : p.a;
     uint64_t* dst = which ? p.c : p.A;
-#define PCGB_CALL(LL) col_fwd_body<LL, mixed_C<LL>(), true>(src, dst, p.l2, j.tile, p.tw1, sm)
-    PCGB_MIXED_SWITCH(p.l1, PCGB_CALL)
+#define PCGB_CALL(LL, L2) \
+    col_fwd_body<LL, mixed_C<LL>(), true, L2>(src, dst, L2, j.tile, p.tw1, sm)
+    PCGB_MIXED_COL_SWITCH(p.l1, p.l2, PCGB_CALL)
 #undef PCGB_CALL
 }
 
@@ -578,11 +589,12 @@ __global__ void __launch_bounds__(kMixedColThreads, 2) mixed_col_inv_kernel(
     extern __shared__ uint64_t sm[];
     const MixedCta j = ctas[blockIdx.x];
     const MixedPoly& p = polys[j.poly];
-#define PCGB_CALL(LL) col_inv_body<LL, mixed_C<LL>()>(p.c, p.l2, j.tile, p.tw1i, sm)
-    PCGB_MIXED_SWITCH(p.l1, PCGB_CALL)
+#define PCGB_CALL(LL, L2) col_inv_body<LL, mixed_C<LL>(), L2>(p.c, L2, j.tile, p.tw1i, sm)
+    PCGB_MIXED_COL_SWITCH(p.l1, p.l2, PCGB_CALL)
 #undef PCGB_CALL
 }
 #undef PCGB_MIXED_SWITCH
+#undef PCGB_MIXED_COL_SWITCH
 
 // ---- multi-request multiply-accumulate ------------------------------------
 // The step-4 transforms of several expansions of different lengths
@@ -619,6 +631,17 @@ static_assert(sizeof(uint64_t) * Geo<7>::PAD * mixed_C<7>() == kMixedColSmem &&
         case 10: CALL(10); break;   \
         default: break;             \
     }
+#define PCGB_MAC_COL_SWITCH(P1, P2, CALL)             \
+    switch (2 * (P1) + ((P2) - (P1))) {                \
+        case 14: CALL(7, 7); break;                    \
+        case 15: CALL(7, 8); break;                    \
+        case 16: CALL(8, 8); break;                    \
+        case 17: CALL(8, 9); break;                    \
+        case 18: CALL(9, 9); break;                    \
+        case 19: CALL(9, 10); break;                   \
+        case 20: CALL(10, 10); break;                  \
+        default: break;                                \
+    }
 
 __global__ void __launch_bounds__(kMixedColThreads, 2) mac_col_fwd_kernel(
     const MacReq* __restrict__ reqs, const MacCta* __restrict__ ctas) {
@@ -626,8 +649,8 @@ __global__ void __launch_bounds__(kMixedColThreads, 2) mac_col_fwd_kernel(
     const MacCta j = ctas[blockIdx.x];
     const MacReq& r = reqs[j.req];
     uint64_t* d = r.g + (static_cast<size_t>(j.q) << (r.l1 + r.l2));
-#define PCGB_CALL(LL) col_fwd_body<LL, mixed_C<LL>(), false>(d, d, r.l2, j.tile, r.tw1, sm)
-    PCGB_MAC_SWITCH(r.l1, PCGB_CALL)
+#define PCGB_CALL(LL, L2) col_fwd_body<LL, mixed_C<LL>(), false, L2>(d, d, L2, j.tile, r.tw1, sm)
+    PCGB_MAC_COL_SWITCH(r.l1, r.l2, PCGB_CALL)
 #undef PCGB_CALL
 }
 
@@ -649,11 +672,12 @@ __global__ void __launch_bounds__(kMixedColThreads, 2) mac_col_inv_kernel(
     extern __shared__ uint64_t sm[];
     const MacCta j = ctas[blockIdx.x];
     const MacReq& r = reqs[j.req];
-#define PCGB_CALL(LL) col_inv_body<LL, mixed_C<LL>()>(r.z, r.l2, j.tile, r.tw1i, sm)
-    PCGB_MAC_SWITCH(r.l1, PCGB_CALL)
+#define PCGB_CALL(LL, L2) col_inv_body<LL, mixed_C<LL>(), L2>(r.z, L2, j.tile, r.tw1i, sm)
+    PCGB_MAC_COL_SWITCH(r.l1, r.l2, PCGB_CALL)
 #undef PCGB_CALL
 }
 #undef PCGB_MAC_SWITCH
+#undef PCGB_MAC_COL_SWITCH
 
 // Shoup pair (v, floor(v * 2^64 / p)) of v < p given in Montgomery form
 // vR = v * 2^64 mod p: the quotient is (v * 2^64 - vR) / p, an exact
