@@ -201,6 +201,45 @@ __global__ void __launch_bounds__(128) expand_tops_kernel(
     tops_walk<W, PRG>(src, id, src_lvl, nlev, levels, cws, &aes_s, dst);
 }
 
+// Binary (w = 1) ChaCha8 walk of a depth D fixed at compile time: the
+// recursion keeps one pending right child per level in registers (its
+// two-way loop is not unrolled, so the code grows linearly with D), where
+// tops_walk's run-time depth keeps its stack in local memory.  LV is the
+// level below the source node (its CWs are cw[LV]); u the output offset of
+// the subtree.  Outputs in the same left-to-right order.
+template <int D, int LV = 0>
+struct TopsFixed1 {
+    __device__ __forceinline__ static void run(const Blk& node, const Blk* __restrict__ cw,
+                                               Blk* __restrict__ out, unsigned u) {
+        Blk k2[2];
+        children<1, kPrgChaCha>(node, cw + LV, static_cast<const AesSmem*>(nullptr), k2);
+        if constexpr (D == 1) {
+            stblk(out + u, k2[0]);
+            stblk(out + u + 1, k2[1]);
+        } else {
+            Blk cur = k2[0];
+            const Blk R = k2[1];
+#pragma unroll 1
+            for (unsigned i = 0; i < 2; ++i) {
+                TopsFixed1<D - 1, LV + 1>::run(cur, cw, out, u + (i << (D - 1)));
+                cur = R;
+            }
+        }
+    }
+};
+constexpr int kTopsFixedMax = 8;
+
+// expand_tops_kernel for ChaCha8, w = 1, nlev = D.
+template <int D>
+__global__ void __launch_bounds__(128) expand_tops_fixed_kernel(
+    const Blk* __restrict__ src, int K, int src_lvl, int levels, const Blk* __restrict__ cws,
+    Blk* __restrict__ dst) {
+    const size_t id = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (id >= (static_cast<size_t>(K) << src_lvl)) return;
+    const size_t key = id >> src_lvl;
+    TopsFixed1<D>::run(ldblk(src + id), cws + key * levels + src_lvl, dst + (id << D), 0);
+}
+
 // One stage of several key groups of different domains in one persistent
 // launch: the grid strides over the concatenated source nodes of all jobs;
 // job j owns global thread indices [first, first + K << (W * src_lvl)).
@@ -469,9 +508,26 @@ void launch_tops(const Blk* src, int K, int src_lvl, int nlev, int levels, const
         }
     }
     const int TPB = 128;
+    const unsigned grid = static_cast<unsigned>((threads + TPB - 1) / TPB);
+    if constexpr (PRG == kPrgChaCha && W == 1) {
+        if (nlev >= 1 && nlev <= kTopsFixedMax) {
+            switch (nlev) {
+#define PCGB_TF(D)                                                                            \
+    case D:                                                                                   \
+        expand_tops_fixed_kernel<D><<<grid, TPB, 0, st>>>(src, K, src_lvl, levels, cws, dst); \
+        break;
+                PCGB_TF(1) PCGB_TF(2) PCGB_TF(3) PCGB_TF(4)
+                PCGB_TF(5) PCGB_TF(6) PCGB_TF(7) PCGB_TF(8)
+#undef PCGB_TF
+                default: break;
+            }
+            PCGB_POST_LAUNCH();
+            return;
+        }
+    }
     const size_t smem = PRG == kPrgAes ? sizeof(AesSmem) : 0;
-    expand_tops_kernel<W, PRG><<<static_cast<unsigned>((threads + TPB - 1) / TPB), TPB, smem,
-                                 st>>>(src, K, src_lvl, nlev, levels, cws, te, rk, dst);
+    expand_tops_kernel<W, PRG><<<grid, TPB, smem, st>>>(src, K, src_lvl, nlev, levels, cws, te,
+                                                        rk, dst);
     PCGB_POST_LAUNCH();
 }
 
