@@ -25,6 +25,29 @@ def test_keyed_full_eval_matches_oracle(pcg, prg, n, w):
     assert (got == want).all()
 
 
+# ChaCha8 w = 1 top-walk stages of 1 .. 8 levels take the compile-time-depth
+# walk, deeper ones the run-time one.  Six keys give stages of n levels for
+# n <= 5; 2^14 keys give a 5-level stage and then one final stage of n - 5
+# levels (a stage of 2^19 or more subtrees is the last): 6, 7, 8 and 9.
+@pytest.mark.parametrize("K,n", [(6, 2), (6, 3), (6, 4), (1 << 14, 11), (1 << 14, 12),
+                                 (1 << 14, 13), (1 << 14, 14)])
+def test_keyed_eval_every_walk_depth(pcg, K, n):
+    rng = np.random.default_rng(900 + n)
+    roots = rng.integers(0, 2**64 - 1, (K, 2), dtype=np.uint64)
+    cws = rng.integers(0, 2**64 - 1, (K, n, 2), dtype=np.uint64)
+    D = 1 << n
+    d_r, d_c = dev(pcg, roots), dev(pcg, cws.reshape(-1, 2))
+    d_l = pcg.DeviceBuffer(16 * K * D)
+    pcg.dpf_keyed_full_eval_device(K, n, 1, O.PRG_CHACHA8, d_r.ptr, d_c.ptr, d_l.ptr)
+    pick = np.unique(np.concatenate([[0, K - 1], rng.integers(0, K, 30)]))
+    want = O.dpf_keyed_full_eval(len(pick), n, 1, roots[pick], cws[pick].reshape(-1, 2))
+    got = np.empty((len(pick), D, 2), np.uint64)
+    for i, k in enumerate(pick):
+        rc = pcg.lib.pcgb_memcpy_d2h(got[i].ctypes.data, d_l.ptr + 16 * D * int(k), 16 * D, None)
+        assert rc == 0
+    assert (got.reshape(-1, 2) == want).all()
+
+
 @pytest.mark.parametrize("prg", [O.PRG_CHACHA8, O.PRG_AES])
 @pytest.mark.parametrize("n,w", [(1, 1), (10, 1), (10, 2), (9, 3), (12, 4)])
 def test_interactive_stub_exchange_matches_oracle(pcg, prg, n, w):
