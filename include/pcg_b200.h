@@ -277,7 +277,9 @@ int pcgb_dpf_keyed_full_eval(int K, int n, int w, int prg, const pcgb_blk* d_roo
  * are device arrays; K, n and the pointer arrays are host arrays.  One
  * launch per top-walk stage serves every group (a persistent grid over a
  * per-stage job table), so the batch takes as many launches as its deepest
- * group has stages.  Leaves equal pcgb_dpf_keyed_full_eval's per group. */
+ * group has stages; for ChaCha8 with w = 1, one launch per distinct walk
+ * depth within a stage (each with the compile-time walk of that depth).
+ * Leaves equal pcgb_dpf_keyed_full_eval's per group. */
 int pcgb_dpf_keyed_full_eval_multi(int groups, const int* K, const int* n, int w, int prg,
                                    const pcgb_blk* const* d_roots, const pcgb_blk* const* d_cws,
                                    const uint8_t* round_keys, pcgb_blk* const* d_leaves,
@@ -339,8 +341,8 @@ int pcgb_expand_device(pcgb_expander* e, int party, const pcgb_blk* d_roots,
  * counterpart; the batching form of GPU_baseline/e2e_full_bench.cu's
  * expansion loop): request i runs expander e[i] for party[i] on the
  * device-resident inputs of pcgb_expand_device.  One launch per top-walk
- * stage, one fused leaf launch, one x launch and three NTT launches cover the
- * whole batch.  The expanders must share w, the ChaCha8 PRG and the leaf
+ * stage and walk depth, one fused leaf launch, one x launch and three NTT
+ * launches cover the whole batch.  The expanders must share w, the ChaCha8 PRG and the leaf
  * shape (leaves per thread; set with pcgb_expander_set_leaf_shape), be
  * unsharded, and have N in 2^14 .. 2^20; each request's x, z equal its
  * pcgb_expand_device outputs.  Each request's scratch comes from the

@@ -26,6 +26,19 @@ std::vector<int> tops_stages(int K, int w, int to_level) {
         l += s;
         b.push_back(l);
     }
+    if (w == 1) {
+        // Split deeper stages into pieces of at most kTopsFixedLevels, the
+        // last piece the full length: [7, 16) becomes [7, 8), [8, 16).
+        std::vector<int> out{b[0]};
+        for (size_t i = 1; i < b.size(); ++i) {
+            std::vector<int> cuts;
+            for (int e = b[i]; e - out.back() > kTopsFixedLevels; e -= kTopsFixedLevels)
+                cuts.push_back(e - kTopsFixedLevels);
+            out.insert(out.end(), cuts.rbegin(), cuts.rend());
+            out.push_back(b[i]);
+        }
+        b = out;
+    }
     return b;
 }
 

@@ -227,7 +227,8 @@ struct TopsFixed1 {
         }
     }
 };
-constexpr int kTopsFixedMax = 8;
+constexpr int kTopsFixedMax = kTopsFixedLevels;
+static_assert(kTopsFixedMax == 8, "one compile-time walk per depth 1 .. 8");
 
 // expand_tops_kernel for ChaCha8, w = 1, nlev = D.
 template <int D>
@@ -258,6 +259,50 @@ __global__ void __launch_bounds__(128) expand_tops_multi_kernel(
         while (j + 1 < njobs && jobs[j + 1].first <= g) ++j;
         const TopsJob J = jobs[j];
         tops_walk<W, PRG>(J.src, g - J.first, J.src_lvl, J.nlev, J.levels, J.cws, &aes_s, J.dst);
+    }
+}
+
+// expand_tops_multi_kernel for ChaCha8, w = 1, every job D levels deep.
+template <int D>
+__global__ void __launch_bounds__(128) expand_tops_multi_depth_kernel(
+    const TopsJob* __restrict__ jobs, int njobs, unsigned long long total) {
+    for (unsigned long long g = static_cast<unsigned long long>(blockIdx.x) * blockDim.x +
+                                threadIdx.x;
+         g < total; g += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        int j = 0;
+        while (j + 1 < njobs && jobs[j + 1].first <= g) ++j;
+        const TopsJob J = jobs[j];
+        const size_t id = g - J.first;
+        TopsFixed1<D>::run(ldblk(J.src + id), J.cws + (id >> J.src_lvl) * J.levels + J.src_lvl,
+                           J.dst + (id << D), 0);
+    }
+}
+
+// expand_tops_multi_kernel for ChaCha8, w = 1, jobs of different depths: a
+// job of 1 .. kTopsFixedMax levels takes the compile-time-depth walk of its
+// depth, a deeper one the run-time walk.
+__global__ void __launch_bounds__(128) expand_tops_multi_fixed_kernel(
+    const TopsJob* __restrict__ jobs, int njobs, unsigned long long total) {
+    for (unsigned long long g = static_cast<unsigned long long>(blockIdx.x) * blockDim.x +
+                                threadIdx.x;
+         g < total; g += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        int j = 0;
+        while (j + 1 < njobs && jobs[j + 1].first <= g) ++j;
+        const TopsJob J = jobs[j];
+        const size_t id = g - J.first;
+        const Blk* kcw = J.cws + (id >> J.src_lvl) * J.levels + J.src_lvl;
+        switch (J.nlev) {
+#define PCGB_TF(D)                                                          \
+    case D:                                                                 \
+        TopsFixed1<D>::run(ldblk(J.src + id), kcw, J.dst + (id << D), 0); \
+        break;
+            PCGB_TF(1) PCGB_TF(2) PCGB_TF(3) PCGB_TF(4)
+            PCGB_TF(5) PCGB_TF(6) PCGB_TF(7) PCGB_TF(8)
+#undef PCGB_TF
+            default:
+                tops_walk<1, kPrgChaCha>(J.src, id, J.src_lvl, J.nlev, J.levels, J.cws,
+                                         static_cast<const AesSmem*>(nullptr), J.dst);
+        }
     }
 }
 
@@ -648,6 +693,47 @@ void tops_multi_launch(const std::vector<TopsJob>& jobs, TopsJob* d_jobs,
     for (const TopsJob& J : jobs)
         if (J.nlev < 0 || J.nlev >= tops_max_depth<W>())
             fail(PCGB_EINVAL, "keyed expansion deeper than the DFS stack");
+    const int TPB = 128;
+    const unsigned long long cap = static_cast<unsigned long long>(sm_count()) * 8;  // persistent
+    if constexpr (PRG == kPrgChaCha && W == 1) {
+        // One launch per distinct depth in the stage, each with the
+        // compile-time walk of that depth (its own register budget); the
+        // jobs of a depth are contiguous in the table, their thread indices
+        // counted from the first of them.
+        std::vector<TopsJob> byd(jobs);
+        std::stable_sort(byd.begin(), byd.end(),
+                         [](const TopsJob& x, const TopsJob& y) { return x.nlev < y.nlev; });
+        std::vector<size_t> seg{0};
+        for (size_t i = 1; i < byd.size(); ++i)
+            if (byd[i].nlev != byd[i - 1].nlev) seg.push_back(i);
+        seg.push_back(byd.size());
+        std::vector<unsigned long long> seg_total(seg.size() - 1, 0);
+        for (size_t k = 0; k + 1 < seg.size(); ++k)
+            for (size_t i = seg[k]; i < seg[k + 1]; ++i) {
+                byd[i].first = seg_total[k];
+                seg_total[k] += static_cast<unsigned long long>(byd[i].K) << byd[i].src_lvl;
+            }
+        PCGB_CK(cudaMemcpyAsync(d_jobs, byd.data(), byd.size() * sizeof(TopsJob),
+                                cudaMemcpyHostToDevice, st));
+        for (size_t k = 0; k + 1 < seg.size(); ++k) {
+            const unsigned long long tot = seg_total[k];
+            if (tot == 0) continue;
+            const unsigned long long blocks = (tot + TPB - 1) / TPB;
+            const unsigned grid = static_cast<unsigned>(blocks < cap ? blocks : cap);
+            const TopsJob* dj = d_jobs + seg[k];
+            const int nj = static_cast<int>(seg[k + 1] - seg[k]);
+            switch (byd[seg[k]].nlev) {
+#define PCGB_TF(D)                                                                         \
+    case D: expand_tops_multi_depth_kernel<D><<<grid, TPB, 0, st>>>(dj, nj, tot); break;
+                PCGB_TF(1) PCGB_TF(2) PCGB_TF(3) PCGB_TF(4)
+                PCGB_TF(5) PCGB_TF(6) PCGB_TF(7) PCGB_TF(8)
+#undef PCGB_TF
+                default: expand_tops_multi_fixed_kernel<<<grid, TPB, 0, st>>>(dj, nj, tot);
+            }
+            PCGB_POST_LAUNCH();
+        }
+        return;
+    }
     PCGB_CK(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(TopsJob),
                             cudaMemcpyHostToDevice, st));
     if constexpr (PRG == kPrgAes) {
@@ -662,13 +748,11 @@ void tops_multi_launch(const std::vector<TopsJob>& jobs, TopsJob* d_jobs,
             return;
         }
     }
-    const int TPB = 128;
     const size_t smem = PRG == kPrgAes ? sizeof(AesSmem) : 0;
     const unsigned long long blocks = (total + TPB - 1) / TPB;
-    const unsigned long long cap = static_cast<unsigned long long>(sm_count()) * 8;  // persistent
-    expand_tops_multi_kernel<W, PRG><<<static_cast<unsigned>(blocks < cap ? blocks : cap), TPB,
-                                       smem, st>>>(d_jobs, static_cast<int>(jobs.size()), total,
-                                                   te, rk);
+    const unsigned grid = static_cast<unsigned>(blocks < cap ? blocks : cap);
+    expand_tops_multi_kernel<W, PRG><<<grid, TPB, smem, st>>>(d_jobs, static_cast<int>(jobs.size()),
+                                                              total, te, rk);
     PCGB_POST_LAUNCH();
 }
 

@@ -110,6 +110,9 @@ void keyed_expand_tops(int K, int n, int w, int prg, const Blk* roots, const Blk
 // subtrees, and the final stage walks from there to the target level.
 // 2^19 threads keep every SM busy and the final walks shallow.
 constexpr size_t kTopsStage2Threads = size_t{1} << 19;
+// w = 1 ChaCha8 stages of up to this many levels walk a depth fixed at
+// compile time (registers only); for w = 1 no stage is made deeper.
+constexpr int kTopsFixedLevels = 8;
 // Stage boundaries 0 = l_0 < l_1 < ... < l_s = to_level.
 std::vector<int> tops_stages(int K, int w, int to_level);
 

@@ -62,8 +62,9 @@ def test_batch_equals_single_expansions(pcg, expanders):
     for (e, *_), k, (wx, wz) in zip(reqs, keep, want):
         assert (k[6].download(np.uint64, e.N) == wx).all(), (e.N, e.c, e.t)
         assert (k[7].download(np.uint64, e.N) == wz).all(), (e.N, e.c, e.t)
-    # Stages: top walk (a few launches), leaf, x, three NTT passes.
-    assert batch_launches <= 10 < single_launches
+    # Top walk (one launch per stage and walk depth), leaf, x, three NTT
+    # passes, against eight launches per request one at a time.
+    assert batch_launches <= single_launches // 2
 
 
 def test_batch_request_matches_oracle(pcg, expanders):

@@ -25,10 +25,11 @@ def test_keyed_full_eval_matches_oracle(pcg, prg, n, w):
     assert (got == want).all()
 
 
-# ChaCha8 w = 1 top-walk stages of 1 .. 8 levels take the compile-time-depth
-# walk, deeper ones the run-time one.  Six keys give stages of n levels for
-# n <= 5; 2^14 keys give a 5-level stage and then one final stage of n - 5
-# levels (a stage of 2^19 or more subtrees is the last): 6, 7, 8 and 9.
+# ChaCha8 w = 1 top-walk stages take the compile-time-depth walk of their
+# depth, 1 .. 8 levels; a deeper last stage is split in two.  Six keys give
+# stages of n levels for n <= 5; 2^14 keys give a 5-level stage and then the
+# last stage (2^19 or more subtrees) of n - 5 levels: 6, 7, 8, and 9 split
+# into 1 + 8.
 @pytest.mark.parametrize("K,n", [(6, 2), (6, 3), (6, 4), (1 << 14, 11), (1 << 14, 12),
                                  (1 << 14, 13), (1 << 14, 14)])
 def test_keyed_eval_every_walk_depth(pcg, K, n):
@@ -212,7 +213,9 @@ MULTI_CASES = [
 def test_keyed_multi_domain_batch(pcg, prg, w, groups):
     """pcgb_dpf_keyed_full_eval_multi: key groups of different domains in one
     batch give each group's single-call leaves (and the oracle's for the
-    smallest group), in as many launches as the deepest group's stage plan."""
+    smallest group), in as many launches as the deepest group's stage plan
+    (ChaCha8, w = 1: one per stage and walk depth, so at least that many and
+    fewer than one call per group)."""
     nk = (1 << w) - 1
     rks = O.aes_tree_round_keys(np.arange(16, dtype=np.uint8), nk) if prg == O.PRG_AES else None
     rng = np.random.default_rng(len(groups) * 10 + w)
@@ -238,7 +241,11 @@ def test_keyed_multi_domain_batch(pcg, prg, w, groups):
     pcg.dpf_keyed_full_eval_multi_device([(K, n, r.ptr, c.ptr, o.ptr) for K, n, r, c, o in bufs],
                                          w, prg, round_keys=rks)
     pcg.synchronize()
-    assert pcg.launch_count() - before == max(stages)
+    launches = pcg.launch_count() - before
+    if prg == O.PRG_CHACHA8 and w == 1:
+        assert max(stages) <= launches < sum(stages)
+    else:
+        assert launches == max(stages)
     for (K, n, _, _, d_out), wv in zip(bufs, want):
         assert (d_out.download(np.uint64, 2 * (K << n)) == wv).all(), (K, n)
 
