@@ -312,6 +312,45 @@ __global__ void __launch_bounds__(128) expand_tops_multi_fixed_kernel(
 // table is filled once per CTA, not once per 128 threads).
 constexpr int kAesPrmtThreads = 1024;
 
+// TopsFixed1 for AES with the PRMT-addressed tables.
+template <int D, int LV = 0>
+struct TopsFixedAes {
+    __device__ __forceinline__ static void run(const Blk& node, const Blk* __restrict__ cw,
+                                               const AesPrmt* aes, Blk* __restrict__ out,
+                                               unsigned u) {
+        Blk k2[2];
+        children<1, kPrgAes>(node, cw + LV, aes, k2);
+        if constexpr (D == 1) {
+            stblk(out + u, k2[0]);
+            stblk(out + u + 1, k2[1]);
+        } else {
+            Blk cur = k2[0];
+            const Blk R = k2[1];
+#pragma unroll 1
+            for (unsigned i = 0; i < 2; ++i) {
+                TopsFixedAes<D - 1, LV + 1>::run(cur, cw, aes, out, u + (i << (D - 1)));
+                cur = R;
+            }
+        }
+    }
+};
+
+// expand_tops_prmt_kernel<1> with the walk depth D fixed at compile time.
+template <int D>
+__global__ void __launch_bounds__(kAesPrmtThreads) expand_tops_prmt_fixed_kernel(
+    const Blk* __restrict__ src, int K, int src_lvl, int levels, const Blk* __restrict__ cws,
+    const uint32_t* __restrict__ aes_te, const uint32_t* __restrict__ aes_rk,
+    Blk* __restrict__ dst) {
+    extern __shared__ __align__(16) unsigned char prmt_dsm[];
+    __shared__ AesPrmtKeys keys;
+    const AesPrmt A = aes_prmt_setup<1>(prmt_dsm, keys, aes_te, aes_rk);
+    const size_t total = static_cast<size_t>(K) << src_lvl;
+    for (size_t id = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; id < total;
+         id += static_cast<size_t>(gridDim.x) * blockDim.x)
+        TopsFixedAes<D>::run(ldblk(src + id), cws + (id >> src_lvl) * levels + src_lvl, &A,
+                             dst + (id << D), 0);
+}
+
 template <int W>
 __global__ void __launch_bounds__(kAesPrmtThreads) expand_tops_prmt_kernel(
     const Blk* __restrict__ src, int K, int src_lvl, int nlev, int levels,
@@ -542,6 +581,27 @@ void launch_tops(const Blk* src, int K, int src_lvl, int nlev, int levels, const
         // A stage with fewer threads than one wave of PRMT CTAs keeps the
         // replicated table in small CTAs, spread over every SM.
         if (threads >= aes_prmt_wave()) {
+            if constexpr (W == 1) {
+                if (nlev >= 1 && nlev <= kTopsFixedMax) {
+                    switch (nlev) {
+#define PCGB_TF(D)                                                                              \
+    case D:                                                                                     \
+        PCGB_CK(cudaFuncSetAttribute(expand_tops_prmt_fixed_kernel<D>,                          \
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,               \
+                                     static_cast<int>(kAesPrmtSmemBytes)));                     \
+        expand_tops_prmt_fixed_kernel<D><<<aes_prmt_grid(threads), kAesPrmtThreads,             \
+                                           kAesPrmtSmemBytes, st>>>(src, K, src_lvl, levels,    \
+                                                                    cws, te, rk, dst);          \
+        break;
+                        PCGB_TF(1) PCGB_TF(2) PCGB_TF(3) PCGB_TF(4)
+                        PCGB_TF(5) PCGB_TF(6) PCGB_TF(7) PCGB_TF(8)
+#undef PCGB_TF
+                        default: break;
+                    }
+                    PCGB_POST_LAUNCH();
+                    return;
+                }
+            }
             PCGB_CK(cudaFuncSetAttribute(expand_tops_prmt_kernel<W>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(kAesPrmtSmemBytes)));
