@@ -1003,6 +1003,21 @@ void ntt_forward(const NttPlan& pl, uint64_t* d, int batch, cudaStream_t st) {
     row_fwd(pl, d, batch, st);
 }
 
+// Per device: a second stream and two events for the two-half schedule of
+// poly_mul_device; the mutex keeps one call's fork, launches and join
+// together when several host threads multiply on the same device.
+struct HalfFork {
+    std::mutex mu;
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+HalfFork& half_fork() {
+    static HalfFork f[64];
+    int dev = 0;
+    PCGB_CK(cudaGetDevice(&dev));
+    return f[dev];
+}
+
 void poly_mul_device(const NttPlan& pl, uint64_t* c, const uint64_t* a, const uint64_t* b,
                      int batch, uint64_t* scratch, cudaStream_t st) {
     const ulonglong2* wir = wi_times_r(const_cast<NttPlan&>(pl), st);
@@ -1011,6 +1026,39 @@ void poly_mul_device(const NttPlan& pl, uint64_t* c, const uint64_t* a, const ui
     // launches (each needs about 70 registers a thread where the fused
     // pass needs 96, so more CTAs fit on an SM).
     // a is read before c is first written, so c may alias a or b.
+    // A batch of two or more runs as two halves on two streams, pass by
+    // pass: each pass kernel alone leaves the IMAD pipe a third idle (its
+    // barriers and its tail), and the other half's CTAs fill those slots
+    // (16 x 2^20: 0.882 -> 0.843 ms; four quarters gave 0.839).  Each half
+    // reads and writes only its own products, so aliasing holds per half.
+    if (batch >= 2) {
+        HalfFork& f = half_fork();
+        std::lock_guard<std::mutex> lk(f.mu);
+        if (!f.side) {
+            PCGB_CK(cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming));
+            PCGB_CK(cudaEventCreateWithFlags(&f.join, cudaEventDisableTiming));
+            PCGB_CK(cudaStreamCreateWithFlags(&f.side, cudaStreamNonBlocking));
+        }
+        const int h0 = batch / 2, h1 = batch - h0;
+        const size_t o = static_cast<size_t>(h0) * pl.N;
+        PCGB_CK(cudaEventRecord(f.fork, st));
+        PCGB_CK(cudaStreamWaitEvent(f.side, f.fork, 0));
+        col_fwd(pl, a, scratch, h0, true, st);
+        col_fwd(pl, a + o, scratch + o, h1, true, f.side);
+        row_fwd(pl, scratch, h0, st);
+        row_fwd(pl, scratch + o, h1, f.side);
+        col_fwd(pl, b, c, h0, true, st);
+        col_fwd(pl, b + o, c + o, h1, true, f.side);
+        row_fwd(pl, c, h0, st);
+        row_fwd(pl, c + o, h1, f.side);
+        row_pmul_inv(pl, c, scratch, h0, wir, st);
+        row_pmul_inv(pl, c + o, scratch + o, h1, wir, f.side);
+        col_inv(pl, c, h0, st);
+        col_inv(pl, c + o, h1, f.side);
+        PCGB_CK(cudaEventRecord(f.join, f.side));
+        PCGB_CK(cudaStreamWaitEvent(st, f.join, 0));
+        return;
+    }
     col_fwd(pl, a, scratch, batch, true, st);
     row_fwd(pl, scratch, batch, st);
     col_fwd(pl, b, c, batch, true, st);
